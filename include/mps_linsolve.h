@@ -1,0 +1,169 @@
+/*
+ * mps_linsolve.h -- C ABI of the B200 multigrid / Krylov linear solver for the
+ * mps3d 7-point finite-volume operators.
+ *
+ * The entry points replace the solver calls of the reference's equation
+ * modules (plain C types only: no CUDA or torch types in the signatures; the
+ * stream of the *_dev variants is a cudaStream_t passed as void*):
+ *
+ *   mps_vcycle_once   <- perform_vcycle, mgridlib/mgridsteps.f90:384-417
+ *                        (one call, same arguments and in/out meaning)
+ *   mps_linsolve      <- the caller loop "do i=1,nvcycles; call perform_vcycle;
+ *                        if(resnorm .le. err_tol) exit" of
+ *                        plasma_pde/poissoneq.f90:427-450,
+ *                        plasma_pde/edeneq.f90:489-503, plasma_pde/ionseq.f90:600-614,
+ *                        plasma_pde/eenergyeq.f90:817-829,
+ *                        plasma_pde/neutralseq.f90:481-494, generic_pde/pdedefs.f90:304-328
+ *   mps_apply_A       <- find_AX, mgridlib/discretepde.f90:672-1119 (AX only)
+ *   mps_find_bvec     <- find_bvec, mgridlib/discretepde.f90:382-618 (applybcflag=.true.)
+ *   mps_fill_ghosts   <- update_boundary_ghostvalues, mgridlib/discretepde.f90:1121-1267
+ *
+ * Array conventions are the reference's: real*8 fields ghosted by one layer
+ * (-g_nglayers+1 : l+g_nglayers, par_decompose.f90:18) in Fortran order
+ * (i fastest); vel carries a trailing NDIM=3 axis; face arrays are
+ * left/right (ly,lz), bottom/top (lx,lz), back/front (lx,ly)
+ * (globalvars.f90:57-66); faces are ordered LEFT, RIGHT, BOTTOM, TOP, BACK,
+ * FRONT (globalvars.f90:11-17).  The reference's character(4) codes map to
+ * the MPS_BC_* integers below.
+ *
+ * Errors are returned as an integer status; the library never aborts, traps
+ * or exits (the reference calls abort()/MPI_Abort at gmres.f90:398 and
+ * mgridsteps.f90:359).
+ */
+#ifndef MPS_LINSOLVE_H
+#define MPS_LINSOLVE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+enum mps_status {
+    MPS_OK = 0,
+    MPS_ERR_NOT_CONVERGED = 1, /* maxit reached; the reference silently accepts this */
+    MPS_ERR_NAN = 2,           /* NaN/Inf in a residual or Krylov quantity (gmres.f90:113-120) */
+    MPS_ERR_BREAKDOWN = 3,     /* singular coarse operator or Krylov breakdown */
+    MPS_ERR_BAD_ARG = 4,
+    MPS_ERR_TIMEOUT = 5,       /* a bounded device-side wait expired */
+    MPS_ERR_CUDA = 6,
+    MPS_ERR_NOMEM = 7
+};
+
+/* ---- boundary-condition codes (discretepde.f90; PERI is an extension) ---- */
+enum { MPS_BC_DIRC = 1, MPS_BC_FLUX = 2, MPS_BC_ZGRD = 3, MPS_BC_PERI = 4, MPS_BC_DZGD = 5 };
+
+enum { MPS_HIER_CELL = 0,      /* reference hierarchy: l/2 by integer division,
+                                  8-cell average, central-slope prolongation,
+                                  coarsest when a per-rank size reaches LMIN=1 */
+       MPS_HIER_GEOM = 1 };    /* any size: l/2 cells with the odd cell merged into the
+                                  last coarse cell, exact cell widths, volume-weighted
+                                  restriction, trilinear prolongation (extension) */
+enum { MPS_PREC_FP64 = 0, MPS_PREC_MIXED = 1 };  /* MIXED: FP32 V-cycle inside FP64 refinement */
+enum { MPS_KRYLOV_NONE = 0, MPS_KRYLOV_FGMRES = 1 };
+enum { MPS_FLUX_UPWIND = 0, MPS_FLUX_SG = 1 };
+enum { MPS_TOL_RMS_ABS = 0,    /* sqrt(sum r^2 / ncells) <= tol (compute_norm, globalvars.f90:136-159) */
+       MPS_TOL_REL_L2 = 1 };   /* ||b - A x||_2 / ||b||_2 <= tol */
+
+typedef struct {
+    int lx, ly, lz;                /* cells per direction (g_lx, g_ly, g_lz) */
+    double llenx, lleny, llenz;    /* box lengths (g_llenx, ...; dx = llenx/lx) */
+} mps_grid;
+
+typedef struct {
+    double tol;          /* default 1e-10 */
+    int tol_kind;        /* MPS_TOL_*; default REL_L2 */
+    int maxit;           /* outer iterations (V-cycles or FGMRES steps); default 50 */
+    int nu1, nu2;        /* pre/post red-black GS sweeps; default 2,2 (mgridsteps.f90:473) */
+    int hierarchy;       /* MPS_HIER_*; default GEOM */
+    int ranks[3];        /* CELL only: rank layout px,py,pz fixing the coarsest level; default 1,1,1 */
+    int max_coarse;      /* GEOM only: coarsen while a level has more cells; default 125 */
+    int precision;       /* MPS_PREC_*; default FP64 */
+    int inner_cycles;    /* MIXED: FP32 V-cycles per FP64 refinement step; default 0 = automatic */
+    int krylov;          /* MPS_KRYLOV_*; default NONE (stationary V-cycle iteration) */
+    int restart;         /* FGMRES restart length m; default 30 */
+    int fill_ghosts;     /* 1: write solution ghosts like update_boundary_ghostvalues; default 0 */
+    int use_graph;       /* 1: replay the V-cycle as a CUDA graph; default 1 */
+    int transpose;       /* 1: solve with A^T (adjoint); default 0 */
+    int flux;            /* MPS_FLUX_*: convective flux of the operator; default UPWIND
+                            (find_AX); SG = Scharfetter-Gummel faces
+                            (mps1d/source/convdiff.f90:10-64) */
+} mps_solver_opts;
+
+typedef struct {
+    int status;          /* mps_status of the solve */
+    int iters;           /* outer iterations done */
+    int vcycles;         /* V-cycles done (all precisions) */
+    int levels;          /* multigrid levels including the coarsest */
+    double rel_res;      /* final ||b - A x||_2 / ||b||_2 (FP64) */
+    double rms_res;      /* final sqrt(sum r^2 / ncells), the reference's norm */
+    double rel_res0;     /* initial relative residual */
+    double time_ms;      /* device time of the solve (CUDA events) */
+} mps_solve_info;
+
+typedef struct mps_handle_s* mps_handle;
+
+/* defaults listed in mps_solver_opts */
+void mps_default_opts(mps_solver_opts* o);
+/* library version string */
+const char* mps_version(void);
+
+/* A handle owns a CUDA stream and the device workspace (level hierarchy,
+ * coefficient pyramid, Krylov basis), reused across calls with the same grid.
+ * device < 0 selects the current device. */
+int mps_create(mps_handle* h, int device);
+int mps_destroy(mps_handle h);
+/* the handle's stream (cudaStream_t) */
+void* mps_stream(mps_handle h);
+/* text of the last error seen by the handle ("" when none) */
+const char* mps_last_error(mps_handle h);
+
+/* Solve A soln = b with b = find_bvec(applybcflag=.true.) + mgridsterm.
+ * Host pointers (Fortran-order ghosted arrays, copied to and from the device
+ * inside the call).  vel, reac and mgridsterm may be NULL (zero).  soln holds
+ * the initial guess on entry and the solution on exit (interior; ghosts too
+ * when opts->fill_ghosts).  Replaces the caller loop around perform_vcycle. */
+int mps_linsolve(mps_handle h, const mps_grid* g, int timederiv, double dt,
+                 const double* vel, const double* dcoeff, const double* reac,
+                 const double* source, const int bc_code[6], const double* const bcval[6],
+                 const double* mgridsterm, double* soln, const mps_solver_opts* opts,
+                 mps_solve_info* info);
+
+/* Same with device pointers on `stream` (cudaStream_t, NULL = handle's stream);
+ * no host<->device copies of the fields. */
+int mps_linsolve_dev(mps_handle h, const mps_grid* g, int timederiv, double dt,
+                     const double* vel, const double* dcoeff, const double* reac,
+                     const double* source, const int bc_code[6], const double* const bcval[6],
+                     const double* mgridsterm, double* soln, const mps_solver_opts* opts,
+                     mps_solve_info* info, void* stream);
+
+/* Exactly one V-cycle with perform_vcycle's meaning (host pointers):
+ * soln in/out (ghosted), resnorm out = RMS norm of the post-smoothing
+ * residual (mgridsteps.f90:575).  opts may be NULL (CELL hierarchy, 2/2 sweeps). */
+int mps_vcycle_once(mps_handle h, const mps_grid* g, int timederiv, double dt,
+                    const double* vel, const double* dcoeff, const double* reac,
+                    const double* source, const int bc_code[6], const double* const bcval[6],
+                    const double* mgridsterm, double* soln, double* resnorm,
+                    const mps_solver_opts* opts);
+
+/* AX = A soln (interior, Fortran order), device pointers; opts selects the flux
+ * scheme and transpose. */
+int mps_apply_A_dev(mps_handle h, const mps_grid* g, int timederiv, double dt,
+                    const double* vel, const double* dcoeff, const double* reac,
+                    const int bc_code[6], const double* soln, double* AX,
+                    const mps_solver_opts* opts, void* stream);
+
+/* b = find_bvec (applybcflag=.true.) + mgridsterm, device pointers, interior out. */
+int mps_find_bvec_dev(mps_handle h, const mps_grid* g, const double* vel, const double* dcoeff,
+                      const double* source, const int bc_code[6], const double* const bcval[6],
+                      const double* mgridsterm, double* b, const mps_solver_opts* opts,
+                      void* stream);
+
+/* Ghost layer of a ghosted field per update_boundary_ghostvalues (+ periodic
+ * wrap), device pointers. */
+int mps_fill_ghosts_dev(mps_handle h, const mps_grid* g, const int bc_code[6],
+                        const double* const bcval[6], double* soln, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPS_LINSOLVE_H */

@@ -1,0 +1,550 @@
+// mps_kernels.cuh -- CUDA kernels of the B200 multigrid / Krylov solver.
+// All kernels are memory-bound 7-point stencils, transfers or reductions
+// (arithmetic intensity well below the FP64 ridge); none uses tensor cores.
+#pragma once
+
+#include "mps_core.cuh"
+
+namespace mps {
+
+constexpr int TPB = 256;
+
+template <class T>
+struct ZeroU {  // accessor of a field known to be zero
+    __device__ __forceinline__ T get(const Lev&, int, int, int) const { return T(0); }
+};
+template <class T>
+struct OtherOnlyU {  // colour c known zero, the other colour read from memory
+    const T* other;  // half 1-c
+    int c;
+    __device__ __forceinline__ T get(const Lev& L, int i, int j, int k) const
+    {
+        return scol(i, j, k) == c ? T(0) : __ldg(&other[soff(L, i, j, k)]);
+    }
+};
+
+// ---------------------------------------------------------------------
+// one colour pass of red-black Gauss-Seidel, out of place:
+//   out[c] = (f[c] - offdiag(u)) / diag, u = state at the start of the pass
+// (perform_gseidel_smoothing, discretepde.f90:202-229; the reference
+// computes offdiag of all cells before updating a colour, so cells of one
+// colour never see each other's new values -- the same rule holds here at
+// periodic seams of odd size where equal colours touch)
+// ---------------------------------------------------------------------
+template <class T, class Op, class U>
+__global__ void __launch_bounds__(TPB) k_colour(Lev L, Op op, int c, U u, T* __restrict__ out,
+                                                const T* __restrict__ f)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    int i, j, k;
+    if (!decode(L, t, c, i, j, k)) return;
+    T diag, off;
+    row_eval(op, L, u, i, j, k, diag, off);
+    out[t] = gs_value(__ldg(&f[t]), diag, off);
+}
+
+// ---------------------------------------------------------------------
+// residual r = f - A u on the fine level fused with the restriction to the
+// coarse level: coarse value = mean of r over the children {2I,2I+1}^3 that
+// exist (restriction, mgridsteps.f90:11-53, applied to the residual at :531).
+// One thread per coarse cell, natural order.
+// ---------------------------------------------------------------------
+template <class T, class Op>
+__global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
+                                                        Split<T> fc, int geom)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned ncx = C.nx, ncy = C.ny;
+    if (t >= ncx * ncy * (unsigned)C.nz) return;
+    unsigned K = t / (ncx * ncy);
+    unsigned rem = t - K * ncx * ncy;
+    unsigned J = rem / ncx;
+    unsigned I = rem - J * ncx;
+    const int cI[3] = {(int)I, (int)J, (int)K};
+    int lo[3], cnt[3];
+    for (int a = 0; a < 3; a++) {
+        const int nf = lev_n(F, a), nc = lev_n(C, a);
+        lo[a] = nf == nc ? cI[a] : 2 * cI[a];
+        cnt[a] = nf == nc ? 1 : ((geom && cI[a] == nc - 1) ? nf - 2 * (nc - 1) : 2);
+    }
+    T s = T(0), vol = T(0);
+    for (int dk = 0; dk < cnt[2]; dk++) {
+        const int k = lo[2] + dk;
+        const T wz = geom ? (T)cwidth(F, 2, k) : T(1);
+        for (int dj = 0; dj < cnt[1]; dj++) {
+            const int j = lo[1] + dj;
+            const T wy = geom ? (T)cwidth(F, 1, j) : T(1);
+            for (int di = 0; di < cnt[0]; di++) {
+                const int i = lo[0] + di;
+                const T wx = geom ? (T)cwidth(F, 0, i) : T(1);
+                T diag, off;
+                row_eval(op, F, u, i, j, k, diag, off);
+                T r = f.get(F, i, j, k) - (diag * u.get(F, i, j, k) + off);
+                const T v = wx * wy * wz;
+                s += v * r;
+                vol += v;
+            }
+        }
+    }
+    const int ci = I, cj = J, ck = K;
+    fc.c[scol(ci, cj, ck)][soff(C, ci, cj, ck)] = geom ? s / vol : s * (T(1) / vol);
+}
+
+// coarse ghost rule for the correction (update_boundary_ghostvalues applied
+// to restrictsolnnew - restrictsolnold, mgridsteps.f90:552-562): Dirichlet
+// faces mirror with a sign flip, other physical faces copy, periodic wraps
+template <class T>
+__device__ __forceinline__ T coarse_nbr(const Lev& C, const CSplit<T>& e, int I, int J, int K, int ax, int s,
+                                        T e0)
+{
+    int a = I, b = J, c = K;
+    if (nbr(C, ax, s, a, b, c)) return e.get(C, a, b, c);
+    return C.bc[2 * ax + (s > 0)] == BC_DIRC ? -e0 : e0;
+}
+
+// coarse correction at (I,J,K) where any index may be a ghost (-1 or n):
+// each ghost axis maps to the adjacent cell with the sign of its face rule
+// (Dirichlet -1, other +1) or wraps (periodic); equals the face ghosts of
+// update_boundary_ghostvalues, extended to edges and corners
+template <class T>
+__device__ __forceinline__ T coarse_at(const Lev& C, const CSplit<T>& e, int I, int J, int K)
+{
+    int q[3] = {I, J, K};
+    T sgn = T(1);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const int n = lev_n(C, a);
+        if (q[a] >= 0 && q[a] < n) continue;
+        const int side = q[a] < 0 ? 0 : 1;
+        if (C.per[a]) q[a] = q[a] < 0 ? n - 1 : 0;
+        else {
+            if (C.bc[2 * a + side] == BC_DIRC) sgn = -sgn;
+            q[a] = q[a] < 0 ? 0 : n - 1;
+        }
+    }
+    return sgn * e.get(C, q[0], q[1], q[2]);
+}
+
+// ---------------------------------------------------------------------
+// prolongation + correction u_f += P e_c.  CELL: prolongation1
+// (mgridsteps.f90:170-216, correction :567): e_c + sum_ax +-1/8 *
+// (e[I+1]-e[I-1]), odd last fine cell uncorrected.  GEOM: tensor-product
+// linear interpolation between the bracketing coarse centres.  One thread
+// per fine cell.
+// ---------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned nx = F.nx, ny = F.ny;
+    if (t >= nx * ny * (unsigned)F.nz) return;
+    unsigned k = t / (nx * ny);
+    unsigned rem = t - k * nx * ny;
+    unsigned j = rem / nx;
+    unsigned i = rem - j * nx;
+    T v;
+    if (!X.geom) {
+        int I = i >> 1, J = j >> 1, K = k >> 1;
+        if (I >= C.nx || J >= C.ny || K >= C.nz) return;  // odd last cell dropped
+        const T e0 = e.get(C, I, J, K);
+        const T ax = (i & 1) ? T(0.125) : T(-0.125);
+        const T ay = (j & 1) ? T(0.125) : T(-0.125);
+        const T az = (k & 1) ? T(0.125) : T(-0.125);
+        const T dx = coarse_at(C, e, I + 1, J, K) - coarse_at(C, e, I - 1, J, K);
+        const T dy = coarse_at(C, e, I, J + 1, K) - coarse_at(C, e, I, J - 1, K);
+        const T dz = coarse_at(C, e, I, J, K + 1) - coarse_at(C, e, I, J, K - 1);
+        v = e0 + ((ax * dx + ay * dy) + az * dz);
+    } else {
+        int a0[3], a1[3];
+        double tt[3];
+        geom_lin(X, 0, (int)i, a0[0], a1[0], tt[0]);
+        geom_lin(X, 1, (int)j, a0[1], a1[1], tt[1]);
+        geom_lin(X, 2, (int)k, a0[2], a1[2], tt[2]);
+        v = T(0);
+        for (int cz = 0; cz < 2; cz++) {
+            const T wz = (T)(cz ? tt[2] : 1.0 - tt[2]);
+            if (wz == T(0)) continue;
+            for (int cy = 0; cy < 2; cy++) {
+                const T wy = (T)(cy ? tt[1] : 1.0 - tt[1]);
+                if (wy == T(0)) continue;
+                for (int cx = 0; cx < 2; cx++) {
+                    const T wx = (T)(cx ? tt[0] : 1.0 - tt[0]);
+                    if (wx == T(0)) continue;
+                    v += wz * wy * wx *
+                         coarse_at(C, e, cx ? a1[0] : a0[0], cy ? a1[1] : a0[1], cz ? a1[2] : a0[2]);
+                }
+            }
+        }
+    }
+    T* p = &u.c[scol(i, j, k)][soff(F, i, j, k)];
+    *p = *p + v;
+}
+
+// ---------------------------------------------------------------------
+// exact coarsest solve: u = A^{-1} f with the inverse precomputed (column
+// major, FP64).  Replaces bottomsolve's full-dimension GMRES
+// (mgridsteps.f90:218-382), which is an exact solve as well.  One CTA.
+// ---------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(512) k_coarse_solve(Lev C, const double* __restrict__ AinvT, CSplit<T> f,
+                                                      Split<T> u)
+{
+    extern __shared__ double fs[];
+    const int n = C.nx * C.ny * C.nz;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        int i = r % C.nx, j = (r / C.nx) % C.ny, k = r / (C.nx * C.ny);
+        fs[r] = (double)f.get(C, i, j, k);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        double acc = 0.0;
+        for (int q = 0; q < n; q++) acc += AinvT[(long long)q * n + r] * fs[q];
+        int i = r % C.nx, j = (r / C.nx) % C.ny, k = r / (C.nx * C.ny);
+        u.c[scol(i, j, k)][soff(C, i, j, k)] = (T)acc;
+    }
+}
+
+// dense assembly of the coarsest operator (row major, FP64, pre-zeroed)
+template <class T>
+__device__ __forceinline__ void dense_row(const KOp<T>& op, const Lev& L, int i, int j, int k, double* A, int n)
+{
+    const int r = i + L.nx * (j + L.ny * k);
+    const double kc = (double)kval(op, L, i, j, k);
+    double d = op.dex[0] ? (double)op.dex[scol(i, j, k)][soff(L, i, j, k)] : (double)op.dexc;
+    for (int ax = 0; ax < 3; ax++)
+        for (int s = -1; s <= 1; s += 2) {
+            int a = i, b = j, c = k;
+            const int p = ax == 0 ? i : (ax == 1 ? j : k);
+            if (nbr(L, ax, s, a, b, c)) {
+                const int q = ax == 0 ? a : (ax == 1 ? b : c);
+                double w = 0.5 * (kc + (double)kval(op, L, a, b, c)) * fcoef(L, ax, p, q);
+                d += w;
+                A[(long long)r * n + (a + L.nx * (b + L.ny * c))] -= w;
+            } else if (L.bc[2 * ax + (s > 0)] == BC_DIRC) {
+                d += kc * dcoef(L, ax, p);
+            }
+        }
+    A[(long long)r * n + r] += d;
+}
+template <class T>
+__device__ __forceinline__ void dense_row(const ROp<T>& op, const Lev& L, int i, int j, int k, double* A, int n)
+{
+    const int r = i + L.nx * (j + L.ny * k);
+    const int c0 = scol(i, j, k);
+    const long long o0 = soff(L, i, j, k);
+    A[(long long)r * n + r] += (double)op.r[0][c0][o0];
+    for (int ax = 0; ax < 3; ax++)
+        for (int s = -1; s <= 1; s += 2) {
+            int a = i, b = j, c = k;
+            if (nbr(L, ax, s, a, b, c))
+                A[(long long)r * n + (a + L.nx * (b + L.ny * c))] += (double)op.r[1 + 2 * ax + (s > 0)][c0][o0];
+        }
+}
+template <class T, class Op>
+__global__ void k_dense_assemble(Lev L, Op op, double* A)
+{
+    const int n = L.nx * L.ny * L.nz;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        int i = r % L.nx, j = (r / L.nx) % L.ny, k = r / (L.nx * L.ny);
+        dense_row(op, L, i, j, k, A, n);
+    }
+}
+
+// Gauss-Jordan inverse with partial pivoting of the n x n row-major A held in
+// M = [A | I] (n x 2n, row major, prepared by k_gj_prepare); writes the
+// inverse column-major to AinvT.  One CTA; status[0] |= 1 on a zero pivot.
+__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* M, double* AinvT, int* status);
+__global__ void k_gj_prepare(int n, const double* A, double* M);
+
+// ---------------------------------------------------------------------
+// residual + norm: r = f - A u; sum r^2 (and sum f^2) reduced
+// deterministically (per-block partials, the last block sums them in
+// block order).  Optionally writes r (converted to R) to a split field.
+// ---------------------------------------------------------------------
+struct RedBuf {
+    double* partial;      // [2 * maxblocks]
+    unsigned* counter;    // zero-initialised
+    double* out;          // [2]: sum r^2, sum f^2
+};
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    __syncthreads();
+    return s;  // valid in thread 0
+}
+
+__device__ __forceinline__ void finish_two(RedBuf rb, double a, double b, double* sh)
+{
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        rb.partial[2 * blockIdx.x] = a;
+        rb.partial[2 * blockIdx.x + 1] = b;
+        __threadfence();
+        unsigned prev = atomicAdd(rb.counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for (unsigned q = threadIdx.x; q < gridDim.x; q += blockDim.x) {
+        sa += ((volatile double*)rb.partial)[2 * q];
+        sb += ((volatile double*)rb.partial)[2 * q + 1];
+    }
+    sa = block_sum(sa, sh);
+    sb = block_sum(sb, sh);
+    if (threadIdx.x == 0) {
+        rb.out[0] = sa;
+        rb.out[1] = sb;
+        *rb.counter = 0u;
+    }
+}
+
+template <class T, class Op, class R>
+__global__ void __launch_bounds__(TPB) k_resid_norm(Lev L, Op op, CSplit<T> u, CSplit<T> f, Split<R> rout,
+                                                    RedBuf rb)
+{
+    __shared__ double sh[32];
+    double rr = 0.0, ff = 0.0;
+    const unsigned total = (unsigned)L.P * L.rows;
+    for (int c = 0; c < 2; c++) {
+        unsigned t = blockIdx.x * TPB + threadIdx.x;
+        int i, j, k;
+        if (t < total && decode(L, t, c, i, j, k)) {
+            T diag, off;
+            row_eval(op, L, u, i, j, k, diag, off);
+            T fv = __ldg(&f.c[c][t]);
+            T r = fv - (diag * __ldg(&u.c[c][t]) + off);
+            rr += (double)r * (double)r;
+            ff += (double)fv * (double)fv;
+            if (rout.c[0]) rout.c[c][t] = (R)r;
+        }
+    }
+    double a = block_sum(rr, sh);
+    double b = block_sum(ff, sh);
+    finish_two(rb, a, b, sh);
+}
+
+// out = A u (FP64 out, u of any precision), split layout
+template <class T, class Op, class Tu>
+__global__ void __launch_bounds__(TPB) k_apply(Lev L, Op op, CSplit<Tu> u, Split<double> out)
+{
+    const unsigned total = (unsigned)L.P * L.rows;
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    if (t >= total) return;
+    for (int c = 0; c < 2; c++) {
+        int i, j, k;
+        if (decode(L, t, c, i, j, k)) {
+            T diag, off;
+            row_eval(op, L, u, i, j, k, diag, off);
+            out.c[c][t] = (double)(diag * (T)__ldg(&u.c[c][t]) + off);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// setup: ghosted Fortran-order FP64 <-> split layout
+// ---------------------------------------------------------------------
+template <class T>
+__global__ void k_pack(Lev L, const double* __restrict__ g, Split<T> out, double scale, double shift)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned nx = L.nx, ny = L.ny;
+    if (t >= nx * ny * (unsigned)L.nz) return;
+    unsigned k = t / (nx * ny);
+    unsigned rem = t - k * nx * ny;
+    unsigned j = rem / nx;
+    unsigned i = rem - j * nx;
+    long long gi = (long long)(i + 1) + (long long)(nx + 2) * ((long long)(j + 1) + (long long)(ny + 2) * (k + 1));
+    double v = g ? g[gi] * scale + shift : shift;
+    out.c[scol(i, j, k)][soff(L, i, j, k)] = (T)v;
+}
+
+template <class T>
+__global__ void k_unpack(Lev L, CSplit<T> in, double* __restrict__ g)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned nx = L.nx, ny = L.ny;
+    if (t >= nx * ny * (unsigned)L.nz) return;
+    unsigned k = t / (nx * ny);
+    unsigned rem = t - k * nx * ny;
+    unsigned j = rem / nx;
+    unsigned i = rem - j * nx;
+    long long gi = (long long)(i + 1) + (long long)(nx + 2) * ((long long)(j + 1) + (long long)(ny + 2) * (k + 1));
+    g[gi] = (double)in.get(L, i, j, k);
+}
+
+// interior split -> natural (unghosted) FP64
+template <class T>
+__global__ void k_unpack_nat(Lev L, CSplit<T> in, double* __restrict__ g)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned nx = L.nx, ny = L.ny;
+    if (t >= nx * ny * (unsigned)L.nz) return;
+    unsigned k = t / (nx * ny);
+    unsigned rem = t - k * nx * ny;
+    unsigned j = rem / nx;
+    unsigned i = rem - j * nx;
+    g[t] = (double)in.get(L, i, j, k);
+}
+
+// max |x| over the interior of a ghosted field (x - x(1,1,1) when rel=1),
+// reduced with an integer atomicMax on the bit pattern (valid for >= 0)
+__global__ void k_maxabs(Lev L, const double* __restrict__ g, int rel, unsigned long long* out);
+
+// update_boundary_ghostvalues (discretepde.f90:1121-1267) + periodic wrap,
+// on a ghosted FP64 field; faces only (edges/corners untouched, as in the
+// reference)
+__global__ void k_fill_ghosts(Lev L, double* __restrict__ g, const double* bl, const double* br, const double* bb,
+                              const double* bt, const double* bk, const double* bf);
+
+// find_bvec (discretepde.f90:382-618, applybcflag=.true.) + mgridsterm, split
+// FP64 out.  flux=1 uses the half-cell Scharfetter-Gummel weights for DIRC.
+__global__ void k_find_bvec(Lev L, const double* __restrict__ vel, const double* __restrict__ dcoeff,
+                            const double* __restrict__ source, const double* bl, const double* br,
+                            const double* bb, const double* bt, const double* bk, const double* bf,
+                            const double* __restrict__ sterm, int flux, Split<double> b);
+
+// aggregation average (volume weighted for the geometric hierarchy) of a
+// split FP64 field onto the next coarser level
+__global__ void k_restrict_field(Lev F, CSplit<double> in, Lev C, Split<double> out, int geom);
+
+// rows of the upwind (find_AX) or Scharfetter-Gummel operator from split FP64
+// cell fields of one level
+
+// dex = -reac + dtinv, k cast, in split layout
+
+// ---- flat vector kernels (length n, split arrays including zero pads) ----
+__global__ void k_multidot(long long n, int m, const double* const* __restrict__ V, const double* __restrict__ w,
+                           double* __restrict__ partial);
+__global__ void k_multidot_finish(int m, int nblocks, const double* __restrict__ partial, double* __restrict__ h,
+                                  int accumulate);
+__global__ void k_multiaxpy(long long n, int m, const double* const* __restrict__ V, const double* __restrict__ h,
+                            double* __restrict__ w);
+__global__ void k_scale_to(long long n, const double* __restrict__ w, const double* __restrict__ hn, int idx,
+                           double* __restrict__ v, float* __restrict__ v32);
+
+template <class T>
+__global__ void k_build_rows(Lev L, CSplit<double> vx, CSplit<double> vy, CSplit<double> vz, CSplit<double> kf,
+                             CSplit<double> reac, int has_reac, double dtinv, int flux, ROp<T> out_rows)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned nx = L.nx, ny = L.ny;
+    if (t >= nx * ny * (unsigned)L.nz) return;
+    int k = t / (nx * ny);
+    unsigned rem = t - k * nx * ny;
+    int j = rem / nx;
+    int i = rem - j * nx;
+    const CSplit<double>* V[3] = {&vx, &vy, &vz};
+    const double kc = kf.get(L, i, j, k);
+    double d = 0.0;
+    double co[6] = {0, 0, 0, 0, 0, 0};
+    for (int ax = 0; ax < 3; ax++) {
+        const int p = ax == 0 ? i : (ax == 1 ? j : k);
+        const double wc = cwidth(L, ax, p);
+        const double vc = V[ax]->get(L, i, j, k);
+        // a face between cells of widths wa, wb: centre distance (wa+wb)/2, flux
+        // per unit area F = wL*u_L + wR*u_R; row L gains +F/w_L, row R -F/w_R
+        // minus face (neighbour is the left state)
+        {
+            int a = i, b = j, c = k;
+            if (nbr(L, ax, -1, a, b, c)) {
+                const int q = ax == 0 ? a : (ax == 1 ? b : c);
+                const double wn = cwidth(L, ax, q), dd = 0.5 * (wc + wn);
+                double wL, wR;
+                const double vn = V[ax]->get(L, a, b, c), kn = kf.get(L, a, b, c);
+                if (flux == 1) sg_face(vn, vc, kn, kc, dd, wL, wR);
+                else upwind_face(vn, vc, kn, kc, dd, wL, wR);
+                d -= wR * (1.0 / wc);
+                co[2 * ax] = -wL * (1.0 / wc);
+            } else {
+                const int code = L.bc[2 * ax];
+                if (code == BC_DIRC) {
+                    if (flux == 1) { double wL, wR; sg_face(vc, vc, kc, kc, 0.5 * wc, wL, wR); d -= wR / wc; }
+                    else { d += 2.0 * kc / (wc * wc); if (vc < 0.0) d -= vc / wc; }
+                } else if (code == BC_ZGRD) {
+                    d -= vc / wc;
+                }
+            }
+        }
+        // plus face (this cell is the left state)
+        {
+            int a = i, b = j, c = k;
+            if (nbr(L, ax, 1, a, b, c)) {
+                const int q = ax == 0 ? a : (ax == 1 ? b : c);
+                const double wn = cwidth(L, ax, q), dd = 0.5 * (wc + wn);
+                double wL, wR;
+                const double vn = V[ax]->get(L, a, b, c), kn = kf.get(L, a, b, c);
+                if (flux == 1) sg_face(vc, vn, kc, kn, dd, wL, wR);
+                else upwind_face(vc, vn, kc, kn, dd, wL, wR);
+                d += wL * (1.0 / wc);
+                co[2 * ax + 1] = wR * (1.0 / wc);
+            } else {
+                const int code = L.bc[2 * ax + 1];
+                if (code == BC_DIRC) {
+                    if (flux == 1) { double wL, wR; sg_face(vc, vc, kc, kc, 0.5 * wc, wL, wR); d += wL / wc; }
+                    else { d += 2.0 * kc / (wc * wc); if (vc > 0.0) d += vc / wc; }
+                } else if (code == BC_ZGRD) {
+                    d += vc / wc;
+                }
+            }
+        }
+    }
+    d = d - (has_reac ? reac.get(L, i, j, k) : 0.0) + dtinv;
+    const int cc = scol(i, j, k);
+    const long long o = soff(L, i, j, k);
+    ((T*)out_rows.r[0][cc])[o] = (T)d;
+    for (int q = 0; q < 6; q++) ((T*)out_rows.r[1 + q][cc])[o] = (T)co[q];
+}
+
+template <class T>
+__global__ void k_transpose_rows(Lev L, ROp<T> in, ROp<T> out)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned nx = L.nx, ny = L.ny;
+    if (t >= nx * ny * (unsigned)L.nz) return;
+    int k = t / (nx * ny);
+    unsigned rem = t - k * nx * ny;
+    int j = rem / nx;
+    int i = rem - j * nx;
+    const int cc = scol(i, j, k);
+    const long long o = soff(L, i, j, k);
+    ((T*)out.r[0][cc])[o] = in.r[0][cc][o];
+    for (int ax = 0; ax < 3; ax++)
+        for (int s = -1; s <= 1; s += 2) {
+            // coefficient of u_{c+s} in row c of A^T = coefficient of u_c in row c+s of A
+            int a = i, b = j, c = k;
+            T v = T(0);
+            if (nbr(L, ax, s, a, b, c)) {
+                const int q = 1 + 2 * ax + (s > 0 ? 0 : 1);  // opposite direction of s
+                v = in.r[q][scol(a, b, c)][soff(L, a, b, c)];
+            }
+            ((T*)out.r[1 + 2 * ax + (s > 0)][cc])[o] = v;
+        }
+}
+
+template <class T>
+__global__ void k_cast_field(long long n, const double* __restrict__ in, T* __restrict__ out, double scale,
+                             double shift)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = (T)((in ? in[t] : 0.0) * scale + shift);
+}
+
+template <class A, class B>
+__global__ void k_axpy(long long n, double a, const A* __restrict__ x, B* __restrict__ y)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        y[t] = (B)((double)y[t] + a * (double)x[t]);
+}
+
+}  // namespace mps

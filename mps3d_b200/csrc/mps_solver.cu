@@ -1,0 +1,1263 @@
+// mps_solver.cu -- host driver and C ABI of the B200 multigrid / Krylov
+// solver.  One handle = one CUDA stream + a device workspace reused across
+// calls with the same grid signature.
+//
+// Solve structure (correction scheme; equivalent to the reference's FAS
+// V-cycle, mgridlib/mgridsteps.f90:384-579, because the operator is linear):
+//   V(l): nu1 red-black GS sweeps; f_{l+1} = R(f_l - A_l u_l) (fused);
+//         u_{l+1} = 0; V(l+1); u_l += P u_{l+1}; nu2 sweeps.
+//   coarsest: u = A^{-1} f with a precomputed dense inverse.
+// Outer loops: FP64 stationary V-cycle iteration; MIXED = FP64 residual +
+// FP32 V-cycles + FP64 update (defect correction); FGMRES(m) right
+// preconditioned by the V-cycle with FP64 Gram-Schmidt and Givens.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mps_linsolve.h"
+#include "mps_kernels.cuh"
+
+namespace mps {
+
+constexpr int MAXL = 24;
+constexpr int MAX_DENSE = 1024;
+
+static inline unsigned nblk(long long n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+struct Err {
+    int code = 0;
+    std::string msg;
+};
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            ctx.err.code = MPS_ERR_CUDA;                                                           \
+            ctx.err.msg = std::string(#call) + ": " + cudaGetErrorString(e_);                     \
+            return MPS_ERR_CUDA;                                                                   \
+        }                                                                                          \
+    } while (0)
+#define CKL()                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess) {                                                                   \
+            ctx.err.code = MPS_ERR_CUDA;                                                           \
+            ctx.err.msg = std::string("launch at ") + __FILE__ + ":" + std::to_string(__LINE__) +   \
+                          ": " + cudaGetErrorString(e_);                                           \
+            return MPS_ERR_CUDA;                                                                   \
+        }                                                                                          \
+    } while (0)
+
+struct Arena {
+    std::vector<void*> blocks;
+    size_t bytes = 0;
+    void* get(size_t n)
+    {
+        void* p = nullptr;
+        if (n == 0) n = 16;
+        if (cudaMalloc(&p, n) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, n) != cudaSuccess) { cudaFree(p); return nullptr; }
+        blocks.push_back(p);
+        bytes += n;
+        return p;
+    }
+    void clear()
+    {
+        for (void* p : blocks) cudaFree(p);
+        blocks.clear();
+        bytes = 0;
+    }
+};
+
+template <class T>
+struct Hier {
+    T* U[MAXL][2] = {};  // two full split buffers (2*half) per level
+    T* F[MAXL] = {};     // right-hand side (split)
+    int ri[MAXL] = {}, bi[MAXL] = {};
+    KOp<T> kop[MAXL];
+    ROp<T> rop[MAXL];
+    double* AinvT = nullptr;
+};
+
+struct Signature {
+    int dims[3] = {0, 0, 0};
+    int bc[6] = {0, 0, 0, 0, 0, 0};
+    int hier = -1, ranks[3] = {0, 0, 0}, max_coarse = 0, opclass = -1, prec = -1, krylov = -1, restart = 0;
+    int has_reac = -1, kuni = -1, transpose = -1;
+    bool operator==(const Signature& o) const { return std::memcmp(this, &o, sizeof(Signature)) == 0; }
+};
+
+struct Ctx {
+    int dev = 0;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Err err;
+    Arena ar;       // grid-dependent workspace
+    Arena inbuf;    // host-API staging of the inputs
+    size_t inbuf_bytes = 0;
+    Signature sig;
+    int nlev = 0;
+    Lev lev[MAXL];
+    Xfer xf[MAXL];
+    // FP64 coefficient pyramid (split cell fields)
+    double* pk[MAXL] = {};
+    double* preac[MAXL] = {};
+    double* pv[3][MAXL] = {};
+    double* dex64[MAXL] = {};
+    float* k32[MAXL] = {};
+    float* dex32[MAXL] = {};
+    double* rows64[MAXL] = {};
+    float* rows32[MAXL] = {};
+    Hier<double> h64;
+    Hier<float> h32;
+    double* x64 = nullptr;  // outer iterate (mixed / fgmres)
+    double* b64 = nullptr;
+    KOp<double> kop64;      // fine-level FP64 operator for outer residuals
+    ROp<double> rop64;
+    double* dense = nullptr;
+    double* gjM = nullptr;
+    int* dstatus = nullptr;
+    RedBuf rb;
+    unsigned long long* dmax = nullptr;
+    double* hpin = nullptr;  // pinned host scratch
+    // FGMRES
+    double* V = nullptr;
+    void* Z = nullptr;
+    double* w = nullptr;
+    double* hcol = nullptr;
+    double** Vptr = nullptr;
+    double* dpart = nullptr;
+    int mdot_blocks = 0;
+    double* zero_face = nullptr;
+    size_t zero_face_n = 0;
+};
+
+}  // namespace mps
+
+struct mps_handle_s {
+    mps::Ctx ctx;
+};
+
+namespace mps {
+
+// ----------------------------------------------------------------------
+static Lev make_lev(int nx, int ny, int nz, const double w[3], const double wl[3], const int bc[6])
+{
+    Lev L;
+    std::memset(&L, 0, sizeof(L));
+    L.nx = nx; L.ny = ny; L.nz = nz;
+    L.nh = (nx + 1) / 2;
+    L.P = ((L.nh + 7) / 8) * 8;
+    L.half = (long long)L.P * ny * nz;
+    for (int f = 0; f < 6; f++) L.bc[f] = bc[f];
+    for (int a = 0; a < 3; a++) L.per[a] = bc[2 * a] == BC_PERI;
+    const int n[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; a++) {
+        const double ww = w[a], wwl = wl[a];
+        L.w[a] = ww;
+        L.wl[a] = wwl;
+        const double dl = 0.5 * (ww + wwl);
+        L.cr[a] = 1.0 / (ww * ww);
+        L.cl[a] = n[a] == 1 ? 1.0 / (wwl * wwl) : 1.0 / (dl * wwl);
+        L.cp[a] = 1.0 / (dl * ww);
+        L.dr[a] = 2.0 / (ww * ww);
+        L.dlast[a] = 2.0 / (wwl * wwl);
+    }
+    L.divP.init((unsigned)L.P);
+    L.divNy.init((unsigned)ny);
+    L.rows = (unsigned)ny * (unsigned)nz;
+    return L;
+}
+
+static Lev make_lev_uniform(int nx, int ny, int nz, const double llen[3], const int bc[6])
+{
+    const double w[3] = {llen[0] / nx, llen[1] / ny, llen[2] / nz};
+    return make_lev(nx, ny, nz, w, w, bc);
+}
+
+// level sizes and cell widths.  CELL = the reference (l/2 by integer division,
+// mgridsteps.f90:21-23; dx = llen/l on every level, find_AX :724-726; coarsest
+// when a per-rank size reaches LMIN=1, :512).  GEOM = l/2 with the odd cell of
+// an odd size merged into the last coarse cell and exact widths; coarsest when
+// a level has at most max_coarse cells.
+static int plan_levels(const mps_grid* g, const mps_solver_opts* o, const int bc[6], Lev* lev, Xfer* xf,
+                       std::string& why)
+{
+    int d[3] = {g->lx, g->ly, g->lz};
+    const double llen[3] = {g->llenx, g->lleny, g->llenz};
+    double w[3], wl[3];
+    for (int a = 0; a < 3; a++) w[a] = wl[a] = llen[a] / d[a];
+    int n = 0;
+    const int* P = o->ranks;
+    const bool cell = o->hierarchy == MPS_HIER_CELL;
+    if (cell) {
+        for (int a = 0; a < 3; a++)
+            if (P[a] < 1 || d[a] % P[a] != 0) { why = "CELL hierarchy: size not divisible by ranks"; return -1; }
+    }
+    for (;;) {
+        lev[n] = make_lev(d[0], d[1], d[2], w, wl, bc);
+        long long cells = (long long)d[0] * d[1] * d[2];
+        bool coarsest;
+        if (cell)
+            coarsest = d[0] / P[0] <= 1 || d[1] / P[1] <= 1 || d[2] / P[2] <= 1;
+        else
+            coarsest = cells <= o->max_coarse || (d[0] == 1 && d[1] == 1 && d[2] == 1);
+        if (coarsest || n == MAXL - 1) {
+            if (!coarsest) { why = "too many levels"; return -1; }
+            if (cells > MAX_DENSE) { why = "coarsest level too large for the dense solve"; return -1; }
+            return n + 1;
+        }
+        int c[3];
+        double cw[3], cwl[3];
+        Xfer X;
+        std::memset(&X, 0, sizeof(X));
+        X.geom = !cell;
+        for (int a = 0; a < 3; a++) {
+            if (cell) {
+                int l = d[a] / P[a];
+                if ((l & 1) && P[a] > 1) { why = "CELL hierarchy: odd per-rank size with several ranks"; return -1; }
+                c[a] = P[a] * (l / 2);
+                cw[a] = cwl[a] = llen[a] / c[a];
+            } else if (d[a] == 1) {
+                c[a] = 1;
+                cw[a] = cwl[a] = wl[a];
+            } else {
+                c[a] = d[a] / 2;
+                cw[a] = 2.0 * w[a];
+                cwl[a] = (d[a] & 1) ? 2.0 * w[a] + wl[a] : w[a] + wl[a];
+                if (c[a] == 1) cw[a] = cwl[a];
+            }
+            X.nf[a] = d[a];
+            X.nc[a] = c[a];
+            X.rf[a] = wl[a] / w[a];
+            X.Rc[a] = cwl[a] / w[a];
+            X.per[a] = bc[2 * a] == BC_PERI;
+        }
+        xf[n] = X;
+        for (int a = 0; a < 3; a++) { d[a] = c[a]; w[a] = cw[a]; wl[a] = cwl[a]; }
+        n++;
+    }
+}
+
+template <class T>
+static Split<T> cur(Hier<T>& H, const Lev& L, int l)
+{
+    Split<T> s;
+    s.c[0] = H.U[l][H.ri[l]];
+    s.c[1] = H.U[l][H.bi[l]] + L.half;
+    return s;
+}
+template <class T>
+static CSplit<T> ccur(Hier<T>& H, const Lev& L, int l)
+{
+    CSplit<T> s;
+    s.c[0] = H.U[l][H.ri[l]];
+    s.c[1] = H.U[l][H.bi[l]] + L.half;
+    return s;
+}
+template <class T>
+static CSplit<T> csplit(const T* base, const Lev& L)
+{
+    CSplit<T> s;
+    s.c[0] = base;
+    s.c[1] = base + L.half;
+    return s;
+}
+template <class T>
+static Split<T> split(T* base, const Lev& L)
+{
+    Split<T> s;
+    s.c[0] = base;
+    s.c[1] = base + L.half;
+    return s;
+}
+
+// ---- one colour pass ----
+template <class T, class Op>
+static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zero_state)
+{
+    const Lev& L = ctx.lev[l];
+    const unsigned nb = nblk((long long)L.P * L.rows);
+    T* out;
+    const T* fh = H.F[l] + (c ? L.half : 0);
+    if (c == 0) out = H.U[l][H.ri[l] ^ 1];
+    else out = H.U[l][H.bi[l] ^ 1] + L.half;
+    if (zero_state == 2) {  // whole state zero
+        k_colour<T, Op, ZeroU<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh);
+    } else if (zero_state == 1) {  // colour c zero, other colour valid
+        OtherOnlyU<T> u;
+        u.c = c;
+        u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
+        k_colour<T, Op, OtherOnlyU<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, u, out, fh);
+    } else {
+        k_colour<T, Op, CSplit<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, ccur(H, L, l), out, fh);
+    }
+    CKL();
+    if (c == 0) H.ri[l] ^= 1;
+    else H.bi[l] ^= 1;
+    return 0;
+}
+
+template <class T>
+static int coarse_solve(Ctx& ctx, Hier<T>& H, int l)
+{
+    const Lev& L = ctx.lev[l];
+    const int n = L.nx * L.ny * L.nz;
+    k_coarse_solve<T><<<1, 512, n * sizeof(double), ctx.s>>>(L, H.AinvT, csplit<T>(H.F[l], L), cur(H, L, l));
+    CKL();
+    return 0;
+}
+
+template <class T, class Op>
+static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solver_opts* o, bool zero_guess)
+{
+    if (l == ctx.nlev - 1) return coarse_solve(ctx, H, l);
+    const Lev& L = ctx.lev[l];
+    const Lev& C = ctx.lev[l + 1];
+    int st;
+    for (int s = 0; s < o->nu1; s++) {
+        bool z = zero_guess && s == 0;
+        if ((st = colour_pass(ctx, H, ops[l], l, 0, z ? 2 : 0))) return st;
+        if ((st = colour_pass(ctx, H, ops[l], l, 1, z ? 1 : 0))) return st;
+    }
+    if (o->nu1 == 0 && zero_guess) {
+        // no pre-smoothing from a zero guess: materialise the zero state
+        CK(cudaMemsetAsync(H.U[l][H.ri[l]], 0, sizeof(T) * L.half, ctx.s));
+        CK(cudaMemsetAsync(H.U[l][H.bi[l]] + L.half, 0, sizeof(T) * L.half, ctx.s));
+    }
+    k_resid_restrict<T, Op><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
+        L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom);
+    CKL();
+    if ((st = vcycle_rec(ctx, H, ops, l + 1, o, true))) return st;
+    k_prolong_correct<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
+        L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l]);
+    CKL();
+    for (int s = 0; s < o->nu2; s++) {
+        if ((st = colour_pass(ctx, H, ops[l], l, 0, 0))) return st;
+        if ((st = colour_pass(ctx, H, ops[l], l, 1, 0))) return st;
+    }
+    return 0;
+}
+
+template <class T>
+static int vcycle(Ctx& ctx, Hier<T>& H, int opclass, const mps_solver_opts* o, bool zero_guess)
+{
+    if (opclass == 0) return vcycle_rec(ctx, H, H.kop, 0, o, zero_guess);
+    return vcycle_rec(ctx, H, H.rop, 0, o, zero_guess);
+}
+
+// r = f - A u, sums (r.r, f.f) -> ctx.rb.out; optional r written to rout (type R)
+template <class T, class Op, class R>
+static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R> rout)
+{
+    const Lev& L = ctx.lev[0];
+    k_resid_norm<T, Op, R><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, op, u, f, rout, ctx.rb);
+    CKL();
+    return 0;
+}
+
+static int fetch(Ctx& ctx, const double* dsrc, int n)
+{
+    CK(cudaMemcpyAsync(ctx.hpin, dsrc, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx.s));
+    CK(cudaStreamSynchronize(ctx.s));
+    return 0;
+}
+
+// ----------------------------------------------------------------------
+struct Inputs {  // device pointers (ghosted Fortran-order fields)
+    const double* vel;
+    const double* dcoeff;
+    const double* reac;
+    const double* source;
+    const double* bcval[6];
+    const double* sterm;
+    double* soln;
+};
+
+template <class T>
+static void alloc_hier(Ctx& ctx, Hier<T>& H, bool& ok)
+{
+    for (int l = 0; l < ctx.nlev; l++) {
+        const Lev& L = ctx.lev[l];
+        size_t b = sizeof(T) * 2 * L.half;
+        H.U[l][0] = (T*)ctx.ar.get(b);
+        H.U[l][1] = (T*)ctx.ar.get(b);
+        H.F[l] = (T*)ctx.ar.get(b);
+        H.ri[l] = H.bi[l] = 0;
+        ok = ok && H.U[l][0] && H.U[l][1] && H.F[l];
+    }
+    const Lev& C = ctx.lev[ctx.nlev - 1];
+    const long long n = (long long)C.nx * C.ny * C.nz;
+    H.AinvT = (double*)ctx.ar.get(sizeof(double) * n * n);
+    ok = ok && H.AinvT;
+}
+
+static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts* o, int need64, int need32)
+{
+    if (sig == ctx.sig) return 0;
+    ctx.ar.clear();
+    ctx.sig = Signature();
+    bool ok = true;
+    const int nl = ctx.nlev;
+    for (int l = 0; l < nl; l++) {
+        const Lev& L = ctx.lev[l];
+        const size_t b64 = sizeof(double) * 2 * L.half, b32 = sizeof(float) * 2 * L.half;
+        ctx.pk[l] = (double*)ctx.ar.get(b64);
+        ctx.preac[l] = sig.has_reac ? (double*)ctx.ar.get(b64) : nullptr;
+        ctx.dex64[l] = sig.has_reac ? (double*)ctx.ar.get(b64) : nullptr;
+        for (int a = 0; a < 3; a++) ctx.pv[a][l] = sig.opclass == 1 ? (double*)ctx.ar.get(b64) : nullptr;
+        ok = ok && ctx.pk[l];
+        if (sig.opclass == 1) {
+            ctx.rows64[l] = (need64 || l == 0) ? (double*)ctx.ar.get(7 * b64) : nullptr;
+            ctx.rows32[l] = need32 ? (float*)ctx.ar.get(7 * b32) : nullptr;
+        } else {
+            ctx.k32[l] = (need32 && !sig.kuni) ? (float*)ctx.ar.get(b32) : nullptr;
+            ctx.dex32[l] = (need32 && sig.has_reac) ? (float*)ctx.ar.get(b32) : nullptr;
+        }
+    }
+    if (need64) alloc_hier(ctx, ctx.h64, ok);
+    if (need32) alloc_hier(ctx, ctx.h32, ok);
+    const Lev& L0 = ctx.lev[0];
+    ctx.x64 = (double*)ctx.ar.get(sizeof(double) * 2 * L0.half);
+    ctx.b64 = (double*)ctx.ar.get(sizeof(double) * 2 * L0.half);
+    const Lev& C = ctx.lev[nl - 1];
+    const long long nc = (long long)C.nx * C.ny * C.nz;
+    ctx.dense = (double*)ctx.ar.get(sizeof(double) * nc * nc);
+    ctx.gjM = (double*)ctx.ar.get(sizeof(double) * nc * nc * 2);
+    ctx.dstatus = (int*)ctx.ar.get(sizeof(int) * 4);
+    const unsigned maxb = nblk((long long)L0.P * L0.rows);
+    ctx.rb.partial = (double*)ctx.ar.get(sizeof(double) * 2 * (maxb + 1));
+    ctx.rb.counter = (unsigned*)ctx.ar.get(sizeof(unsigned) * 4);
+    ctx.rb.out = (double*)ctx.ar.get(sizeof(double) * 4);
+    if (sig.krylov == MPS_KRYLOV_FGMRES) {
+        const int m = sig.restart;
+        const size_t n = 2 * L0.half;
+        ctx.V = (double*)ctx.ar.get(sizeof(double) * n * (m + 1));
+        ctx.Z = ctx.ar.get((need32 ? sizeof(float) : sizeof(double)) * n * m);
+        ctx.w = (double*)ctx.ar.get(sizeof(double) * n);
+        ctx.hcol = (double*)ctx.ar.get(sizeof(double) * 2 * (m + 2));
+        ctx.Vptr = (double**)ctx.ar.get(sizeof(double*) * (m + 2));
+        ctx.mdot_blocks = 592;
+        ctx.dpart = (double*)ctx.ar.get(sizeof(double) * (m + 2) * ctx.mdot_blocks);
+        ok = ok && ctx.V && ctx.Z && ctx.w && ctx.hcol && ctx.Vptr && ctx.dpart;
+        if (ok) {
+            std::vector<double*> hp(m + 2);
+            for (int j = 0; j <= m; j++) hp[j] = ctx.V + (size_t)j * n;
+            hp[m + 1] = ctx.w;
+            if (cudaMemcpy(ctx.Vptr, hp.data(), sizeof(double*) * (m + 2), cudaMemcpyHostToDevice) != cudaSuccess)
+                ok = false;
+        }
+    }
+    ok = ok && ctx.x64 && ctx.b64 && ctx.dense && ctx.gjM && ctx.dstatus && ctx.rb.partial && ctx.rb.counter &&
+         ctx.rb.out;
+    if (!ok) {
+        ctx.ar.clear();
+        ctx.err.code = MPS_ERR_NOMEM;
+        ctx.err.msg = "device allocation failed";
+        return MPS_ERR_NOMEM;
+    }
+    ctx.sig = sig;
+    return 0;
+}
+
+template <class T>
+static void set_kop(Ctx& ctx, KOp<T>* ops, T* const* kT, T* const* dexT, double kc, double dtinv, bool kuni,
+                    bool has_reac)
+{
+    for (int l = 0; l < ctx.nlev; l++) {
+        const Lev& L = ctx.lev[l];
+        KOp<T> op;
+        if (kuni) { op.k[0] = op.k[1] = nullptr; op.kc = (T)kc; }
+        else { op.k[0] = kT[l]; op.k[1] = kT[l] + L.half; op.kc = T(0); }
+        if (has_reac) { op.dex[0] = dexT[l]; op.dex[1] = dexT[l] + L.half; op.dexc = T(0); }
+        else { op.dex[0] = op.dex[1] = nullptr; op.dexc = (T)dtinv; }
+        ops[l] = op;
+    }
+}
+template <class T>
+static ROp<T> make_rop(T* rows, const Lev& L)
+{
+    ROp<T> r;
+    for (int q = 0; q < 7; q++) {
+        r.r[q][0] = rows + (size_t)q * 2 * L.half;
+        r.r[q][1] = rows + (size_t)q * 2 * L.half + L.half;
+    }
+    return r;
+}
+
+template <class T>
+static int build_rows_level(Ctx& ctx, int l, T* rows, double dtinv, int flux, int transpose, T* tmp)
+{
+    const Lev& L = ctx.lev[l];
+    const double* z = ctx.pk[l];  // any valid pointer for unused fields
+    auto cs = [&](const double* p) { return csplit<double>(p ? p : z, L); };
+    T* dst = transpose ? tmp : rows;
+    k_build_rows<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
+        L, cs(ctx.pv[0][l]), cs(ctx.pv[1][l]), cs(ctx.pv[2][l]), cs(ctx.pk[l]), cs(ctx.preac[l]),
+        ctx.preac[l] != nullptr, dtinv, flux, make_rop<T>(dst, L));
+    CKL();
+    if (transpose) {
+        k_transpose_rows<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(L, make_rop<T>(tmp, L),
+                                                                                   make_rop<T>(rows, L));
+        CKL();
+    }
+    return 0;
+}
+
+template <class T, class Op>
+static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
+{
+    const int l = ctx.nlev - 1;
+    const Lev& L = ctx.lev[l];
+    const int n = L.nx * L.ny * L.nz;
+    CK(cudaMemsetAsync(ctx.dense, 0, sizeof(double) * n * n, ctx.s));
+    k_dense_assemble<T, Op><<<nblk(n), TPB, 0, ctx.s>>>(L, op, ctx.dense);
+    CKL();
+    k_gj_prepare<<<nblk(2LL * n * n), TPB, 0, ctx.s>>>(n, ctx.dense, ctx.gjM);
+    CKL();
+    k_gauss_jordan<<<1, 1024, 0, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus);
+    CKL();
+    return 0;
+}
+
+// ----------------------------------------------------------------------
+static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, const Inputs& in, const int bc[6],
+                      const mps_solver_opts* o, mps_solve_info* info, int ref_norm_only)
+{
+    mps_solve_info inf;
+    std::memset(&inf, 0, sizeof(inf));
+    inf.status = MPS_OK;
+    // ---- argument checks ----
+    if (!g || g->lx < 1 || g->ly < 1 || g->lz < 1 || !(g->llenx > 0) || !(g->lleny > 0) || !(g->llenz > 0) ||
+        !in.dcoeff || !in.source || !in.soln) {
+        ctx.err.msg = "bad grid or null field";
+        return MPS_ERR_BAD_ARG;
+    }
+    if ((long long)g->lx * g->ly * g->lz >= (1LL << 31) / 2) { ctx.err.msg = "grid too large"; return MPS_ERR_BAD_ARG; }
+    for (int f = 0; f < 6; f++)
+        if (bc[f] < 1 || bc[f] > 5) { ctx.err.msg = "bad BC code"; return MPS_ERR_BAD_ARG; }
+    for (int a = 0; a < 3; a++)
+        if ((bc[2 * a] == BC_PERI) != (bc[2 * a + 1] == BC_PERI)) {
+            ctx.err.msg = "PERI must be set on both faces of a direction";
+            return MPS_ERR_BAD_ARG;
+        }
+    if (timederiv && !(dt > 0)) { ctx.err.msg = "dt must be positive"; return MPS_ERR_BAD_ARG; }
+    if (o->nu1 < 0 || o->nu2 < 0 || o->maxit < 0 || o->restart < 1 || o->restart > 250 || o->max_coarse < 1 ||
+        o->max_coarse > MAX_DENSE) {
+        ctx.err.msg = "bad solver option";
+        return MPS_ERR_BAD_ARG;
+    }
+    for (int f = 0; f < 6; f++)
+        if (!in.bcval[f] && (bc[f] == BC_DIRC || bc[f] == BC_FLUX)) {
+            ctx.err.msg = "missing boundary values for a DIRC/FLUX face";
+            return MPS_ERR_BAD_ARG;
+        }
+    std::string why;
+    int nl = plan_levels(g, o, bc, ctx.lev, ctx.xf, why);
+    if (nl < 1) { ctx.err.msg = why; return MPS_ERR_BAD_ARG; }
+    ctx.nlev = nl;
+    const Lev& L0 = ctx.lev[0];
+    const double dtinv = timederiv ? 1.0 / dt : 0.0;
+
+    CK(cudaEventRecord(ctx.e0, ctx.s));
+    // ---- operator detection (one small device->host read) ----
+    unsigned long long* dm = ctx.dmax;
+    CK(cudaMemsetAsync(dm, 0, sizeof(unsigned long long) * 8, ctx.s));
+    const long long ncell = (long long)L0.nx * L0.ny * L0.nz;
+    const long long ng = (long long)(L0.nx + 2) * (L0.ny + 2) * (L0.nz + 2);
+    const unsigned mb = std::min<unsigned>(nblk(ncell), 1184);
+    if (in.vel)
+        for (int a = 0; a < 3; a++) { k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.vel + a * ng, 0, dm + 0); CKL(); }
+    if (in.reac) { k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.reac, 0, dm + 1); CKL(); }
+    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.dcoeff, 1, dm + 2);
+    CKL();
+    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.source, 0, dm + 3);
+    CKL();
+    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.soln, 0, dm + 4);
+    CKL();
+    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.dcoeff, 0, dm + 5);
+    CKL();
+    unsigned long long hm[8];
+    CK(cudaMemcpyAsync(hm, dm, sizeof(hm), cudaMemcpyDeviceToHost, ctx.s));
+    double k0 = 0.0;
+    CK(cudaMemcpyAsync(&k0, in.dcoeff + 1 + (L0.nx + 2) * (1 + (long long)(L0.ny + 2)), sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx.s));
+    CK(cudaStreamSynchronize(ctx.s));
+    auto asd = [](unsigned long long b) { double d; std::memcpy(&d, &b, 8); return d; };
+    const double maxvel = asd(hm[0]), maxreac = asd(hm[1]), dkvar = asd(hm[2]), maxsrc = asd(hm[3]),
+                 maxsol = asd(hm[4]), maxk = asd(hm[5]);
+    if (!(maxvel <= 1e308) || !(maxreac <= 1e308) || !(dkvar <= 1e308) || !(maxsrc <= 1e308) ||
+        !(maxsol <= 1e308) || !(maxk <= 1e308)) {
+        ctx.err.msg = "NaN or Inf in the inputs";
+        inf.status = MPS_ERR_NAN;
+        if (info) *info = inf;
+        return MPS_ERR_NAN;
+    }
+    Signature sig;
+    sig.dims[0] = g->lx; sig.dims[1] = g->ly; sig.dims[2] = g->lz;
+    for (int f = 0; f < 6; f++) sig.bc[f] = bc[f];
+    sig.hier = o->hierarchy;
+    for (int a = 0; a < 3; a++) sig.ranks[a] = o->hierarchy == MPS_HIER_CELL ? o->ranks[a] : 0;
+    sig.max_coarse = o->hierarchy == MPS_HIER_GEOM ? o->max_coarse : 0;
+    sig.opclass = (o->transpose == 0 && o->flux == MPS_FLUX_UPWIND && maxvel == 0.0) ? 0 : 1;
+    if (o->flux == MPS_FLUX_UPWIND && maxvel == 0.0) sig.opclass = 0;  // symmetric: A^T = A
+    sig.prec = o->precision;
+    sig.krylov = o->krylov;
+    sig.restart = o->krylov == MPS_KRYLOV_FGMRES ? o->restart : 0;
+    sig.has_reac = maxreac > 0.0;
+    sig.kuni = dkvar == 0.0;
+    sig.transpose = o->transpose && sig.opclass == 1;
+    const bool mixed = o->precision == MPS_PREC_MIXED;
+    const int need64 = !mixed, need32 = mixed;
+    int st = setup_workspace(ctx, sig, o, need64, need32);
+    if (st) return st;
+
+    // ---- coefficient pyramid (FP64) ----
+    k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.dcoeff, split<double>(ctx.pk[0], L0), 1.0, 0.0);
+    CKL();
+    if (sig.has_reac) {
+        k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.reac, split<double>(ctx.preac[0], L0), 1.0, 0.0);
+        CKL();
+    }
+    if (sig.opclass == 1)
+        for (int a = 0; a < 3; a++) {
+            k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.vel ? in.vel + a * ng : nullptr,
+                                                           split<double>(ctx.pv[a][0], L0), 1.0, 0.0);
+            CKL();
+        }
+    for (int l = 0; l + 1 < nl; l++) {
+        const Lev& F = ctx.lev[l];
+        const Lev& C = ctx.lev[l + 1];
+        const unsigned nb = nblk((long long)C.nx * C.ny * C.nz);
+        const int geom = ctx.xf[l].geom;
+        k_restrict_field<<<nb, TPB, 0, ctx.s>>>(F, csplit<double>(ctx.pk[l], F), C, split<double>(ctx.pk[l + 1], C),
+                                                geom);
+        CKL();
+        if (sig.has_reac) {
+            k_restrict_field<<<nb, TPB, 0, ctx.s>>>(F, csplit<double>(ctx.preac[l], F), C,
+                                                    split<double>(ctx.preac[l + 1], C), geom);
+            CKL();
+        }
+        if (sig.opclass == 1)
+            for (int a = 0; a < 3; a++) {
+                k_restrict_field<<<nb, TPB, 0, ctx.s>>>(F, csplit<double>(ctx.pv[a][l], F), C,
+                                                        split<double>(ctx.pv[a][l + 1], C), geom);
+                CKL();
+            }
+    }
+    // ---- operators ----
+    if (sig.opclass == 0) {
+        for (int l = 0; l < nl; l++) {
+            const long long n2 = 2 * ctx.lev[l].half;
+            if (sig.has_reac) {
+                k_cast_field<double><<<std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s>>>(n2, ctx.preac[l], ctx.dex64[l], -1.0, dtinv);
+                CKL();
+            }
+            if (need32) {
+                if (!sig.kuni) {
+                    k_cast_field<float><<<std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s>>>(n2, ctx.pk[l], ctx.k32[l], 1.0, 0.0);
+                    CKL();
+                }
+                if (sig.has_reac) {
+                    k_cast_field<float><<<std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s>>>(n2, ctx.preac[l], ctx.dex32[l], -1.0, dtinv);
+                    CKL();
+                }
+            }
+        }
+        KOp<double> k64[MAXL];
+        set_kop<double>(ctx, k64, ctx.pk, ctx.dex64, k0, dtinv, sig.kuni, sig.has_reac);
+        ctx.kop64 = k64[0];
+        if (need64) std::copy(k64, k64 + nl, ctx.h64.kop);
+        if (need32) set_kop<float>(ctx, ctx.h32.kop, ctx.k32, ctx.dex32, k0, dtinv, sig.kuni, sig.has_reac);
+    } else {
+        for (int l = 0; l < nl; l++) {
+            if (ctx.rows64[l]) {
+                // transposed rows need a scratch copy of the forward rows: use rows32's
+                // FP64-sized neighbour (x64 is large enough only at level 0), so build into
+                // the FGMRES-free scratch: the dense matrix buffer is too small; allocate once
+                double* tmp = nullptr;
+                if (sig.transpose) {
+                    CK(cudaMallocAsync((void**)&tmp, sizeof(double) * 7 * 2 * ctx.lev[l].half, ctx.s));
+                }
+                if ((st = build_rows_level<double>(ctx, l, ctx.rows64[l], dtinv, o->flux, sig.transpose, tmp))) return st;
+                if (tmp) CK(cudaFreeAsync(tmp, ctx.s));
+                if (need64) ctx.h64.rop[l] = make_rop<double>(ctx.rows64[l], ctx.lev[l]);
+            }
+            if (ctx.rows32[l]) {
+                float* tmp = nullptr;
+                if (sig.transpose) {
+                    CK(cudaMallocAsync((void**)&tmp, sizeof(float) * 7 * 2 * ctx.lev[l].half, ctx.s));
+                }
+                if ((st = build_rows_level<float>(ctx, l, ctx.rows32[l], dtinv, o->flux, sig.transpose, tmp))) return st;
+                if (tmp) CK(cudaFreeAsync(tmp, ctx.s));
+                ctx.h32.rop[l] = make_rop<float>(ctx.rows32[l], ctx.lev[l]);
+            }
+        }
+        ctx.rop64 = make_rop<double>(ctx.rows64[0], L0);
+    }
+    // ---- right-hand side and initial guess ----
+    {
+        const double* bv[6];
+        for (int f = 0; f < 6; f++) bv[f] = in.bcval[f];
+        k_find_bvec<<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.vel, in.dcoeff, in.source, bv[0], bv[1], bv[2], bv[3],
+                                                    bv[4], bv[5], in.sterm, o->flux, split<double>(ctx.b64, L0));
+        CKL();
+        k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.soln, split<double>(ctx.x64, L0), 1.0, 0.0);
+        CKL();
+    }
+    // ---- coarsest inverse ----
+    CK(cudaMemsetAsync(ctx.dstatus, 0, sizeof(int) * 4, ctx.s));
+    if (need64) {
+        if (sig.opclass == 0) st = coarse_inverse(ctx, ctx.h64, ctx.h64.kop[nl - 1]);
+        else st = coarse_inverse(ctx, ctx.h64, ctx.h64.rop[nl - 1]);
+    } else {
+        if (sig.opclass == 0) st = coarse_inverse(ctx, ctx.h32, ctx.h32.kop[nl - 1]);
+        else st = coarse_inverse(ctx, ctx.h32, ctx.h32.rop[nl - 1]);
+    }
+    if (st) return st;
+
+    // ---- iterations ----
+    const Lev& L = L0;
+    const long long n2 = 2 * L.half;
+    double bnorm = 0.0, rel = 0.0, rms = 0.0;
+    int it = 0, vcycles = 0;
+    auto norms = [&](double rr, double ff) {
+        rel = ff > 0.0 ? std::sqrt(rr) / std::sqrt(ff) : std::sqrt(rr);
+        rms = std::sqrt(rr / (double)ncell);
+    };
+    auto conv = [&]() { return o->tol_kind == MPS_TOL_RMS_ABS ? rms <= o->tol : rel <= o->tol; };
+    Split<double> no64;
+    no64.c[0] = no64.c[1] = nullptr;
+
+    if (o->krylov == MPS_KRYLOV_NONE && !mixed) {
+        // FP64 stationary V-cycle iteration on h64 (x lives in level-0 U)
+        Hier<double>& H = ctx.h64;
+        CK(cudaMemcpyAsync(H.U[0][0], ctx.x64, sizeof(double) * n2, cudaMemcpyDeviceToDevice, ctx.s));
+        CK(cudaMemcpyAsync(H.F[0], ctx.b64, sizeof(double) * n2, cudaMemcpyDeviceToDevice, ctx.s));
+        H.ri[0] = H.bi[0] = 0;
+        for (;;) {
+            if (sig.opclass == 0) st = resid_norm(ctx, H.kop[0], ccur(H, L, 0), csplit<double>(H.F[0], L), no64);
+            else st = resid_norm(ctx, H.rop[0], ccur(H, L, 0), csplit<double>(H.F[0], L), no64);
+            if (st) return st;
+            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+            if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
+            norms(ctx.hpin[0], ctx.hpin[1]);
+            if (it == 0) inf.rel_res0 = rel;
+            if (ref_norm_only ? it >= o->maxit : (conv() || it >= o->maxit)) break;
+            if ((st = vcycle(ctx, H, sig.opclass, o, false))) return st;
+            vcycles++;
+            it++;
+        }
+        // copy the iterate back to x64 (split, both colours)
+        CK(cudaMemcpyAsync(ctx.x64, H.U[0][H.ri[0]], sizeof(double) * L.half, cudaMemcpyDeviceToDevice, ctx.s));
+        CK(cudaMemcpyAsync(ctx.x64 + L.half, H.U[0][H.bi[0]] + L.half, sizeof(double) * L.half,
+                           cudaMemcpyDeviceToDevice, ctx.s));
+    } else if (o->krylov == MPS_KRYLOV_NONE && mixed) {
+        // FP64 defect correction with FP32 V-cycles
+        Hier<float>& H = ctx.h32;
+        const int inner = o->inner_cycles > 0 ? o->inner_cycles : 2;
+        for (;;) {
+            Split<float> r32 = split<float>(H.F[0], L);
+            if (sig.opclass == 0)
+                st = resid_norm(ctx, ctx.kop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
+            else
+                st = resid_norm(ctx, ctx.rop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
+            if (st) return st;
+            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+            if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
+            norms(ctx.hpin[0], ctx.hpin[1]);
+            if (it == 0) inf.rel_res0 = rel;
+            if (conv() || it >= o->maxit) break;
+            for (int c = 0; c < inner; c++) {
+                if ((st = vcycle(ctx, H, sig.opclass, o, c == 0))) return st;
+                vcycles++;
+            }
+            const unsigned ab = std::min<unsigned>(nblk(L.half), 4736);
+            k_axpy<float, double><<<ab, TPB, 0, ctx.s>>>(L.half, 1.0, H.U[0][H.ri[0]], ctx.x64);
+            CKL();
+            k_axpy<float, double><<<ab, TPB, 0, ctx.s>>>(L.half, 1.0, H.U[0][H.bi[0]] + L.half, ctx.x64 + L.half);
+            CKL();
+            it++;
+        }
+    } else {
+        // FGMRES(m), right preconditioned by one V-cycle (FP32 when MIXED)
+        const int m = o->restart;
+        const long long n = n2;
+        const unsigned db = ctx.mdot_blocks;
+        std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), gq(m + 1), y(m);
+        auto HH = [&](int i, int j) -> double& { return H[(size_t)i + (size_t)(m + 1) * j]; };
+        for (;;) {
+            // w = b - A x, beta = ||w||
+            if (sig.opclass == 0)
+                st = resid_norm(ctx, ctx.kop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L),
+                                split<double>(ctx.w, L));
+            else
+                st = resid_norm(ctx, ctx.rop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L),
+                                split<double>(ctx.w, L));
+            if (st) return st;
+            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+            if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
+            norms(ctx.hpin[0], ctx.hpin[1]);
+            if (it == 0) { inf.rel_res0 = rel; bnorm = std::sqrt(ctx.hpin[1]); }
+            if (conv() || it >= o->maxit) break;
+            const double beta = std::sqrt(ctx.hpin[0]);
+            // v0 = w / beta
+            ctx.hpin[0] = beta;
+            CK(cudaMemcpyAsync(ctx.hcol, ctx.hpin, sizeof(double), cudaMemcpyHostToDevice, ctx.s));
+            k_scale_to<<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, ctx.w, ctx.hcol, 0, ctx.V, nullptr);
+            CKL();
+            std::fill(H.begin(), H.end(), 0.0);
+            std::fill(gq.begin(), gq.end(), 0.0);
+            gq[0] = beta;
+            int j = 0;
+            bool done = false;
+            for (j = 0; j < m && it < o->maxit; j++) {
+                double* vj = ctx.V + (size_t)j * n;
+                // z_j = M^{-1} v_j (one V-cycle from zero), then w = A z_j in FP64
+                if (mixed) {
+                    Hier<float>& P = ctx.h32;
+                    k_cast_field<float><<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, vj, P.F[0], 1.0, 0.0);
+                    CKL();
+                    if ((st = vcycle(ctx, P, sig.opclass, o, true))) return st;
+                    float* zj = (float*)ctx.Z + (size_t)j * n;
+                    CK(cudaMemcpyAsync(zj, P.U[0][P.ri[0]], sizeof(float) * L.half, cudaMemcpyDeviceToDevice, ctx.s));
+                    CK(cudaMemcpyAsync(zj + L.half, P.U[0][P.bi[0]] + L.half, sizeof(float) * L.half,
+                                       cudaMemcpyDeviceToDevice, ctx.s));
+                    if (sig.opclass == 0)
+                        k_apply<double, KOp<double>, float><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                            L, ctx.kop64, csplit<float>(zj, L), split<double>(ctx.w, L));
+                    else
+                        k_apply<double, ROp<double>, float><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                            L, ctx.rop64, csplit<float>(zj, L), split<double>(ctx.w, L));
+                    CKL();
+                } else {
+                    Hier<double>& P = ctx.h64;
+                    CK(cudaMemcpyAsync(P.F[0], vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx.s));
+                    if ((st = vcycle(ctx, P, sig.opclass, o, true))) return st;
+                    double* zj = (double*)ctx.Z + (size_t)j * n;
+                    CK(cudaMemcpyAsync(zj, P.U[0][P.ri[0]], sizeof(double) * L.half, cudaMemcpyDeviceToDevice, ctx.s));
+                    CK(cudaMemcpyAsync(zj + L.half, P.U[0][P.bi[0]] + L.half, sizeof(double) * L.half,
+                                       cudaMemcpyDeviceToDevice, ctx.s));
+                    if (sig.opclass == 0)
+                        k_apply<double, KOp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                            L, ctx.kop64, csplit<double>(zj, L), split<double>(ctx.w, L));
+                    else
+                        k_apply<double, ROp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                            L, ctx.rop64, csplit<double>(zj, L), split<double>(ctx.w, L));
+                    CKL();
+                }
+                vcycles++;
+                // CGS2 against v_0..v_j: pass 1 coefficients in hcol[0..j], pass 2 in
+                // hcol[m+2 ..]; the Hessenberg column is their sum
+                for (int pass = 0; pass < 2; pass++) {
+                    double* hp = ctx.hcol + (pass ? m + 2 : 0);
+                    k_multidot<<<db, TPB, 0, ctx.s>>>(n, j + 1, ctx.Vptr, ctx.w, ctx.dpart);
+                    CKL();
+                    k_multidot_finish<<<j + 1, TPB, 0, ctx.s>>>(j + 1, db, ctx.dpart, hp, 0);
+                    CKL();
+                    k_multiaxpy<<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, j + 1, ctx.Vptr, hp, ctx.w);
+                    CKL();
+                }
+                // ||w||^2 (Vptr[m+1] points at w) into hcol[j+1]
+                k_multidot<<<db, TPB, 0, ctx.s>>>(n, 1, ctx.Vptr + m + 1, ctx.w, ctx.dpart);
+                CKL();
+                k_multidot_finish<<<1, TPB, 0, ctx.s>>>(1, db, ctx.dpart, ctx.hcol + j + 1, 0);
+                CKL();
+                CK(cudaMemcpyAsync(ctx.hpin, ctx.hcol, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, ctx.s));
+                CK(cudaMemcpyAsync(ctx.hpin + 256, ctx.hcol + m + 2, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost,
+                                   ctx.s));
+                CK(cudaStreamSynchronize(ctx.s));
+                for (int i = 0; i <= j; i++) HH(i, j) = ctx.hpin[i] + ctx.hpin[256 + i];
+                double hn = std::sqrt(std::max(ctx.hpin[j + 1], 0.0));
+                if (!(hn <= 1e308)) { inf.status = MPS_ERR_NAN; done = true; break; }
+                HH(j + 1, j) = hn;
+                ctx.hpin[0] = hn;
+                CK(cudaMemcpyAsync(ctx.hcol + j + 1, ctx.hpin, sizeof(double), cudaMemcpyHostToDevice, ctx.s));
+                if (hn > 0.0) {
+                    k_scale_to<<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, ctx.w, ctx.hcol, j + 1,
+                                                                                    ctx.V + (size_t)(j + 1) * n, nullptr);
+                    CKL();
+                }
+                for (int i = 0; i < j; i++) {
+                    double t = cs[i] * HH(i, j) + sn[i] * HH(i + 1, j);
+                    HH(i + 1, j) = -sn[i] * HH(i, j) + cs[i] * HH(i + 1, j);
+                    HH(i, j) = t;
+                }
+                double a = HH(j, j), b = HH(j + 1, j), rr = std::sqrt(a * a + b * b);
+                cs[j] = rr == 0.0 ? 1.0 : a / rr;
+                sn[j] = rr == 0.0 ? 0.0 : b / rr;
+                HH(j, j) = cs[j] * a + sn[j] * b;
+                HH(j + 1, j) = 0.0;
+                gq[j + 1] = -sn[j] * gq[j];
+                gq[j] = cs[j] * gq[j];
+                it++;
+                const double est = std::fabs(gq[j + 1]) / (bnorm > 0 ? bnorm : 1.0);
+                if ((o->tol_kind == MPS_TOL_REL_L2 && est <= o->tol) || hn == 0.0) { j++; break; }
+            }
+            if (done) break;
+            // y = H^{-1} g ; x += Z y
+            for (int i = j - 1; i >= 0; i--) {
+                double s = gq[i];
+                for (int q = i + 1; q < j; q++) s -= HH(i, q) * y[q];
+                y[i] = (HH(i, i) != 0.0) ? s / HH(i, i) : 0.0;
+            }
+            for (int i = 0; i < j; i++) {
+                if (mixed)
+                    k_axpy<float, double><<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, y[i], (float*)ctx.Z + (size_t)i * n, ctx.x64);
+                else
+                    k_axpy<double, double><<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, y[i], (double*)ctx.Z + (size_t)i * n, ctx.x64);
+                CKL();
+            }
+        }
+    }
+    // ---- output ----
+    int gst = 0;
+    CK(cudaMemcpyAsync(&gst, ctx.dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx.s));
+    k_unpack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, csplit<double>(ctx.x64, L0), in.soln);
+    CKL();
+    if (o->fill_ghosts) {
+        const int mx = std::max(std::max(L0.ny * L0.nz, L0.nx * L0.nz), L0.nx * L0.ny);
+        const double* zf[6];
+        for (int f = 0; f < 6; f++) zf[f] = in.bcval[f];
+        k_fill_ghosts<<<nblk(mx), TPB, 0, ctx.s>>>(L0, in.soln, zf[0], zf[1], zf[2], zf[3], zf[4], zf[5]);
+        CKL();
+    }
+    CK(cudaEventRecord(ctx.e1, ctx.s));
+    CK(cudaStreamSynchronize(ctx.s));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx.e0, ctx.e1));
+    inf.iters = it;
+    inf.vcycles = vcycles;
+    inf.levels = nl;
+    inf.rel_res = rel;
+    inf.rms_res = rms;
+    inf.time_ms = ms;
+    if (inf.status == MPS_OK && !ref_norm_only && !conv()) inf.status = MPS_ERR_NOT_CONVERGED;
+    (void)gst;
+    if (info) *info = inf;
+    return inf.status == MPS_ERR_NAN ? MPS_ERR_NAN : 0;
+}
+
+}  // namespace mps
+
+// ======================================================================
+// C ABI
+// ======================================================================
+using namespace mps;
+
+extern "C" {
+
+void mps_default_opts(mps_solver_opts* o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-10;
+    o->tol_kind = MPS_TOL_REL_L2;
+    o->maxit = 50;
+    o->nu1 = 2;
+    o->nu2 = 2;
+    o->hierarchy = MPS_HIER_GEOM;
+    o->ranks[0] = o->ranks[1] = o->ranks[2] = 1;
+    o->max_coarse = 125;
+    o->precision = MPS_PREC_FP64;
+    o->inner_cycles = 0;
+    o->krylov = MPS_KRYLOV_NONE;
+    o->restart = 30;
+    o->fill_ghosts = 0;
+    o->use_graph = 1;
+    o->transpose = 0;
+    o->flux = MPS_FLUX_UPWIND;
+}
+
+const char* mps_version(void) { return "mps3d_b200 0.1 (sm_100a)"; }
+
+int mps_create(mps_handle* h, int device)
+{
+    if (!h) return MPS_ERR_BAD_ARG;
+    *h = nullptr;
+    mps_handle_s* H = new (std::nothrow) mps_handle_s();
+    if (!H) return MPS_ERR_NOMEM;
+    Ctx& ctx = H->ctx;
+    int dev = device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) { delete H; return MPS_ERR_CUDA; }
+    if (cudaSetDevice(dev) != cudaSuccess) { delete H; return MPS_ERR_CUDA; }
+    ctx.dev = dev;
+    if (cudaStreamCreateWithFlags(&ctx.s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx.e0) != cudaSuccess || cudaEventCreate(&ctx.e1) != cudaSuccess ||
+        cudaMallocHost((void**)&ctx.hpin, sizeof(double) * 512) != cudaSuccess ||
+        cudaMalloc((void**)&ctx.dmax, sizeof(unsigned long long) * 8) != cudaSuccess) {
+        delete H;
+        return MPS_ERR_CUDA;
+    }
+    *h = H;
+    return MPS_OK;
+}
+
+int mps_destroy(mps_handle h)
+{
+    if (!h) return MPS_ERR_BAD_ARG;
+    Ctx& ctx = h->ctx;
+    cudaSetDevice(ctx.dev);
+    cudaStreamSynchronize(ctx.s);
+    ctx.ar.clear();
+    ctx.inbuf.clear();
+    if (ctx.dmax) cudaFree(ctx.dmax);
+    if (ctx.hpin) cudaFreeHost(ctx.hpin);
+    if (ctx.e0) cudaEventDestroy(ctx.e0);
+    if (ctx.e1) cudaEventDestroy(ctx.e1);
+    if (ctx.s) cudaStreamDestroy(ctx.s);
+    delete h;
+    return MPS_OK;
+}
+
+void* mps_stream(mps_handle h) { return h ? (void*)h->ctx.s : nullptr; }
+
+const char* mps_last_error(mps_handle h) { return h ? h->ctx.err.msg.c_str() : "null handle"; }
+
+static int run_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel, const double* dcoeff,
+                   const double* reac, const double* source, const int bc_code[6], const double* const bcval[6],
+                   const double* sterm, double* soln, const mps_solver_opts* opts, mps_solve_info* info,
+                   void* stream, int ref_norm_only)
+{
+    if (!h || !bc_code) return MPS_ERR_BAD_ARG;
+    Ctx& ctx = h->ctx;
+    ctx.err = Err();
+    if (cudaSetDevice(ctx.dev) != cudaSuccess) return MPS_ERR_CUDA;
+    mps_solver_opts o;
+    if (opts) o = *opts;
+    else mps_default_opts(&o);
+    cudaStream_t user = (cudaStream_t)stream;
+    cudaEvent_t ev = nullptr;
+    if (user && user != ctx.s) {  // order the handle's stream after the caller's
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return MPS_ERR_CUDA;
+        cudaEventRecord(ev, user);
+        cudaStreamWaitEvent(ctx.s, ev, 0);
+    }
+    Inputs in;
+    in.vel = vel; in.dcoeff = dcoeff; in.reac = reac; in.source = source; in.sterm = sterm; in.soln = soln;
+    for (int f = 0; f < 6; f++) in.bcval[f] = bcval ? bcval[f] : nullptr;
+    int st = solve_impl(ctx, g, timederiv, dt, in, bc_code, &o, info, ref_norm_only);
+    if (ev) {
+        cudaEventRecord(ev, ctx.s);
+        cudaStreamWaitEvent(user, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    if (st && info) info->status = st;
+    return st;
+}
+
+int mps_linsolve_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel,
+                     const double* dcoeff, const double* reac, const double* source, const int bc_code[6],
+                     const double* const bcval[6], const double* mgridsterm, double* soln,
+                     const mps_solver_opts* opts, mps_solve_info* info, void* stream)
+{
+    int st = run_dev(h, g, timederiv, dt, vel, dcoeff, reac, source, bc_code, bcval, mgridsterm, soln, opts, info,
+                     stream, 0);
+    if (st) return st;
+    return info ? info->status : MPS_OK;
+}
+
+// host-pointer front end: stage the ghosted inputs on the device
+static int run_host(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel,
+                    const double* dcoeff, const double* reac, const double* source, const int bc_code[6],
+                    const double* const bcval[6], const double* mgridsterm, double* soln,
+                    const mps_solver_opts* opts, mps_solve_info* info, int ref_norm_only)
+{
+    if (!h || !g || !dcoeff || !source || !soln || !bc_code) return MPS_ERR_BAD_ARG;
+    if (g->lx < 1 || g->ly < 1 || g->lz < 1) return MPS_ERR_BAD_ARG;
+    Ctx& ctx = h->ctx;
+    if (cudaSetDevice(ctx.dev) != cudaSuccess) return MPS_ERR_CUDA;
+    const size_t ng = (size_t)(g->lx + 2) * (g->ly + 2) * (g->lz + 2);
+    const size_t ni = (size_t)g->lx * g->ly * g->lz;
+    const size_t fs[6] = {(size_t)g->ly * g->lz, (size_t)g->ly * g->lz, (size_t)g->lx * g->lz,
+                          (size_t)g->lx * g->lz, (size_t)g->lx * g->ly, (size_t)g->lx * g->ly};
+    size_t need = ng * (3 + 1 + 1 + 1 + 1) + ni + fs[0] * 2 + fs[2] * 2 + fs[4] * 2;
+    need *= sizeof(double);
+    if (ctx.inbuf_bytes < need) {
+        ctx.inbuf.clear();
+        ctx.inbuf_bytes = 0;
+        if (!ctx.inbuf.get(need)) return MPS_ERR_NOMEM;
+        ctx.inbuf_bytes = need;
+    }
+    double* base = (double*)ctx.inbuf.blocks[0];
+    double* d_vel = base;
+    double* d_dc = d_vel + 3 * ng;
+    double* d_re = d_dc + ng;
+    double* d_src = d_re + ng;
+    double* d_sol = d_src + ng;
+    double* d_st = d_sol + ng;
+    double* d_bc = d_st + ni;
+    const double* dbv[6];
+    cudaStream_t s = ctx.s;
+#define H2D(dst, src, n) \
+    if (cudaMemcpyAsync(dst, src, sizeof(double) * (n), cudaMemcpyHostToDevice, s) != cudaSuccess) return MPS_ERR_CUDA
+    if (vel) { H2D(d_vel, vel, 3 * ng); }
+    H2D(d_dc, dcoeff, ng);
+    if (reac) { H2D(d_re, reac, ng); }
+    H2D(d_src, source, ng);
+    H2D(d_sol, soln, ng);
+    if (mgridsterm) { H2D(d_st, mgridsterm, ni); }
+    double* p = d_bc;
+    for (int f = 0; f < 6; f++) {
+        dbv[f] = nullptr;
+        if (bcval && bcval[f]) {
+            H2D(p, bcval[f], fs[f]);
+            dbv[f] = p;
+        }
+        p += fs[f];
+    }
+#undef H2D
+    int st = run_dev(h, g, timederiv, dt, vel ? d_vel : nullptr, d_dc, reac ? d_re : nullptr, d_src, bc_code, dbv,
+                     mgridsterm ? d_st : nullptr, d_sol, opts, info, nullptr, ref_norm_only);
+    if (st) return st;
+    if (cudaMemcpyAsync(soln, d_sol, sizeof(double) * ng, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPS_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_ERR_CUDA;
+    return info ? info->status : MPS_OK;
+}
+
+int mps_linsolve(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel, const double* dcoeff,
+                 const double* reac, const double* source, const int bc_code[6], const double* const bcval[6],
+                 const double* mgridsterm, double* soln, const mps_solver_opts* opts, mps_solve_info* info)
+{
+    return run_host(h, g, timederiv, dt, vel, dcoeff, reac, source, bc_code, bcval, mgridsterm, soln, opts, info, 0);
+}
+
+int mps_vcycle_once(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel,
+                    const double* dcoeff, const double* reac, const double* source, const int bc_code[6],
+                    const double* const bcval[6], const double* mgridsterm, double* soln, double* resnorm,
+                    const mps_solver_opts* opts)
+{
+    mps_solver_opts o;
+    if (opts) o = *opts;
+    else {
+        mps_default_opts(&o);
+        o.hierarchy = MPS_HIER_CELL;
+    }
+    o.maxit = 1;
+    o.krylov = MPS_KRYLOV_NONE;
+    o.precision = MPS_PREC_FP64;
+    mps_solve_info info;
+    int st = run_host(h, g, timederiv, dt, vel, dcoeff, reac, source, bc_code, bcval, mgridsterm, soln, &o, &info, 1);
+    if (resnorm) *resnorm = info.rms_res;
+    return st;
+}
+
+int mps_apply_A_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel,
+                    const double* dcoeff, const double* reac, const int bc_code[6], const double* soln, double* AX,
+                    const mps_solver_opts* opts, void* stream)
+{
+    if (!h || !g || !dcoeff || !soln || !AX || !bc_code) return MPS_ERR_BAD_ARG;
+    Ctx& ctx = h->ctx;
+    ctx.err = Err();
+    if (cudaSetDevice(ctx.dev) != cudaSuccess) return MPS_ERR_CUDA;
+    mps_solver_opts o;
+    if (opts) o = *opts;
+    else mps_default_opts(&o);
+    // A u through the same operator setup as a solve: run a zero-iteration
+    // solve to build the fine operator, then apply it
+    o.maxit = 0;
+    o.krylov = MPS_KRYLOV_NONE;
+    o.precision = MPS_PREC_FP64;
+    o.hierarchy = MPS_HIER_GEOM;
+    const size_t ng = (size_t)(g->lx + 2) * (g->ly + 2) * (g->lz + 2);
+    double* tmp = nullptr;
+    double* zsrc = nullptr;
+    cudaStream_t s = ctx.s;
+    if (cudaMallocAsync((void**)&tmp, sizeof(double) * ng * 2, s) != cudaSuccess) return MPS_ERR_CUDA;
+    zsrc = tmp + ng;
+    cudaMemcpyAsync(tmp, soln, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
+    cudaMemsetAsync(zsrc, 0, sizeof(double) * ng, s);
+    const double* nob[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    int bcfix[6];
+    for (int f = 0; f < 6; f++) bcfix[f] = bc_code[f];
+    mps_solve_info info;
+    double zeros_face_dummy = 0.0;
+    (void)zeros_face_dummy;
+    // DIRC/FLUX faces need value arrays for find_bvec; they do not enter A
+    std::vector<double*> fb;
+    const double* bv[6];
+    for (int f = 0; f < 6; f++) {
+        bv[f] = nob[f];
+        if (bc_code[f] == BC_DIRC || bc_code[f] == BC_FLUX) {
+            size_t n = (f < 2) ? (size_t)g->ly * g->lz : (f < 4 ? (size_t)g->lx * g->lz : (size_t)g->lx * g->ly);
+            double* d = nullptr;
+            if (cudaMallocAsync((void**)&d, sizeof(double) * n, s) != cudaSuccess) return MPS_ERR_CUDA;
+            cudaMemsetAsync(d, 0, sizeof(double) * n, s);
+            fb.push_back(d);
+            bv[f] = d;
+        }
+    }
+    int st = run_dev(h, g, timederiv, dt, vel, dcoeff, reac, zsrc, bcfix, bv, nullptr, tmp, &o, &info, stream, 1);
+    if (!st) {
+        const Lev& L = ctx.lev[0];
+        double* out = ctx.w ? ctx.w : nullptr;
+        double* buf = nullptr;
+        if (cudaMallocAsync((void**)&buf, sizeof(double) * 2 * L.half, s) != cudaSuccess) return MPS_ERR_CUDA;
+        out = buf;
+        if (ctx.sig.opclass == 0)
+            k_apply<double, KOp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, s>>>(
+                L, ctx.kop64, csplit<double>(ctx.x64, L), split<double>(out, L));
+        else
+            k_apply<double, ROp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, s>>>(
+                L, ctx.rop64, csplit<double>(ctx.x64, L), split<double>(out, L));
+        k_unpack_nat<double><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, s>>>(L, csplit<double>(out, L), AX);
+        cudaFreeAsync(buf, s);
+        if (cudaGetLastError() != cudaSuccess) st = MPS_ERR_CUDA;
+    }
+    for (double* d : fb) cudaFreeAsync(d, s);
+    cudaFreeAsync(tmp, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_ERR_CUDA;
+    return st;
+}
+
+int mps_find_bvec_dev(mps_handle h, const mps_grid* g, const double* vel, const double* dcoeff,
+                      const double* source, const int bc_code[6], const double* const bcval[6],
+                      const double* mgridsterm, double* b, const mps_solver_opts* opts, void* stream)
+{
+    if (!h || !g || !dcoeff || !source || !b || !bc_code) return MPS_ERR_BAD_ARG;
+    Ctx& ctx = h->ctx;
+    if (cudaSetDevice(ctx.dev) != cudaSuccess) return MPS_ERR_CUDA;
+    for (int f = 0; f < 6; f++)
+        if (bc_code[f] < 1 || bc_code[f] > 5 || (!(bcval && bcval[f]) && (bc_code[f] == BC_DIRC || bc_code[f] == BC_FLUX)))
+            return MPS_ERR_BAD_ARG;
+    const double llen[3] = {g->llenx, g->lleny, g->llenz};
+    Lev L = make_lev_uniform(g->lx, g->ly, g->lz, llen, bc_code);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx.s;
+    double* buf = nullptr;
+    if (cudaMallocAsync((void**)&buf, sizeof(double) * 2 * L.half, s) != cudaSuccess) return MPS_ERR_CUDA;
+    cudaMemsetAsync(buf, 0, sizeof(double) * 2 * L.half, s);
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    k_find_bvec<<<nblk(n), TPB, 0, s>>>(L, vel, dcoeff, source, bcval[0], bcval[1], bcval[2], bcval[3], bcval[4],
+                                        bcval[5], mgridsterm, opts ? opts->flux : 0, split<double>(buf, L));
+    k_unpack_nat<double><<<nblk(n), TPB, 0, s>>>(L, csplit<double>(buf, L), b);
+    cudaFreeAsync(buf, s);
+    if (cudaGetLastError() != cudaSuccess) return MPS_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_ERR_CUDA;
+    return MPS_OK;
+}
+
+int mps_fill_ghosts_dev(mps_handle h, const mps_grid* g, const int bc_code[6], const double* const bcval[6],
+                        double* soln, void* stream)
+{
+    if (!h || !g || !soln || !bc_code) return MPS_ERR_BAD_ARG;
+    Ctx& ctx = h->ctx;
+    if (cudaSetDevice(ctx.dev) != cudaSuccess) return MPS_ERR_CUDA;
+    for (int f = 0; f < 6; f++)
+        if (bc_code[f] < 1 || bc_code[f] > 5 || (!(bcval && bcval[f]) && bc_code[f] == BC_DIRC)) return MPS_ERR_BAD_ARG;
+    const double llen[3] = {g->llenx, g->lleny, g->llenz};
+    Lev L = make_lev_uniform(g->lx, g->ly, g->lz, llen, bc_code);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx.s;
+    const int mx = std::max(std::max(L.ny * L.nz, L.nx * L.nz), L.nx * L.ny);
+    k_fill_ghosts<<<nblk(mx), TPB, 0, s>>>(L, soln, bcval ? bcval[0] : nullptr, bcval ? bcval[1] : nullptr,
+                                           bcval ? bcval[2] : nullptr, bcval ? bcval[3] : nullptr,
+                                           bcval ? bcval[4] : nullptr, bcval ? bcval[5] : nullptr);
+    if (cudaGetLastError() != cudaSuccess) return MPS_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_ERR_CUDA;
+    return MPS_OK;
+}
+
+}  // extern "C"

@@ -320,7 +320,8 @@ void orc_gs_smooth(const orc_grid* g, double* soln, int timederiv, double dt,
 /* ---- hierarchy sizes ----
  * CELL: lx/2 by integer division (mgridsteps.f90:21-23), stop when any local
  *       size (global / ranks) <= LMIN (:512).
- * UNIFORM (extension): ceil(l/2), a size of 1 stays 1, stop when the level
+ * GEOM (extension): l/2 coarse cells (pairs; for an odd size the last
+ *       coarse cell takes three; a size of 1 stays 1); stop when the level
  *       holds <= max_coarse cells. */
 static dims3 coarse_dims(const orc_grid* g, dims3 f)
 {
@@ -330,9 +331,9 @@ static dims3 coarse_dims(const orc_grid* g, dims3 f)
         c.ly = g->py * ((f.ly / g->py) / 2);
         c.lz = g->pz * ((f.lz / g->pz) / 2);
     } else {
-        c.lx = f.lx > 1 ? (f.lx + 1) / 2 : 1;
-        c.ly = f.ly > 1 ? (f.ly + 1) / 2 : 1;
-        c.lz = f.lz > 1 ? (f.lz + 1) / 2 : 1;
+        c.lx = f.lx > 1 ? f.lx / 2 : 1;
+        c.ly = f.ly > 1 ? f.ly / 2 : 1;
+        c.lz = f.lz > 1 ? f.lz / 2 : 1;
     }
     return c;
 }
@@ -345,48 +346,100 @@ static int is_coarsest(const orc_grid* g, dims3 d)
            (d.lx == 1 && d.ly == 1 && d.lz == 1);
 }
 
-/* children of coarse cell I (1-based) along one direction */
-static inline int child_lo(int I) { return 2 * I - 1; }
-static inline int child_n(int I, int nf) { return (2 * I <= nf) ? 2 : 1; }
+/* Cell widths per level (GEOM hierarchy).  Coarse cells are pairs of fine
+ * cells; when a size is odd the last coarse cell takes three.  Every level is
+ * then uniform except for its last cell, whose width is tracked exactly:
+ * w = regular width, wl = width of the last cell (wl/w -> 1 with depth).  The CELL hierarchy keeps the
+ * reference's dx = llen/l at every level (find_AX, discretepde.f90:724-726). */
+typedef struct { int n[3]; double w[3], wl[3]; } geo3;
 
-/* restriction, mgridsteps.f90:11-53 (8-cell average); UNIFORM: average over
- * the children that exist (the last coarse cell of an odd size has one). */
-static void restrict_field(const orc_grid* g, dims3 f, dims3 c, const double* fine, int fine_ghosted,
-                           double* coarse, int coarse_ghosted)
+static geo3 geo_fine(const orc_grid* g)
 {
+    geo3 G;
+    G.n[0] = g->lx; G.n[1] = g->ly; G.n[2] = g->lz;
+    const double L[3] = {g->llenx, g->lleny, g->llenz};
+    for (int a = 0; a < 3; a++) G.w[a] = G.wl[a] = L[a] / G.n[a];
+    return G;
+}
+
+static geo3 geo_coarse(const orc_grid* g, geo3 f)
+{
+    dims3 fd = {f.n[0], f.n[1], f.n[2]};
+    dims3 cd = coarse_dims(g, fd);
+    geo3 c;
+    c.n[0] = cd.lx; c.n[1] = cd.ly; c.n[2] = cd.lz;
+    const double L[3] = {g->llenx, g->lleny, g->llenz};
+    for (int a = 0; a < 3; a++) {
+        if (g->hier == ORC_HIER_CELL) {
+            c.w[a] = c.wl[a] = L[a] / c.n[a];
+        } else if (f.n[a] == 1) {
+            c.w[a] = c.wl[a] = f.wl[a];
+        } else {
+            c.w[a] = 2.0 * f.w[a];
+            c.wl[a] = (f.n[a] & 1) ? 2.0 * f.w[a] + f.wl[a] : f.w[a] + f.wl[a];
+            if (c.n[a] == 1) c.w[a] = c.wl[a];
+        }
+    }
+    return c;
+}
+
+static inline double cwidth(const geo3* G, int ax, int i0) /* 0-based index */
+{
+    return i0 == G->n[ax] - 1 ? G->wl[ax] : G->w[ax];
+}
+
+/* children of coarse cell I (1-based) along one direction: 2I-1 and 2I, plus
+ * 2I+1 for the last coarse cell of an odd size */
+static inline int child_lo(int I) { return 2 * I - 1; }
+static inline int child_n(int I, int nf, int nc) { return nf == 1 ? 1 : (I == nc ? nf - 2 * (nc - 1) : 2); }
+
+/* restriction, mgridsteps.f90:11-53 (8-cell average).  UNIFORM: the
+ * volume-weighted average of the children that exist (equal to the 8-cell
+ * average when all children are regular cells). */
+static void restrict_fieldg(const orc_grid* g, const geo3* fg, const geo3* cg, const double* fine,
+                            int fine_ghosted, double* coarse, int coarse_ghosted)
+{
+    const int cell = g->hier == ORC_HIER_CELL;
+    dims3 f = {fg->n[0], fg->n[1], fg->n[2]}, c = {cg->n[0], cg->n[1], cg->n[2]};
 #pragma omp parallel for schedule(static)
     for (int K = 1; K <= c.lz; K++)
         for (int J = 1; J <= c.ly; J++)
             for (int I = 1; I <= c.lx; I++) {
-                double s = 0.0;
-                int nx = child_n(I, f.lx), ny = child_n(J, f.ly), nz = child_n(K, f.lz);
-                if (g->hier == ORC_HIER_CELL) { nx = ny = nz = 2; }
-                /* reference summation order: pairs in x, then y, then z */
+                double s = 0.0, vol = 0.0;
+                int nx = cell ? 2 : child_n(I, f.lx, c.lx), ny = cell ? 2 : child_n(J, f.ly, c.ly),
+                    nz = cell ? 2 : child_n(K, f.lz, c.lz);
+                /* reference summation order: x, then y, then z */
                 for (int dk = 0; dk < nz; dk++)
                     for (int dj = 0; dj < ny; dj++)
                         for (int di = 0; di < nx; di++) {
                             int i = child_lo(I) + di, j = child_lo(J) + dj, k = child_lo(K) + dk;
                             long src;
-                            if (fine_ghosted) {
-                                int lx = f.lx, ly = f.ly;
-                                src = GX(i, j, k);
+                            int lx = f.lx, ly = f.ly;
+                            src = fine_ghosted ? GX(i, j, k) : IX(i, j, k);
+                            if (cell) {
+                                s += fine[src];
                             } else {
-                                int lx = f.lx, ly = f.ly;
-                                src = IX(i, j, k);
+                                double v = cwidth(fg, 0, i - 1) * cwidth(fg, 1, j - 1) * cwidth(fg, 2, k - 1);
+                                s += v * fine[src];
+                                vol += v;
                             }
-                            s += fine[src];
                         }
-                double v = s * (1.0 / (double)(nx * ny * nz));
-                long dst;
-                if (coarse_ghosted) {
-                    int lx = c.lx, ly = c.ly;
-                    dst = GX(I, J, K);
-                } else {
-                    int lx = c.lx, ly = c.ly;
-                    dst = IX(I, J, K);
-                }
-                coarse[dst] = v;
+                double val = cell ? s * (1.0 / 8.0) : s / vol;
+                int lx = c.lx, ly = c.ly;
+                long dst = coarse_ghosted ? GX(I, J, K) : IX(I, J, K);
+                coarse[dst] = val;
             }
+}
+
+static void restrict_field(const orc_grid* g, dims3 f, dims3 c, const double* fine, int fine_ghosted,
+                           double* coarse, int coarse_ghosted)
+{
+    /* CELL only (uniform widths) */
+    geo3 fg, cg;
+    fg.n[0] = f.lx; fg.n[1] = f.ly; fg.n[2] = f.lz;
+    cg.n[0] = c.lx; cg.n[1] = c.ly; cg.n[2] = c.lz;
+    for (int a = 0; a < 3; a++) { fg.w[a] = fg.wl[a] = 1.0; cg.w[a] = cg.wl[a] = 1.0; }
+    restrict_fieldg(g, &fg, &cg, fine, fine_ghosted, coarse, coarse_ghosted);
 }
 
 /* restrict_boundary, mgridsteps.f90:55-128 (average of 4 children; UNIFORM:
@@ -400,7 +453,7 @@ static void restrict_bcvals(dims3 f, dims3 c, int cell, const double* const* bf,
         int n1 = fa[ax][0], c1 = ca[ax][0], c2 = ca[ax][1];
         for (int b = 1; b <= c2; b++)
             for (int a = 1; a <= c1; a++) {
-                int na = cell ? 2 : child_n(a, fa[ax][0]), nb = cell ? 2 : child_n(b, fa[ax][1]);
+                int na = cell ? 2 : child_n(a, fa[ax][0], c1), nb = cell ? 2 : child_n(b, fa[ax][1], c2);
                 double s = 0.0;
                 for (int db = 0; db < nb; db++)
                     for (int da = 0; da < na; da++)
@@ -455,44 +508,131 @@ void orc_fill_ghosts(const orc_grid* g, double* soln, const int* bc, const doubl
     ghost_update(d, soln, bc, bcvals);
 }
 
-/* prolongation slope factor of fine cell i (1-based) whose parent is
- * I=(i+1)/2: CELL uses -1/8 / +1/8 (prolongation1, mgridsteps.f90:197-209:
- * 0.25 * 0.5 * (e[I+1]-e[I-1])); UNIFORM uses the true offset of the fine
- * centre from the parent centre divided by twice the coarse spacing. */
-static inline double prolong_alpha(int cell, int i, int nf, int nc)
+/* prolongation1, mgridsteps.f90:170-216 (CELL): e_f = e_c + sum_ax alpha_ax *
+ * (e_c[I+1] - e_c[I-1]) with alpha = -1/8 / +1/8 (0.25*0.5*..., :197-209);
+ * the odd last fine cell has no parent and is not corrected.
+ * GEOM: tensor-product linear interpolation between the coarse centres that
+ * bracket the fine centre, positions measured in units of the fine regular
+ * width; ghost centres mirror across the wall with the value -e (Dirichlet)
+ * or +e (other faces), or wrap for periodic faces.  (The additive central-
+ * slope form loses its two-grid rate next to an odd last cell in 3D; the
+ * tensor-product form keeps the even-size rate.) */
+/* value of the coarse correction at ghosted index (qx,qy,qz), where any of
+ * the indices may be a ghost (0 or n+1): each ghost axis maps back to the
+ * adjacent interior cell with the sign of its face rule (Dirichlet -1,
+ * other +1) or wraps for a periodic face.  Equals the face ghosts that
+ * update_boundary_ghostvalues sets, extended to edges and corners. */
+static double ghost_val(dims3 c, const double* ec, const int* bc, int qx, int qy, int qz)
 {
-    int I = (i + 1) / 2;
-    if (cell || 2 * nc == nf) return (i & 1) ? -0.125 : 0.125;
-    if (nf == nc) return 0.0;
-    return (((double)i - 0.5) * (double)nc / (double)nf - ((double)I - 0.5)) * 0.5;
+    int q[3] = {qx, qy, qz}, n[3] = {c.lx, c.ly, c.lz};
+    double sgn = 1.0;
+    for (int a = 0; a < 3; a++) {
+        if (q[a] >= 1 && q[a] <= n[a]) continue;
+        int side = q[a] < 1 ? 0 : 1;
+        if (bc[2 * a] == ORC_PERI) q[a] = q[a] < 1 ? n[a] : 1;
+        else {
+            if (bc[2 * a + side] == ORC_DIRC) sgn = -sgn;
+            q[a] = q[a] < 1 ? 1 : n[a];
+        }
+    }
+    int lx = c.lx, ly = c.ly;
+    return sgn * ec[GX(q[0], q[1], q[2])];
 }
 
-/* prolongation1, mgridsteps.f90:170-216, generalised to the UNIFORM sizes.
- * ec is ghosted at the coarse size with valid face ghosts; ef (ghosted, fine
- * size) receives the interpolant on the fine cells that have a parent. */
-static void prolong(int cell, dims3 f, dims3 c, const double* ec, double* ef)
+typedef struct { int j0, j1; double t; } lin1; /* e = (1-t) e[j0] + t e[j1]; j = -1 / nc: ghost */
+
+static lin1 geom_lin(const geo3* fg, const geo3* cg, int ax, int i0, int per)
 {
+    lin1 r;
+    const int nf = fg->n[ax], nc = cg->n[ax];
+    if (nf == nc) { r.j0 = r.j1 = i0; r.t = 0.0; return r; }
+    const double rf = fg->wl[ax] / fg->w[ax], Rc = cg->wl[ax] / fg->w[ax];
+    const double xf = (i0 == nf - 1) ? (nf - 1) + 0.5 * rf : i0 + 0.5;
+    const double Ltot = 2.0 * (nc - 1) + Rc;
+    const double X0 = (nc == 1) ? 0.5 * Rc : 1.0;
+    const double Xl = 2.0 * (nc - 1) + 0.5 * Rc;
+    int I = (i0 >> 1) < nc - 1 ? (i0 >> 1) : nc - 1;
+    double XI = (I == nc - 1) ? Xl : 2.0 * I + 1.0;
+    int J = xf >= XI ? I : I - 1;
+    double XJ, XJ1;
+    if (J < 0) XJ = per ? Xl - Ltot : -X0;
+    else XJ = (J == nc - 1) ? Xl : 2.0 * J + 1.0;
+    if (J + 1 > nc - 1) XJ1 = per ? X0 + Ltot : 2.0 * Ltot - Xl;
+    else XJ1 = (J + 1 == nc - 1) ? Xl : 2.0 * (J + 1) + 1.0;
+    r.j0 = J;
+    r.j1 = J + 1;
+    r.t = (xf - XJ) / (XJ1 - XJ);
+    return r;
+}
+
+/* coarse value with ghost rule (1-based index into a ghosted coarse array
+ * whose face ghosts are already set by ghost_update); jz is 0-based along ax */
+static void prolongg(const orc_grid* g, const geo3* fg, const geo3* cg, const int* bc, const double* ec,
+                     double* ef)
+{
+    const int cell = g->hier == ORC_HIER_CELL;
+    dims3 f = {fg->n[0], fg->n[1], fg->n[2]}, c = {cg->n[0], cg->n[1], cg->n[2]};
+    const int per[3] = {bc[0] == ORC_PERI, bc[2] == ORC_PERI, bc[4] == ORC_PERI};
 #pragma omp parallel for schedule(static)
     for (int k = 1; k <= f.lz; k++)
         for (int j = 1; j <= f.ly; j++)
             for (int i = 1; i <= f.lx; i++) {
-                int I = (i + 1) / 2, J = (j + 1) / 2, K = (k + 1) / 2;
-                if (I > c.lx || J > c.ly || K > c.lz) continue; /* CELL: odd last cell dropped */
-                int lx = c.lx, ly = c.ly;
-                double e0 = ec[GX(I, J, K)];
-                double ax = prolong_alpha(cell, i, f.lx, c.lx);
-                double ay = prolong_alpha(cell, j, f.ly, c.ly);
-                double az = prolong_alpha(cell, k, f.lz, c.lz);
-                double dxv = ec[GX(I + 1, J, K)] - ec[GX(I - 1, J, K)];
-                double dyv = ec[GX(I, J + 1, K)] - ec[GX(I, J - 1, K)];
-                double dzv = ec[GX(I, J, K + 1)] - ec[GX(I, J, K - 1)];
-                if (f.lx == c.lx) dxv = 0.0;
-                if (f.ly == c.ly) dyv = 0.0;
-                if (f.lz == c.lz) dzv = 0.0;
-                double v = e0 + ((ax * dxv + ay * dyv) + az * dzv);
-                lx = f.lx; ly = f.ly;
+                if (cell) {
+                    int I = (i + 1) / 2, J = (j + 1) / 2, K = (k + 1) / 2;
+                    if (I > c.lx || J > c.ly || K > c.lz) continue; /* odd last cell dropped */
+                    int lx = c.lx, ly = c.ly;
+                    double e0 = ec[GX(I, J, K)];
+                    double ax = (i & 1) ? -0.125 : 0.125;
+                    double ay = (j & 1) ? -0.125 : 0.125;
+                    double az = (k & 1) ? -0.125 : 0.125;
+                    double dxv = ec[GX(I + 1, J, K)] - ec[GX(I - 1, J, K)];
+                    double dyv = ec[GX(I, J + 1, K)] - ec[GX(I, J - 1, K)];
+                    double dzv = ec[GX(I, J, K + 1)] - ec[GX(I, J, K - 1)];
+                    double v = e0 + ((ax * dxv + ay * dyv) + az * dzv);
+                    lx = f.lx; ly = f.ly;
+                    ef[GX(i, j, k)] = v;
+                    continue;
+                }
+                lin1 L3[3] = {geom_lin(fg, cg, 0, i - 1, per[0]), geom_lin(fg, cg, 1, j - 1, per[1]),
+                              geom_lin(fg, cg, 2, k - 1, per[2])};
+                /* ghosted coarse array: 0-based index q maps to q+1; ghosts at 0 and n+1
+                 * hold the face rule, which for a 1-D bracket is the value we need */
+                double v = 0.0;
+                for (int cz = 0; cz < 2; cz++) {
+                    double wz = cz ? L3[2].t : 1.0 - L3[2].t;
+                    if (wz == 0.0) continue;
+                    int qz = (cz ? L3[2].j1 : L3[2].j0) + 1;
+                    for (int cy = 0; cy < 2; cy++) {
+                        double wy = cy ? L3[1].t : 1.0 - L3[1].t;
+                        if (wy == 0.0) continue;
+                        int qy = (cy ? L3[1].j1 : L3[1].j0) + 1;
+                        for (int cx = 0; cx < 2; cx++) {
+                            double wx = cx ? L3[0].t : 1.0 - L3[0].t;
+                            if (wx == 0.0) continue;
+                            int qx = (cx ? L3[0].j1 : L3[0].j0) + 1;
+                            int lx = c.lx, ly = c.ly;
+                            v += wz * wy * wx * ghost_val(c, ec, bc, qx, qy, qz);
+                        }
+                    }
+                }
+                int lx = f.lx, ly = f.ly;
                 ef[GX(i, j, k)] = v;
             }
+}
+
+static void prolong(int cell, dims3 f, dims3 c, const double* ec, double* ef)
+{
+    /* CELL only */
+    orc_grid g;
+    memset(&g, 0, sizeof(g));
+    g.hier = ORC_HIER_CELL;
+    geo3 fg, cg;
+    fg.n[0] = f.lx; fg.n[1] = f.ly; fg.n[2] = f.lz;
+    cg.n[0] = c.lx; cg.n[1] = c.ly; cg.n[2] = c.lz;
+    for (int a = 0; a < 3; a++) { fg.w[a] = fg.wl[a] = cg.w[a] = cg.wl[a] = 1.0; }
+    int bc[6] = {0, 0, 0, 0, 0, 0};
+    (void)cell;
+    prolongg(&g, &fg, &cg, bc, ec, ef);
 }
 
 /* ---- GMRES bottom solve: gmres.f90:9-434 with gseidel_precond
@@ -798,6 +938,7 @@ int orc_vcycle(const orc_grid* g, double* soln, int timederiv, double dt,
 {
     const long n = nin(g->lx, g->ly, g->lz);
     double* zero = NULL;
+    if (g->hier != ORC_HIER_CELL) return 4; /* the restatement is the reference hierarchy */
     if (!mgridsterm) { zero = zalloc(n); mgridsterm = zero; }
     int st = vcycle_rec(g, 1, soln, timederiv, dt, vel, dcoeff, reac, source, bc, bcvals,
                         mgridsterm, resnorm);
@@ -886,49 +1027,51 @@ void orc_sg_face(double cL, double cR, double DL, double DR, double dx, double* 
 
 /* upwind rows from the find_AX formulas (discretepde.f90:620-1116); SG rows
  * from the 1D flux applied per face (convdiff.f90:280-288) with the same
- * boundary treatment as find_AX for ZGRD and a half-cell SG flux for DIRC. */
-void orc_build_rows(const orc_grid* g, int flux, int timederiv, double dt,
-                    const double* vel, const double* dcoeff, const double* reac,
-                    const int* bc, double* rows)
+ * boundary treatment as find_AX for ZGRD and a half-cell SG flux for DIRC.
+ * A face between cells of widths wa, wb has centre distance d = (wa+wb)/2;
+ * its flux per unit area is F = wL*u_L + wR*u_R and row L gains +F/w_L, row
+ * R gains -F/w_R (on uniform cells: find_AX's (k_half/dx)*(1/dx) etc.). */
+static void build_rows_geo(const geo3* G, int flux, int timederiv, double dt, const double* vel,
+                           const double* dcoeff, const double* reac, const int* bc, double* rows)
 {
-    const int lx = g->lx, ly = g->ly, lz = g->lz;
+    const int lx = G->n[0], ly = G->n[1], lz = G->n[2];
     const long ng = ngh(lx, ly, lz), n = nin(lx, ly, lz);
-    const double h[3] = {g->llenx / lx, g->lleny / ly, g->llenz / lz};
     const int L[3] = {lx, ly, lz};
     memset(rows, 0, sizeof(double) * 7 * n);
     for (int ax = 0; ax < 3; ax++) {
         const double* v = vel + ax * ng;
         const int per = bc[2 * ax] == ORC_PERI;
-        const double dx = h[ax];
         for (int k = 1; k <= lz; k++)
             for (int j = 1; j <= ly; j++)
                 for (int i = 1; i <= lx; i++) {
                     int idx[3] = {i, j, k};
                     int pos = idx[ax];
                     long c = IX(i, j, k);
+                    const double wc = cwidth(G, ax, pos - 1);
                     /* face on the + side of this cell (between pos and pos+1) */
                     if (pos < L[ax] || per) {
                         int r3[3] = {i, j, k};
                         r3[ax] = pos < L[ax] ? pos + 1 : 1;
                         long cr = IX(r3[0], r3[1], r3[2]);
+                        const double wn = cwidth(G, ax, r3[ax] - 1);
+                        const double d = 0.5 * (wc + wn);
                         double kl = dcoeff[GX(i, j, k)], kr = dcoeff[GX(r3[0], r3[1], r3[2])];
                         double vl = v[GX(i, j, k)], vr = v[GX(r3[0], r3[1], r3[2])];
                         double wL, wR;
                         if (flux == ORC_FLUX_SG) {
-                            orc_sg_face(vl, vr, kl, kr, dx, &wL, &wR);
-                            wL /= dx; wR /= dx;
+                            orc_sg_face(vl, vr, kl, kr, d, &wL, &wR);
                         } else {
-                            double d = (0.5 * (kl + kr) / dx) * (1.0 / dx);
+                            double kh = 0.5 * (kl + kr) / d;
                             double vh = 0.5 * (vl + vr);
-                            wL = d; wR = -d;
-                            if (vh > 0.0) wL += vh * (1.0 / dx);
-                            else wR += vh * (1.0 / dx);
+                            wL = kh; wR = -kh;
+                            if (vh > 0.0) wL += vh;
+                            else wR += vh;
                         }
-                        /* flux F = wL u_L + wR u_R: row L += F, row R -= F */
-                        R7(0, c) += wL;
-                        R7(2 + 2 * ax, c) += wR;
-                        R7(0, cr) -= wR;
-                        R7(1 + 2 * ax, cr) -= wL;
+                        const double al = 1.0 / wc, ar = 1.0 / wn;
+                        R7(0, c) += wL * al;
+                        R7(2 + 2 * ax, c) += wR * al;
+                        R7(0, cr) -= wR * ar;
+                        R7(1 + 2 * ax, cr) -= wL * ar;
                     }
                     /* physical boundary faces */
                     if (!per && (pos == 1 || pos == L[ax])) {
@@ -939,17 +1082,17 @@ void orc_build_rows(const orc_grid* g, int flux, int timederiv, double dt,
                             if (code == ORC_DIRC) {
                                 if (flux == ORC_FLUX_SG) {
                                     double wL, wR;
-                                    orc_sg_face(vb, vb, kb, kb, 0.5 * dx, &wL, &wR);
-                                    if (side == 0) R7(0, c) -= wR / dx; /* F = wL g + wR u */
-                                    else R7(0, c) += wL / dx;           /* F = wL u + wR g */
+                                    orc_sg_face(vb, vb, kb, kb, 0.5 * wc, &wL, &wR);
+                                    if (side == 0) R7(0, c) -= wR / wc; /* F = wL g + wR u */
+                                    else R7(0, c) += wL / wc;           /* F = wL u + wR g */
                                 } else {
-                                    R7(0, c) += 2.0 * kb / (dx * dx);
-                                    if (side == 0 && vb < 0.0) R7(0, c) -= vb / dx;
-                                    if (side == 1 && vb > 0.0) R7(0, c) += vb / dx;
+                                    R7(0, c) += 2.0 * kb / (wc * wc);
+                                    if (side == 0 && vb < 0.0) R7(0, c) -= vb / wc;
+                                    if (side == 1 && vb > 0.0) R7(0, c) += vb / wc;
                                 }
                             } else if (code == ORC_ZGRD) {
-                                if (side == 0) R7(0, c) -= vb / dx;
-                                else R7(0, c) += vb / dx;
+                                if (side == 0) R7(0, c) -= vb / wc;
+                                else R7(0, c) += vb / wc;
                             }
                         }
                     }
@@ -962,6 +1105,14 @@ void orc_build_rows(const orc_grid* g, int flux, int timederiv, double dt,
                 R7(0, c) -= reac[GX(i, j, k)];
                 if (timederiv) R7(0, c) += 1.0 / dt;
             }
+}
+
+void orc_build_rows(const orc_grid* g, int flux, int timederiv, double dt,
+                    const double* vel, const double* dcoeff, const double* reac,
+                    const int* bc, double* rows)
+{
+    geo3 G = geo_fine(g);
+    build_rows_geo(&G, flux, timederiv, dt, vel, dcoeff, reac, bc, rows);
 }
 
 void orc_build_rhs(const orc_grid* g, int flux, const double* vel, const double* dcoeff,
@@ -1064,6 +1215,7 @@ struct orc_mg {
     int bc[6];
     int nlev;
     dims3 d[32];
+    geo3 geo[32];
     double* rows[32];
     double* u[32];
     double* f[32];
@@ -1090,6 +1242,7 @@ orc_mg* orc_mg_create(const orc_grid* g, int flux, int timederiv, double dt,
     mg->g = *g;
     memcpy(mg->bc, bc, sizeof(int) * 6);
     dims3 d = {g->lx, g->ly, g->lz};
+    geo3 G = geo_fine(g);
     long ng = ngh(d.lx, d.ly, d.lz);
     double* v = zalloc(3 * ng);
     double* kc = zalloc(ng);
@@ -1099,13 +1252,14 @@ orc_mg* orc_mg_create(const orc_grid* g, int flux, int timederiv, double dt,
     memcpy(rc, reac, sizeof(double) * ng);
     int l = 0;
     for (;;) {
-        orc_grid gl = *g;
-        gl.lx = d.lx; gl.ly = d.ly; gl.lz = d.lz;
         long n = nin(d.lx, d.ly, d.lz);
         mg->d[l] = d;
+        mg->geo[l] = G;
         mg->rows[l] = zalloc(7 * n);
-        orc_build_rows(&gl, flux, timederiv, dt, v, kc, rc, bc, mg->rows[l]);
+        build_rows_geo(&G, flux, timederiv, dt, v, kc, rc, bc, mg->rows[l]);
         if (transpose) {
+            orc_grid gl = *g;
+            gl.lx = d.lx; gl.ly = d.ly; gl.lz = d.lz;
             double* t = zalloc(7 * n);
             orc_rows_transpose(&gl, bc, mg->rows[l], t);
             free(mg->rows[l]);
@@ -1115,17 +1269,18 @@ orc_mg* orc_mg_create(const orc_grid* g, int flux, int timederiv, double dt,
         mg->f[l] = zalloc(n);
         mg->r[l] = zalloc(n);
         if (is_coarsest(g, d) || l == 31) break;
-        dims3 c = coarse_dims(g, d);
+        geo3 Gc = geo_coarse(g, G);
+        dims3 c = {Gc.n[0], Gc.n[1], Gc.n[2]};
         long ngc = ngh(c.lx, c.ly, c.lz);
         double* vc = zalloc(3 * ngc);
         double* kcc = zalloc(ngc);
         double* rcc = zalloc(ngc);
-        for (int q = 0; q < 3; q++) restrict_field(g, d, c, v + q * ng, 1, vc + q * ngc, 1);
-        restrict_field(g, d, c, kc, 1, kcc, 1);
-        restrict_field(g, d, c, rc, 1, rcc, 1);
+        for (int q = 0; q < 3; q++) restrict_fieldg(g, &G, &Gc, v + q * ng, 1, vc + q * ngc, 1);
+        restrict_fieldg(g, &G, &Gc, kc, 1, kcc, 1);
+        restrict_fieldg(g, &G, &Gc, rc, 1, rcc, 1);
         free(v); free(kc); free(rc);
         v = vc; kc = kcc; rc = rcc;
-        d = c; ng = ngc; l++;
+        d = c; G = Gc; ng = ngc; l++;
     }
     free(v); free(kc); free(rc);
     mg->nlev = l + 1;
@@ -1238,7 +1393,7 @@ static void mg_rec(orc_mg* mg, int l, double* u, const double* f)
     for (long c = 0; c < n; c++) r[c] = f[c] - r[c];
     double* fc = mg->f[l + 1];
     double* uc = mg->u[l + 1];
-    restrict_field(&mg->g, fd, cd, r, 0, fc, 0);
+    restrict_fieldg(&mg->g, &mg->geo[l], &mg->geo[l + 1], r, 0, fc, 0);
     memset(uc, 0, sizeof(double) * nc);
     mg_rec(mg, l + 1, uc, fc);
     /* ghosted copy of the coarse correction with the prolongation ghosts:
@@ -1260,7 +1415,7 @@ static void mg_rec(orc_mg* mg, int l, double* u, const double* f)
     ghost_update(cd, eg, mg->bc, (const double* const*)zb);
     long ngf = ngh(fd.lx, fd.ly, fd.lz);
     double* ef = zalloc(ngf);
-    prolong(cell, fd, cd, eg, ef);
+    prolongg(&mg->g, &mg->geo[l], &mg->geo[l + 1], mg->bc, eg, ef);
     {
         int lx = fd.lx, ly = fd.ly;
         for (int k = 1; k <= fd.lz; k++)

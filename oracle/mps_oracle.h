@@ -12,7 +12,8 @@
  *       V-cycle / GMRES bottom solve), each function citing the reference
  *       file:line it follows;
  *   (B) extensions the reference does not have (periodic faces, the
- *       ceil-coarsening "uniform" hierarchy, Scharfetter-Gummel rows taken
+ *       "geom" hierarchy for any size (ceil coarsening, exact cell widths,
+ *       trilinear prolongation), Scharfetter-Gummel rows taken
  *       from the 1D code, transposed operators, right-preconditioned FGMRES),
  *       built on an explicit 7-point row representation and checked against
  *       layer (A) where the two overlap.
@@ -33,15 +34,15 @@ extern "C" {
  * codes of discretepde.f90 ('DIRC','FLUX','ZGRD'); PERI is an extension. */
 enum { ORC_LEFT = 0, ORC_RIGHT, ORC_BOTTOM, ORC_TOP, ORC_BACK, ORC_FRONT };
 enum { ORC_DIRC = 1, ORC_FLUX = 2, ORC_ZGRD = 3, ORC_PERI = 4, ORC_DZGD = 5 };
-enum { ORC_HIER_CELL = 0, ORC_HIER_UNIFORM = 1 };
+enum { ORC_HIER_CELL = 0, ORC_HIER_GEOM = 1 };
 enum { ORC_FLUX_UPWIND = 0, ORC_FLUX_SG = 1 };
 
 typedef struct {
     int lx, ly, lz;                 /* cells per direction */
     double llenx, lleny, llenz;     /* physical lengths */
     int px, py, pz;                 /* rank layout (CELL hierarchy coarsest rule) */
-    int hier;                       /* ORC_HIER_CELL or ORC_HIER_UNIFORM */
-    int max_coarse;                 /* UNIFORM: coarsen while cells > max_coarse */
+    int hier;                       /* ORC_HIER_CELL or ORC_HIER_GEOM */
+    int max_coarse;                 /* GEOM: coarsen while cells > max_coarse */
     int nu1, nu2;                   /* pre/post smoothing sweeps (reference: 2,2) */
 } orc_grid;
 

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "_build", "libmps_oracle.so")
 
 HIER_CELL = 0
-HIER_UNIFORM = 1
+HIER_GEOM = 1
 
 
 def build():
@@ -200,7 +200,7 @@ def sg_face(cL, cR, DL, DR, dx):
 class RowsMG:
     """Correction-scheme V-cycle over explicit 7-point rows (extension layer)."""
 
-    def __init__(self, prob, hier=HIER_UNIFORM, ranks=(1, 1, 1), max_coarse=125, nu1=2, nu2=2,
+    def __init__(self, prob, hier=HIER_GEOM, ranks=(1, 1, 1), max_coarse=125, nu1=2, nu2=2,
                  transpose=False, flux=None):
         self.prob = prob
         self._g = _grid(prob, hier, ranks, max_coarse, nu1, nu2)
