@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""Benchmark: 257^3 plasma-Poisson solves/s to 1e-10 relative residual.
+
+Workload (the headline configuration): 257^3 cells on a 1 cm cube, relative
+permittivity 1 in the gas and 4 in a 10-cell dielectric slab at z=0,
+Dirichlet 0 V (z=0) and 1000 V (z=1), periodic x/y, right-hand side
+e(n_i - n_e)/eps0 with lognormal densities (seeded synthetic stand-in).
+
+One step = one complete solve from a zero initial guess to
+||b - A x||_2 / ||b||_2 <= 1e-10, operator setup included, inputs resident in
+HBM.  ``value`` is the mixed-precision solve (FP32 V-cycles inside FP64
+refinement); the plain FP64 V-cycle solve is timed beside it (``fp64``).
+``e2e`` repeats the mixed solve through the host C ABI (mps_linsolve) with
+pinned host buffers, host<->device copies inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU (torchrun); the solve does not shard, every
+rank solves its own replica (weak scaling), time = max over ranks.
+--impl reference times the CPU restatement of the reference's own V-cycle
+(perform_vcycle, oracle port) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+import numpy as np  # noqa: E402
+
+METRIC = "257³ Poisson solves/s @1e-10 rel. residual: mixed vs FP64 GPU; HBM GB/s"
+UNIT = "solves/s"
+N_DEFAULT = 257
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def workload_config(n, extra=None):
+    cfg = {
+        "workload": f"plasma Poisson {n}^3 cells, 1 cm cube, eps_r 1 / 4 (10-cell slab at z=0), "
+                    f"Dirichlet 0 V / 1000 V on z, periodic x/y, e(n_i-n_e)/eps0 lognormal(ln 1e16, 1)",
+        "cells": n ** 3,
+        "tol_rel_residual": 1e-10,
+        "hierarchy": "geom (l/2, odd cell merged, trilinear prolongation), RB-GS 2/2, coarsest <=125 cells dense",
+        "initial_guess": "zero",
+        "l2": "no flush: inputs (>=7 fields of 139 MB) exceed the 126 MB L2",
+        "parallelism": "replicas",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def oracle_cpu_sample(n, cycles, problem=None):
+    """Consecutive V-cycles of the FP64 restatement of perform_vcycle (the
+    reference hierarchy, mgridlib/mgridsteps.f90:384-579) on the full problem,
+    OpenMP over all host cores.  Returns (seconds per cycle list, rel-residual
+    history, cycles needed to reach 1e-10 at the measured asymptotic rate)."""
+    from mps3d_b200 import workloads as W
+    from oracle import oracle as orc
+
+    p = problem or W.plasma_poisson(n)
+    x = p.zeros_ghosted()
+    b = orc.find_bvec(p)
+    bn = np.linalg.norm(b)
+    times, rel = [], []
+    for _ in range(cycles):
+        t0 = time.perf_counter()
+        rms = orc.vcycle(p, x)
+        times.append(time.perf_counter() - t0)
+        # the reference's RMS residual is sqrt(sum r^2 / N): relative L2 = rms*sqrt(N)/||b||
+        rel.append(rms * np.sqrt(p.ncells) / bn)
+    # iterations to 1e-10 from the measured history (asymptotic rate = last ratio)
+    if rel[-1] <= 1e-10:
+        need = next(i + 1 for i, r in enumerate(rel) if r <= 1e-10)
+    else:
+        rate = rel[-1] / rel[-2] if len(rel) > 1 else 0.5
+        rate = min(max(rate, 1e-6), 0.999)
+        need = len(rel) + int(np.ceil(np.log(1e-10 / rel[-1]) / np.log(rate)))
+    return times, rel, need
+
+
+def reference_twin(n):
+    """The reference's cell-centred hierarchy halves sizes by integer division
+    (mgridsteps.f90:21-23) and drops the odd cell; on 2^k+1 sizes with periodic
+    faces its V-cycle diverges, so the reference is timed on the power-of-two
+    twin (same box, same physics, n-1 cells per direction)."""
+    return n - 1 if n % 2 == 1 else n
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    n = args.n
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    from mps3d_b200 import workloads as W
+
+    nt = reference_twin(n)
+    p = W.plasma_poisson(nt)
+    times, rel, need = oracle_cpu_sample(nt, args.warmup + args.steps, problem=p)
+    t_cycle = float(np.mean(times[args.warmup:])) if args.steps > 0 else float(np.mean(times))
+    value = 1.0 / (t_cycle * need)
+    sample = (f"{args.steps} timed V-cycles (after {args.warmup}) of the FP64 restatement of perform_vcycle on the "
+              f"{nt}^3 power-of-two twin of the {n}^3 problem (the reference hierarchy diverges on odd periodic "
+              f"sizes), {cores} OpenMP threads; {t_cycle:.3f} s/cycle x {need} cycles to 1e-10 (rate measured "
+              f"from the same cycles)")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_cycle * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(n, {"reference_twin_cells": nt ** 3,
+                                      "hierarchy": "reference CELL (l/2 integer division), RB-GS 2/2, GMRES bottom"}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_rel_residual_history": rel,
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def colour_pass_bytes(cells, s, coeff_field):
+    """Algorithmic bytes of one red-black colour pass (red/black split layout):
+    read the other colour (N/2 words), read f of the colour (N/2), write the
+    colour (N/2), plus the cell coefficient k of both colours (N) when the
+    operator has one (FP64 k in the FP64 hierarchy, FP32 k in the mixed one)."""
+    b = 1.5 * cells * s
+    if coeff_field == 1:
+        b += cells * s
+    return b
+
+
+def vcycle_bytes(levels_cells, s, coeff_field, nu=4):
+    """Algorithmic bytes of one V-cycle: per level nu*2 colour passes, the
+    fused residual+restriction (read u, f, k; write N/8) and the fused
+    prolongation+correction (read N/8, read+write u)."""
+    tot = 0.0
+    for i, n in enumerate(levels_cells[:-1]):
+        tot += 2 * nu * colour_pass_bytes(n, s, coeff_field)
+        tot += (2 * n + (n if coeff_field == 1 else 0) + n / 8.0) * s
+        tot += (2 * n + n / 8.0) * s
+    return tot
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from mps3d_b200 import capi, solver, workloads as W
+
+    assert torch.cuda.is_available(), "bench needs a CUDA device"
+    dev = local if ws > 1 else 0
+    torch.cuda.set_device(dev)
+    n = args.n
+    p = W.plasma_poisson(n)
+    dp = solver.DeviceProblem(p, device=f"cuda:{dev}")
+    h = capi.Handle(dev)
+    x = torch.zeros(p.ghost_shape, dtype=torch.float64, device=f"cuda:{dev}")
+    common = dict(tol=1e-10, maxit=60)
+
+    def solve(prec):
+        x.zero_()
+        _, info = solver.linsolve_dev(dp, x, handle=h, precision=prec, **common)
+        if info["status"] != 0:
+            raise RuntimeError(f"solve failed: {info} {h.last_error()}")
+        return info
+
+    # warm-up (also allocates the workspace of both precisions)
+    for _ in range(max(args.warmup, 0)):
+        solve("mixed")
+        solve("fp64")
+    torch.cuda.synchronize()
+
+    def timed(prec, profile=False):
+        h.set_profile(profile)
+        h.get_profile(reset=True)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        infos = []
+        with ClockSampler(dev) as cs:
+            e0.record()
+            for _ in range(args.steps):
+                infos.append(solve(prec))
+            e1.record()
+            torch.cuda.synchronize()
+        barrier(ws)
+        ms = e0.elapsed_time(e1)
+        prof = h.get_profile(reset=True)
+        h.set_profile(False)
+        return dist_max(ms, ws), infos, cs.summary(), prof
+
+    ms_mixed, inf_mixed, clk, prof = timed("mixed", profile=True)
+    ms_fp64, inf_fp64, clk64, prof64 = timed("fp64", profile=True)
+    per_mixed = ms_mixed / args.steps
+    per_fp64 = ms_fp64 / args.steps
+    value = ws * 1e3 / per_mixed
+    fp64_value = ws * 1e3 / per_fp64
+
+    # level cell counts of the geometric hierarchy (l/2 per direction, stop at <=125)
+    lev, d = [], [n, n, n]
+    while True:
+        lev.append(d[0] * d[1] * d[2])
+        if lev[-1] <= 125:
+            break
+        d = [max(1, q // 2) for q in d]
+
+    hbm_peak, peak_kind = load_peaks()
+    # roofline of the dominant kernel: finest-level colour pass, mixed solve
+    cells = n ** 3
+    cf = 1 if prof.coeff_field == 1 else 0
+    s32 = prof.precision_bytes or 4
+    cp_ms = prof.ms[capi.PROF_SMOOTH] / max(prof.count[capi.PROF_SMOOTH], 1)
+    cp_bytes = colour_pass_bytes(cells, s32, cf)
+    achieved = cp_bytes / (cp_ms * 1e-3) / 1e9
+    cp64_ms = prof64.ms[capi.PROF_SMOOTH] / max(prof64.count[capi.PROF_SMOOTH], 1)
+    achieved64 = colour_pass_bytes(cells, 8, cf) / (cp64_ms * 1e-3) / 1e9
+    # whole-solve algorithmic GB/s (V-cycles + outer FP64 residual/update)
+    it_m = inf_mixed[-1]["iters"]
+    vc_m = inf_mixed[-1]["vcycles"]
+    solve_bytes_m = vc_m * vcycle_bytes(lev, 4, cf) + (it_m + 1) * (3 * 8 + 4) * cells + it_m * (4 + 16) * cells
+    it_d = inf_fp64[-1]["iters"]
+    solve_bytes_d = it_d * vcycle_bytes(lev, 8, cf) + (it_d + 1) * 3 * 8 * cells
+    gbs_m = solve_bytes_m / (per_mixed * 1e-3) / 1e9
+    gbs_d = solve_bytes_d / (per_fp64 * 1e-3) / 1e9
+
+    # ---- end to end through the host C ABI (pinned host buffers) ----
+    e2e = None
+    if not args.skip_e2e:
+        import ctypes as C
+
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        h_dc, h_src = pin(p.dcoeff), pin(p.source)
+        h_x = torch.zeros(p.ghost_shape, dtype=torch.float64).pin_memory()
+        h_bc = [pin(v) for v in p.bcvals]
+        bcv = (C.c_void_p * 6)(*[C.c_void_p(t.data_ptr()) for t in h_bc])
+        o = solver.make_opts(precision="mixed", **common)
+        g = solver._grid(p)
+        bcc = (C.c_int * 6)(*p.bc)
+
+        def host_solve():
+            h_x.zero_()
+            info = capi.Info()
+            st = h._lib.mps_linsolve(h.h, C.byref(g), 0, 1.0, None, C.c_void_p(h_dc.data_ptr()), None,
+                                     C.c_void_p(h_src.data_ptr()), bcc, bcv, None, C.c_void_p(h_x.data_ptr()),
+                                     C.byref(o), C.byref(info))
+            if st != 0:
+                raise RuntimeError(f"host solve failed {st} {h.last_error()}")
+            return info
+
+        host_solve()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            host_solve()
+        torch.cuda.synchronize()
+        t_e2e = dist_max(time.perf_counter() - t0, ws)
+        ghost = int(np.prod(p.ghost_shape)) * 8
+        faces = sum(int(v.size) for i, v in enumerate(p.bcvals) if p.bc[i] in (1, 2)) * 8
+        e2e = {"value": ws * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 3 * ghost + faces,
+               "d2h_bytes_per_step": ghost}
+        # check the host-path answer against the device-path answer
+        dx = (h_x.to(x.device) - x).abs().max().item() / max(x.abs().max().item(), 1e-300)
+
+    # ---- CPU baseline: the oracle port on the host cores (rank 0, N=1) ----
+    cpu = None
+    if rank == 0 and ws == 1 and not args.skip_cpu:
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        nt = reference_twin(n)
+        times, rel, need = oracle_cpu_sample(nt, args.cpu_cycles, problem=W.plasma_poisson(nt) if nt != n else p)
+        t_cycle = float(np.mean(times[1:] if len(times) > 1 else times))
+        cpu = {"value": 1.0 / (t_cycle * need), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{len(times)} V-cycles of the FP64 restatement of perform_vcycle on the {nt}^3 power-of-two "
+                         f"twin of the {n}^3 problem ({cores} OpenMP threads), {t_cycle:.3f} s/cycle x {need} "
+                         f"cycles to 1e-10 at the measured rate"}
+
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "colour_pass_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        traffic = tj.get("bytes_per_launch_257")
+
+    launches = inf_mixed[-1]["launches"]
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "mixed: f32 V-cycle, f64 residual/update", "data": "synthetic",
+        "config": workload_config(n, {"iters_mixed": it_m, "vcycles_mixed": vc_m, "iters_fp64": it_d}),
+        "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": per_fp64, "dtype": "f64",
+                 "hbm_gbs_solve": gbs_d, "clocks": clk64},
+        "mixed_over_fp64": fp64_value and value / fp64_value,
+        "hbm_gbs_solve": gbs_m,
+        "hbm_frac_solve": gbs_m / hbm_peak,
+        "fp64_hbm_frac_solve": gbs_d / hbm_peak,
+        "roofline": {"bound": "hbm", "kernel": "k_colour (finest-level red/black pass, FP32, mixed solve)",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "peak_kind": peak_kind, "traffic": traffic, "bytes_per_launch": cp_bytes,
+                     "launch_ms": cp_ms, "fp64_achieved": achieved64, "fp64_frac": achieved64 / hbm_peak},
+        "clocks": clk,
+        "gpu_launches": launches * args.steps,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "final_rel_residual": inf_mixed[-1]["rel_res"],
+    }
+    if e2e is not None:
+        out["e2e_vs_device_max_rel_diff"] = dx
+    if rank == 0:
+        print(json.dumps(out))
+    h.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-cycles", type=int, default=3)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, ws, rank)
+        return run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

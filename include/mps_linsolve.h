@@ -98,7 +98,24 @@ typedef struct {
     double rms_res;      /* final sqrt(sum r^2 / ncells), the reference's norm */
     double rel_res0;     /* initial relative residual */
     double time_ms;      /* device time of the solve (CUDA events) */
+    int launches;        /* kernels launched by the solve */
 } mps_solve_info;
+
+/* per-kernel-class device time of the finest level, accumulated over solves
+ * while profiling is on (CUDA events around each launch on the handle's
+ * stream) */
+enum { MPS_PROF_SMOOTH = 0,   /* red-black colour passes, finest level */
+       MPS_PROF_RESTRICT = 1, /* fused residual + restriction, finest level */
+       MPS_PROF_PROLONG = 2,  /* fused prolongation + correction, finest level */
+       MPS_PROF_RESID = 3,    /* FP64 residual + norm of the outer iteration */
+       MPS_PROF_NCLASS = 8 };
+typedef struct {
+    int count[MPS_PROF_NCLASS];
+    double ms[MPS_PROF_NCLASS];
+    int precision_bytes;  /* word size of the V-cycle (8 FP64, 4 mixed) */
+    int coeff_field;      /* 1 when the finest-level operator reads a cell coefficient field */
+    long long cells;      /* finest-level cells */
+} mps_profile;
 
 typedef struct mps_handle_s* mps_handle;
 
@@ -157,6 +174,11 @@ int mps_find_bvec_dev(mps_handle h, const mps_grid* g, const double* vel, const 
                       const double* source, const int bc_code[6], const double* const bcval[6],
                       const double* mgridsterm, double* b, const mps_solver_opts* opts,
                       void* stream);
+
+/* Profiling of the finest-level kernels (off by default).  mps_get_profile
+ * returns the accumulated figures and resets them when reset != 0. */
+int mps_set_profile(mps_handle h, int on);
+int mps_get_profile(mps_handle h, mps_profile* p, int reset);
 
 /* Ghost layer of a ghosted field per update_boundary_ghostvalues (+ periodic
  * wrap), device pointers. */

@@ -35,8 +35,15 @@ TOL_RMS_ABS, TOL_REL_L2 = 0, 1
 EXPORTS = [
     "mps_default_opts", "mps_version", "mps_create", "mps_destroy", "mps_stream", "mps_last_error",
     "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once", "mps_apply_A_dev", "mps_find_bvec_dev",
-    "mps_fill_ghosts_dev",
+    "mps_fill_ghosts_dev", "mps_set_profile", "mps_get_profile",
 ]
+
+PROF_SMOOTH, PROF_RESTRICT, PROF_PROLONG, PROF_RESID, PROF_NCLASS = 0, 1, 2, 3, 8
+
+
+class Profile(C.Structure):
+    _fields_ = [("count", C.c_int * 8), ("ms", C.c_double * 8), ("precision_bytes", C.c_int),
+                ("coeff_field", C.c_int), ("cells", C.c_longlong)]
 
 
 class Grid(C.Structure):
@@ -57,7 +64,7 @@ class Opts(C.Structure):
 class Info(C.Structure):
     _fields_ = [("status", C.c_int), ("iters", C.c_int), ("vcycles", C.c_int), ("levels", C.c_int),
                 ("rel_res", C.c_double), ("rms_res", C.c_double), ("rel_res0", C.c_double),
-                ("time_ms", C.c_double)]
+                ("time_ms", C.c_double), ("launches", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -98,7 +105,9 @@ def load(build_if_missing: bool = False):
                                   C.POINTER(Opts), vp]
     L.mps_find_bvec_dev.argtypes = [vp, C.POINTER(Grid), vp, vp, vp, ip, C.POINTER(vp), vp, vp, C.POINTER(Opts), vp]
     L.mps_fill_ghosts_dev.argtypes = [vp, C.POINTER(Grid), ip, C.POINTER(vp), vp, vp]
-    for name in ("mps_create", "mps_destroy", "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once",
+    L.mps_set_profile.argtypes = [vp, C.c_int]
+    L.mps_get_profile.argtypes = [vp, C.POINTER(Profile), C.c_int]
+    for name in ("mps_set_profile", "mps_get_profile", "mps_create", "mps_destroy", "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once",
                  "mps_apply_A_dev", "mps_find_bvec_dev", "mps_fill_ghosts_dev"):
         getattr(L, name).restype = C.c_int
     _lib = L
@@ -149,6 +158,14 @@ class Handle:
     @property
     def stream(self) -> int:
         return self._lib.mps_stream(self.h) or 0
+
+    def set_profile(self, on: bool):
+        self._lib.mps_set_profile(self.h, int(bool(on)))
+
+    def get_profile(self, reset=True) -> Profile:
+        p = Profile()
+        self._lib.mps_get_profile(self.h, C.byref(p), int(bool(reset)))
+        return p
 
     def last_error(self) -> str:
         r = self._lib.mps_last_error(self.h)

@@ -43,6 +43,7 @@ struct Err {
     } while (0)
 #define CKL()                                                                                      \
     do {                                                                                           \
+        ctx.launches++;                                                                            \
         cudaError_t e_ = cudaGetLastError();                                                       \
         if (e_ != cudaSuccess) {                                                                   \
             ctx.err.code = MPS_ERR_CUDA;                                                           \
@@ -91,8 +92,21 @@ struct Signature {
     bool operator==(const Signature& o) const { return std::memcmp(this, &o, sizeof(Signature)) == 0; }
 };
 
+struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> cls;
+    int used = 0;
+    int count[MPS_PROF_NCLASS] = {};
+    double ms[MPS_PROF_NCLASS] = {};
+    int precision_bytes = 8, coeff_field = 0;
+    long long cells = 0;
+};
+
 struct Ctx {
     int dev = 0;
+    long long launches = 0;
+    Prof prof;
     cudaStream_t s = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     Err err;
@@ -276,6 +290,42 @@ static Split<T> split(T* base, const Lev& L)
     return s;
 }
 
+// ---- finest-level profiling (events around launches on the handle's stream) ----
+static void prof_begin(Ctx& ctx, int cls)
+{
+    Prof& P = ctx.prof;
+    if (!P.on) return;
+    if (P.used + 2 > (int)P.ev.size()) {
+        for (int q = 0; q < 256; q++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return;
+            P.ev.push_back(e);
+        }
+    }
+    cudaEventRecord(P.ev[P.used], ctx.s);
+    P.cls.push_back(cls);
+}
+static void prof_end(Ctx& ctx)
+{
+    Prof& P = ctx.prof;
+    if (!P.on || P.cls.size() * 2 != (size_t)P.used + 2) return;
+    cudaEventRecord(P.ev[P.used + 1], ctx.s);
+    P.used += 2;
+}
+static void prof_collect(Ctx& ctx)  // after a stream synchronize
+{
+    Prof& P = ctx.prof;
+    for (size_t q = 0; q < P.cls.size() && (int)(2 * q + 1) < P.used; q++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, P.ev[2 * q], P.ev[2 * q + 1]) == cudaSuccess) {
+            P.ms[P.cls[q]] += ms;
+            P.count[P.cls[q]]++;
+        }
+    }
+    P.cls.clear();
+    P.used = 0;
+}
+
 // ---- one colour pass ----
 template <class T, class Op>
 static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zero_state)
@@ -286,6 +336,7 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     const T* fh = H.F[l] + (c ? L.half : 0);
     if (c == 0) out = H.U[l][H.ri[l] ^ 1];
     else out = H.U[l][H.bi[l] ^ 1] + L.half;
+    if (l == 0) prof_begin(ctx, MPS_PROF_SMOOTH);
     if (zero_state == 2) {  // whole state zero
         k_colour<T, Op, ZeroU<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh);
     } else if (zero_state == 1) {  // colour c zero, other colour valid
@@ -296,6 +347,7 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     } else {
         k_colour<T, Op, CSplit<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, ccur(H, L, l), out, fh);
     }
+    if (l == 0) prof_end(ctx);
     CKL();
     if (c == 0) H.ri[l] ^= 1;
     else H.bi[l] ^= 1;
@@ -329,12 +381,16 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         CK(cudaMemsetAsync(H.U[l][H.ri[l]], 0, sizeof(T) * L.half, ctx.s));
         CK(cudaMemsetAsync(H.U[l][H.bi[l]] + L.half, 0, sizeof(T) * L.half, ctx.s));
     }
+    if (l == 0) prof_begin(ctx, MPS_PROF_RESTRICT);
     k_resid_restrict<T, Op><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
         L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom);
+    if (l == 0) prof_end(ctx);
     CKL();
     if ((st = vcycle_rec(ctx, H, ops, l + 1, o, true))) return st;
+    if (l == 0) prof_begin(ctx, MPS_PROF_PROLONG);
     k_prolong_correct<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
         L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l]);
+    if (l == 0) prof_end(ctx);
     CKL();
     for (int s = 0; s < o->nu2; s++) {
         if ((st = colour_pass(ctx, H, ops[l], l, 0, 0))) return st;
@@ -355,7 +411,9 @@ template <class T, class Op, class R>
 static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R> rout)
 {
     const Lev& L = ctx.lev[0];
+    prof_begin(ctx, MPS_PROF_RESID);
     k_resid_norm<T, Op, R><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, op, u, f, rout, ctx.rb);
+    prof_end(ctx);
     CKL();
     return 0;
 }
@@ -563,6 +621,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     const Lev& L0 = ctx.lev[0];
     const double dtinv = timederiv ? 1.0 / dt : 0.0;
 
+    const long long launches0 = ctx.launches;
     CK(cudaEventRecord(ctx.e0, ctx.s));
     // ---- operator detection (one small device->host read) ----
     unsigned long long* dm = ctx.dmax;
@@ -930,6 +989,13 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     CK(cudaStreamSynchronize(ctx.s));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx.e0, ctx.e1));
+    if (ctx.prof.on) {
+        prof_collect(ctx);
+        ctx.prof.precision_bytes = mixed ? 4 : 8;
+        ctx.prof.coeff_field = sig.opclass == 0 ? !sig.kuni : 7;
+        ctx.prof.cells = ncell;
+    }
+    inf.launches = (int)(ctx.launches - launches0);
     inf.iters = it;
     inf.vcycles = vcycles;
     inf.levels = nl;
@@ -1005,6 +1071,7 @@ int mps_destroy(mps_handle h)
     cudaStreamSynchronize(ctx.s);
     ctx.ar.clear();
     ctx.inbuf.clear();
+    for (cudaEvent_t e : ctx.prof.ev) cudaEventDestroy(e);
     if (ctx.dmax) cudaFree(ctx.dmax);
     if (ctx.hpin) cudaFreeHost(ctx.hpin);
     if (ctx.e0) cudaEventDestroy(ctx.e0);
@@ -1048,6 +1115,27 @@ static int run_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, co
     }
     if (st && info) info->status = st;
     return st;
+}
+
+int mps_set_profile(mps_handle h, int on)
+{
+    if (!h) return MPS_ERR_BAD_ARG;
+    h->ctx.prof.on = on != 0;
+    return MPS_OK;
+}
+
+int mps_get_profile(mps_handle h, mps_profile* p, int reset)
+{
+    if (!h || !p) return MPS_ERR_BAD_ARG;
+    Prof& P = h->ctx.prof;
+    std::memset(p, 0, sizeof(*p));
+    for (int c = 0; c < MPS_PROF_NCLASS; c++) { p->count[c] = P.count[c]; p->ms[c] = P.ms[c]; }
+    p->precision_bytes = P.precision_bytes;
+    p->coeff_field = P.coeff_field;
+    p->cells = P.cells;
+    if (reset)
+        for (int c = 0; c < MPS_PROF_NCLASS; c++) { P.count[c] = 0; P.ms[c] = 0.0; }
+    return MPS_OK;
 }
 
 int mps_linsolve_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel,
