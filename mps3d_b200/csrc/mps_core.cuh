@@ -57,6 +57,9 @@ struct Lev {
     int bc[6];        // BC codes LEFT..FRONT
     double w[3], wl[3];
     double cr[3], cl[3], cp[3], dr[3], dlast[3];
+    int fast_lo[3], fast_hi[3];  // index range per axis where a row has six
+                                 // neighbours of the other colour at regular
+                                 // spacing (interior fast path)
     FastDiv divP, divNy;
     unsigned rows;    // ny*nz
 };
@@ -77,8 +80,15 @@ __host__ __device__ __forceinline__ double cwidth(const Lev& L, int ax, int i)
     return i == lev_n(L, ax) - 1 ? L.wl[ax] : L.w[ax];
 }
 
+// one entry of a 1-D prolongation table: e_f = (1-t) e[j0] + t e[j1]
+struct Lin {
+    int j0, j1;
+    double t;
+};
+
 // transfer between level l (fine) and l+1 (coarse)
 struct Xfer {
+    const Lin* tab[3];  // per-axis tables over the fine index (geometric hierarchy)
     int geom;         // 0: the reference's CELL transfers, 1: geometric
     int nf[3], nc[3];
     double rf[3], Rc[3];  // wl_f / w_f and wl_c / w_f
@@ -125,6 +135,7 @@ struct CSplit {
     {
         return __ldg(&c[scol(i, j, k)][soff(L, i, j, k)]);
     }
+    __device__ __forceinline__ T at(int col, int off) const { return __ldg(&c[col][off]); }
 };
 
 // neighbour along axis ax (0..2), direction s (-1/+1); returns false at a
@@ -216,6 +227,65 @@ __device__ __forceinline__ void row_eval(const ROp<T>& op, const Lev& L, const U
     }
     diag = d;
     off = o;
+}
+
+// interior fast path: the six neighbours of (i,j,k) have the other colour and
+// sit at 32-bit offsets o+q-1, o+q (x), o-+P (y), o-+P*ny (z) of the other
+// half, q = i&1; all faces have the regular coefficient cr.
+__device__ __forceinline__ bool is_fast(const Lev& L, int i, int j, int k)
+{
+    return i >= L.fast_lo[0] && i <= L.fast_hi[0] && j >= L.fast_lo[1] && j <= L.fast_hi[1] &&
+           k >= L.fast_lo[2] && k <= L.fast_hi[2];
+}
+
+template <class T, class U>
+__device__ __forceinline__ void row_eval_fast(const KOp<T>& op, const Lev& L, const U& u, int i, int j, int k,
+                                              T& diag, T& off)
+{
+    const int cc = (i + j + k) & 1, oc = cc ^ 1;
+    const int o = (i >> 1) + L.P * (j + L.ny * k);
+    const int q = i & 1, sy = L.P, sz = L.P * L.ny;
+    const int n0 = o + q - 1, n1 = o + q, n2 = o - sy, n3 = o + sy, n4 = o - sz, n5 = o + sz;
+    const T cx = (T)L.cr[0], cy = (T)L.cr[1], cz = (T)L.cr[2];
+    const T d0 = op.dex[0] ? __ldg(&op.dex[cc][o]) : op.dexc;
+    const T u0 = u.at(oc, n0), u1 = u.at(oc, n1), u2 = u.at(oc, n2), u3 = u.at(oc, n3), u4 = u.at(oc, n4),
+            u5 = u.at(oc, n5);
+    if (op.k[0]) {
+        const T* ko = op.k[oc];
+        const T kc = __ldg(&op.k[cc][o]);
+        const T w0 = (kc + __ldg(&ko[n0])) * cx, w1 = (kc + __ldg(&ko[n1])) * cx;
+        const T w2 = (kc + __ldg(&ko[n2])) * cy, w3 = (kc + __ldg(&ko[n3])) * cy;
+        const T w4 = (kc + __ldg(&ko[n4])) * cz, w5 = (kc + __ldg(&ko[n5])) * cz;
+        diag = d0 + T(0.5) * (((w0 + w1) + (w2 + w3)) + (w4 + w5));
+        off = T(-0.5) * (((w0 * u0 + w1 * u1) + (w2 * u2 + w3 * u3)) + (w4 * u4 + w5 * u5));
+    } else {
+        const T kc = op.kc;
+        diag = d0 + T(2) * kc * ((cx + cy) + cz);
+        off = -kc * ((cx * (u0 + u1) + cy * (u2 + u3)) + cz * (u4 + u5));
+    }
+}
+
+template <class T, class U>
+__device__ __forceinline__ void row_eval_fast(const ROp<T>& op, const Lev& L, const U& u, int i, int j, int k,
+                                              T& diag, T& off)
+{
+    const int cc = (i + j + k) & 1, oc = cc ^ 1;
+    const int o = (i >> 1) + L.P * (j + L.ny * k);
+    const int q = i & 1, sy = L.P, sz = L.P * L.ny;
+    diag = __ldg(&op.r[0][cc][o]);
+    off = ((__ldg(&op.r[1][cc][o]) * u.at(oc, o + q - 1) + __ldg(&op.r[2][cc][o]) * u.at(oc, o + q)) +
+           (__ldg(&op.r[3][cc][o]) * u.at(oc, o - sy) + __ldg(&op.r[4][cc][o]) * u.at(oc, o + sy))) +
+          (__ldg(&op.r[5][cc][o]) * u.at(oc, o - sz) + __ldg(&op.r[6][cc][o]) * u.at(oc, o + sz));
+}
+
+// dispatch: fast path in the interior, general path at boundaries, periodic
+// seams and next to a non-uniform last cell
+template <class T, class Op, class U>
+__device__ __forceinline__ void row_any(const Op& op, const Lev& L, const U& u, int i, int j, int k, T& diag,
+                                        T& off)
+{
+    if (is_fast(L, i, j, k)) row_eval_fast(op, L, u, i, j, k, diag, off);
+    else row_eval(op, L, u, i, j, k, diag, off);
 }
 
 // red-black Gauss-Seidel point update u_c = (f_c - offdiag)/diag

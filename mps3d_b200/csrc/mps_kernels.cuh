@@ -12,6 +12,7 @@ constexpr int TPB = 256;
 template <class T>
 struct ZeroU {  // accessor of a field known to be zero
     __device__ __forceinline__ T get(const Lev&, int, int, int) const { return T(0); }
+    __device__ __forceinline__ T at(int, int) const { return T(0); }
 };
 template <class T>
 struct OtherOnlyU {  // colour c known zero, the other colour read from memory
@@ -21,6 +22,7 @@ struct OtherOnlyU {  // colour c known zero, the other colour read from memory
     {
         return scol(i, j, k) == c ? T(0) : __ldg(&other[soff(L, i, j, k)]);
     }
+    __device__ __forceinline__ T at(int col, int off) const { return col == c ? T(0) : __ldg(&other[off]); }
 };
 
 // ---------------------------------------------------------------------
@@ -39,7 +41,7 @@ __global__ void __launch_bounds__(TPB) k_colour(Lev L, Op op, int c, U u, T* __r
     int i, j, k;
     if (!decode(L, t, c, i, j, k)) return;
     T diag, off;
-    row_eval(op, L, u, i, j, k, diag, off);
+    row_any<T>(op, L, u, i, j, k, diag, off);
     out[t] = gs_value(__ldg(&f[t]), diag, off);
 }
 
@@ -78,7 +80,7 @@ __global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> 
                 const int i = lo[0] + di;
                 const T wx = geom ? (T)cwidth(F, 0, i) : T(1);
                 T diag, off;
-                row_eval(op, F, u, i, j, k, diag, off);
+                row_any<T>(op, F, u, i, j, k, diag, off);
                 T r = f.get(F, i, j, k) - (diag * u.get(F, i, j, k) + off);
                 const T v = wx * wy * wz;
                 s += v * r;
@@ -155,26 +157,25 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
         const T dz = coarse_at(C, e, I, J, K + 1) - coarse_at(C, e, I, J, K - 1);
         v = e0 + ((ax * dx + ay * dy) + az * dz);
     } else {
-        int a0[3], a1[3];
-        double tt[3];
-        geom_lin(X, 0, (int)i, a0[0], a1[0], tt[0]);
-        geom_lin(X, 1, (int)j, a0[1], a1[1], tt[1]);
-        geom_lin(X, 2, (int)k, a0[2], a1[2], tt[2]);
-        v = T(0);
-        for (int cz = 0; cz < 2; cz++) {
-            const T wz = (T)(cz ? tt[2] : 1.0 - tt[2]);
-            if (wz == T(0)) continue;
-            for (int cy = 0; cy < 2; cy++) {
-                const T wy = (T)(cy ? tt[1] : 1.0 - tt[1]);
-                if (wy == T(0)) continue;
-                for (int cx = 0; cx < 2; cx++) {
-                    const T wx = (T)(cx ? tt[0] : 1.0 - tt[0]);
-                    if (wx == T(0)) continue;
-                    v += wz * wy * wx *
-                         coarse_at(C, e, cx ? a1[0] : a0[0], cy ? a1[1] : a0[1], cz ? a1[2] : a0[2]);
-                }
-            }
+        const Lin lx = X.tab[0][i], ly = X.tab[1][j], lz = X.tab[2][k];
+        const T tx = (T)lx.t, ty = (T)ly.t, tz = (T)lz.t;
+        const bool inner = lx.j0 >= 0 && lx.j1 < C.nx && ly.j0 >= 0 && ly.j1 < C.ny && lz.j0 >= 0 && lz.j1 < C.nz;
+        T c000, c100, c010, c110, c001, c101, c011, c111;
+        if (inner) {
+            c000 = e.get(C, lx.j0, ly.j0, lz.j0); c100 = e.get(C, lx.j1, ly.j0, lz.j0);
+            c010 = e.get(C, lx.j0, ly.j1, lz.j0); c110 = e.get(C, lx.j1, ly.j1, lz.j0);
+            c001 = e.get(C, lx.j0, ly.j0, lz.j1); c101 = e.get(C, lx.j1, ly.j0, lz.j1);
+            c011 = e.get(C, lx.j0, ly.j1, lz.j1); c111 = e.get(C, lx.j1, ly.j1, lz.j1);
+        } else {
+            c000 = coarse_at(C, e, lx.j0, ly.j0, lz.j0); c100 = coarse_at(C, e, lx.j1, ly.j0, lz.j0);
+            c010 = coarse_at(C, e, lx.j0, ly.j1, lz.j0); c110 = coarse_at(C, e, lx.j1, ly.j1, lz.j0);
+            c001 = coarse_at(C, e, lx.j0, ly.j0, lz.j1); c101 = coarse_at(C, e, lx.j1, ly.j0, lz.j1);
+            c011 = coarse_at(C, e, lx.j0, ly.j1, lz.j1); c111 = coarse_at(C, e, lx.j1, ly.j1, lz.j1);
         }
+        const T x00 = c000 + tx * (c100 - c000), x10 = c010 + tx * (c110 - c010);
+        const T x01 = c001 + tx * (c101 - c001), x11 = c011 + tx * (c111 - c011);
+        const T y0 = x00 + ty * (x10 - x00), y1 = x01 + ty * (x11 - x01);
+        v = y0 + tz * (y1 - y0);
     }
     T* p = &u.c[scol(i, j, k)][soff(F, i, j, k)];
     *p = *p + v;
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(TPB) k_resid_norm(Lev L, Op op, CSplit<T> u, C
         int i, j, k;
         if (t < total && decode(L, t, c, i, j, k)) {
             T diag, off;
-            row_eval(op, L, u, i, j, k, diag, off);
+            row_any<T>(op, L, u, i, j, k, diag, off);
             T fv = __ldg(&f.c[c][t]);
             T r = fv - (diag * __ldg(&u.c[c][t]) + off);
             rr += (double)r * (double)r;

@@ -110,13 +110,19 @@ struct Ctx {
     cudaStream_t s = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     Err err;
-    Arena ar;       // grid-dependent workspace
+    Arena ar;       // grid-dependent workspace (both precisions)
+    Arena kar;      // Krylov basis (FGMRES), keyed by (length, restart)
+    long long kar_n = 0;
+    int kar_m = 0;
     Arena inbuf;    // host-API staging of the inputs
     size_t inbuf_bytes = 0;
     Signature sig;
     int nlev = 0;
     Lev lev[MAXL];
     Xfer xf[MAXL];
+    Lin* dtab = nullptr;      // device prolongation tables of the current plan
+    size_t dtab_n = 0;
+    std::vector<Lin> htab;
     // FP64 coefficient pyramid (split cell fields)
     double* pk[MAXL] = {};
     double* preac[MAXL] = {};
@@ -180,6 +186,10 @@ static Lev make_lev(int nx, int ny, int nz, const double w[3], const double wl[3
         L.cp[a] = 1.0 / (dl * ww);
         L.dr[a] = 2.0 / (ww * ww);
         L.dlast[a] = 2.0 / (wwl * wwl);
+        // fast path: not on a boundary/seam cell, not the last cell or its
+        // neighbour when the last cell's width differs
+        L.fast_lo[a] = 1;
+        L.fast_hi[a] = n[a] - 2 - (wwl != ww ? 1 : 0);
     }
     L.divP.init((unsigned)L.P);
     L.divNy.init((unsigned)ny);
@@ -470,7 +480,7 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
         for (int a = 0; a < 3; a++) ctx.pv[a][l] = sig.opclass == 1 ? (double*)ctx.ar.get(b64) : nullptr;
         ok = ok && ctx.pk[l];
         if (sig.opclass == 1) {
-            ctx.rows64[l] = (need64 || l == 0) ? (double*)ctx.ar.get(7 * b64) : nullptr;
+            ctx.rows64[l] = (need64 || l == 0) ? (double*)ctx.ar.get(7 * b64) : nullptr;  // l>0: FP64 solves
             ctx.rows32[l] = need32 ? (float*)ctx.ar.get(7 * b32) : nullptr;
         } else {
             ctx.k32[l] = (need32 && !sig.kuni) ? (float*)ctx.ar.get(b32) : nullptr;
@@ -491,25 +501,6 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
     ctx.rb.partial = (double*)ctx.ar.get(sizeof(double) * 2 * (maxb + 1));
     ctx.rb.counter = (unsigned*)ctx.ar.get(sizeof(unsigned) * 4);
     ctx.rb.out = (double*)ctx.ar.get(sizeof(double) * 4);
-    if (sig.krylov == MPS_KRYLOV_FGMRES) {
-        const int m = sig.restart;
-        const size_t n = 2 * L0.half;
-        ctx.V = (double*)ctx.ar.get(sizeof(double) * n * (m + 1));
-        ctx.Z = ctx.ar.get((need32 ? sizeof(float) : sizeof(double)) * n * m);
-        ctx.w = (double*)ctx.ar.get(sizeof(double) * n);
-        ctx.hcol = (double*)ctx.ar.get(sizeof(double) * 2 * (m + 2));
-        ctx.Vptr = (double**)ctx.ar.get(sizeof(double*) * (m + 2));
-        ctx.mdot_blocks = 592;
-        ctx.dpart = (double*)ctx.ar.get(sizeof(double) * (m + 2) * ctx.mdot_blocks);
-        ok = ok && ctx.V && ctx.Z && ctx.w && ctx.hcol && ctx.Vptr && ctx.dpart;
-        if (ok) {
-            std::vector<double*> hp(m + 2);
-            for (int j = 0; j <= m; j++) hp[j] = ctx.V + (size_t)j * n;
-            hp[m + 1] = ctx.w;
-            if (cudaMemcpy(ctx.Vptr, hp.data(), sizeof(double*) * (m + 2), cudaMemcpyHostToDevice) != cudaSuccess)
-                ok = false;
-        }
-    }
     ok = ok && ctx.x64 && ctx.b64 && ctx.dense && ctx.gjM && ctx.dstatus && ctx.rb.partial && ctx.rb.counter &&
          ctx.rb.out;
     if (!ok) {
@@ -518,7 +509,45 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
         ctx.err.msg = "device allocation failed";
         return MPS_ERR_NOMEM;
     }
+    // the arena zeroes new blocks with cudaMemset on the legacy stream; the
+    // solver's stream does not synchronise with it, so wait here
+    if (cudaDeviceSynchronize() != cudaSuccess) return MPS_ERR_CUDA;
     ctx.sig = sig;
+    return 0;
+}
+
+// FGMRES basis: V (m+1 FP64 vectors), Z (m preconditioned vectors, FP32 in
+// mixed precision), w, the Hessenberg column and the dot-product partials
+static int setup_krylov(Ctx& ctx, long long n, int m)
+{
+    if (ctx.kar_n == n && ctx.kar_m == m) return 0;
+    ctx.kar.clear();
+    ctx.kar_n = 0;
+    ctx.kar_m = 0;
+    bool ok = true;
+    ctx.V = (double*)ctx.kar.get(sizeof(double) * n * (m + 1));
+    ctx.Z = ctx.kar.get(sizeof(double) * n * m);
+    ctx.w = (double*)ctx.kar.get(sizeof(double) * n);
+    ctx.hcol = (double*)ctx.kar.get(sizeof(double) * 2 * (m + 2));
+    ctx.Vptr = (double**)ctx.kar.get(sizeof(double*) * (m + 2));
+    ctx.mdot_blocks = 592;
+    ctx.dpart = (double*)ctx.kar.get(sizeof(double) * (m + 2) * ctx.mdot_blocks);
+    ok = ctx.V && ctx.Z && ctx.w && ctx.hcol && ctx.Vptr && ctx.dpart;
+    if (ok) {
+        std::vector<double*> hp(m + 2);
+        for (int j = 0; j <= m; j++) hp[j] = ctx.V + (size_t)j * n;
+        hp[m + 1] = ctx.w;
+        if (cudaMemcpy(ctx.Vptr, hp.data(), sizeof(double*) * (m + 2), cudaMemcpyHostToDevice) != cudaSuccess)
+            ok = false;
+    }
+    if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
+        ctx.kar.clear();
+        ctx.err.code = MPS_ERR_NOMEM;
+        ctx.err.msg = "device allocation failed (Krylov basis)";
+        return MPS_ERR_NOMEM;
+    }
+    ctx.kar_n = n;
+    ctx.kar_m = m;
     return 0;
 }
 
@@ -619,6 +648,37 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     if (nl < 1) { ctx.err.msg = why; return MPS_ERR_BAD_ARG; }
     ctx.nlev = nl;
     const Lev& L0 = ctx.lev[0];
+    {  // 1-D prolongation tables of the geometric transfers
+        size_t total = 0;
+        for (int l = 0; l + 1 < nl; l++)
+            for (int a = 0; a < 3; a++) total += ctx.xf[l].nf[a];
+        std::vector<Lin> tab(total > 0 ? total : 1);
+        size_t pos = 0;
+        for (int l = 0; l + 1 < nl; l++)
+            for (int a = 0; a < 3; a++) {
+                for (int i = 0; i < ctx.xf[l].nf[a]; i++) {
+                    Lin e;
+                    geom_lin(ctx.xf[l], a, i, e.j0, e.j1, e.t);
+                    tab[pos + i] = e;
+                }
+                pos += ctx.xf[l].nf[a];
+            }
+        if (tab.size() > ctx.dtab_n) {
+            if (ctx.dtab) cudaFree(ctx.dtab);
+            ctx.dtab = nullptr;
+            ctx.dtab_n = 0;
+            CK(cudaMalloc((void**)&ctx.dtab, sizeof(Lin) * tab.size()));
+            ctx.dtab_n = tab.size();
+        }
+        ctx.htab.swap(tab);
+        CK(cudaMemcpyAsync(ctx.dtab, ctx.htab.data(), sizeof(Lin) * ctx.htab.size(), cudaMemcpyHostToDevice, ctx.s));
+        pos = 0;
+        for (int l = 0; l + 1 < nl; l++)
+            for (int a = 0; a < 3; a++) {
+                ctx.xf[l].tab[a] = ctx.dtab + pos;
+                pos += ctx.xf[l].nf[a];
+            }
+    }
     const double dtinv = timederiv ? 1.0 / dt : 0.0;
 
     const long long launches0 = ctx.launches;
@@ -664,16 +724,19 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     sig.max_coarse = o->hierarchy == MPS_HIER_GEOM ? o->max_coarse : 0;
     sig.opclass = (o->transpose == 0 && o->flux == MPS_FLUX_UPWIND && maxvel == 0.0) ? 0 : 1;
     if (o->flux == MPS_FLUX_UPWIND && maxvel == 0.0) sig.opclass = 0;  // symmetric: A^T = A
-    sig.prec = o->precision;
-    sig.krylov = o->krylov;
-    sig.restart = o->krylov == MPS_KRYLOV_FGMRES ? o->restart : 0;
+    sig.prec = 0;
+    sig.krylov = 0;
+    sig.restart = 0;
     sig.has_reac = maxreac > 0.0;
     sig.kuni = dkvar == 0.0;
     sig.transpose = o->transpose && sig.opclass == 1;
     const bool mixed = o->precision == MPS_PREC_MIXED;
+    // both hierarchies stay allocated (switching precision costs no allocation);
+    // only the one this solve uses is filled
+    int st = setup_workspace(ctx, sig, o, 1, 1);
     const int need64 = !mixed, need32 = mixed;
-    int st = setup_workspace(ctx, sig, o, need64, need32);
     if (st) return st;
+    if (o->krylov == MPS_KRYLOV_FGMRES && (st = setup_krylov(ctx, 2 * ctx.lev[0].half, o->restart))) return st;
 
     // ---- coefficient pyramid (FP64) ----
     k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.dcoeff, split<double>(ctx.pk[0], L0), 1.0, 0.0);
@@ -734,7 +797,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         if (need32) set_kop<float>(ctx, ctx.h32.kop, ctx.k32, ctx.dex32, k0, dtinv, sig.kuni, sig.has_reac);
     } else {
         for (int l = 0; l < nl; l++) {
-            if (ctx.rows64[l]) {
+            if (ctx.rows64[l] && (need64 || l == 0)) {
                 // transposed rows need a scratch copy of the forward rows: use rows32's
                 // FP64-sized neighbour (x64 is large enough only at level 0), so build into
                 // the FGMRES-free scratch: the dense matrix buffer is too small; allocate once
@@ -746,7 +809,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 if (tmp) CK(cudaFreeAsync(tmp, ctx.s));
                 if (need64) ctx.h64.rop[l] = make_rop<double>(ctx.rows64[l], ctx.lev[l]);
             }
-            if (ctx.rows32[l]) {
+            if (ctx.rows32[l] && need32) {
                 float* tmp = nullptr;
                 if (sig.transpose) {
                     CK(cudaMallocAsync((void**)&tmp, sizeof(float) * 7 * 2 * ctx.lev[l].half, ctx.s));
@@ -1070,8 +1133,10 @@ int mps_destroy(mps_handle h)
     cudaSetDevice(ctx.dev);
     cudaStreamSynchronize(ctx.s);
     ctx.ar.clear();
+    ctx.kar.clear();
     ctx.inbuf.clear();
     for (cudaEvent_t e : ctx.prof.ev) cudaEventDestroy(e);
+    if (ctx.dtab) cudaFree(ctx.dtab);
     if (ctx.dmax) cudaFree(ctx.dmax);
     if (ctx.hpin) cudaFreeHost(ctx.hpin);
     if (ctx.e0) cudaEventDestroy(ctx.e0);
@@ -1169,6 +1234,7 @@ static int run_host(mps_handle h, const mps_grid* g, int timederiv, double dt, c
         ctx.inbuf.clear();
         ctx.inbuf_bytes = 0;
         if (!ctx.inbuf.get(need)) return MPS_ERR_NOMEM;
+        if (cudaDeviceSynchronize() != cudaSuccess) return MPS_ERR_CUDA;
         ctx.inbuf_bytes = need;
     }
     double* base = (double*)ctx.inbuf.blocks[0];
