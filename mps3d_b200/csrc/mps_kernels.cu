@@ -15,8 +15,14 @@ __global__ void k_gj_prepare(int n, const double* A, double* M)
     }
 }
 
-__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* M, double* AinvT, int* status)
+__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* Mg, double* AinvT, int* status, int smem)
 {
+    extern __shared__ double Ms[];
+    double* M = smem ? Ms : Mg;
+    if (smem) {
+        for (long long t = threadIdx.x; t < 2LL * n * n; t += blockDim.x) Ms[t] = Mg[t];
+        __syncthreads();
+    }
     __shared__ double sval[32];
     __shared__ int sidx[32];
     __shared__ double fac[1024];

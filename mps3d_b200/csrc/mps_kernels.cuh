@@ -254,7 +254,8 @@ __global__ void k_dense_assemble(Lev L, Op op, double* A)
 // Gauss-Jordan inverse with partial pivoting of the n x n row-major A held in
 // M = [A | I] (n x 2n, row major, prepared by k_gj_prepare); writes the
 // inverse column-major to AinvT.  One CTA; status[0] |= 1 on a zero pivot.
-__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* M, double* AinvT, int* status);
+// smem=1: the augmented matrix is staged in dynamic shared memory (small n)
+__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* M, double* AinvT, int* status, int smem);
 __global__ void k_gj_prepare(int n, const double* A, double* M);
 
 // ---------------------------------------------------------------------

@@ -103,10 +103,34 @@ struct Prof {
     long long cells = 0;
 };
 
+// a captured iteration, replayed with cudaGraphLaunch; keyed by everything
+// that is baked into its kernel parameters
+struct GraphKey {
+    Signature sig;
+    int kind = -1, prec = -1, inner = 0, nu1 = 0, nu2 = 0, nlev = 0, flux = 0, transpose = 0;
+    double kc = 0, dexc = 0;
+    const void* ws = nullptr;  // workspace identity (first arena block)
+    bool operator==(const GraphKey& o) const
+    {
+        return sig == o.sig && kind == o.kind && prec == o.prec && inner == o.inner && nu1 == o.nu1 &&
+               nu2 == o.nu2 && nlev == o.nlev && flux == o.flux && transpose == o.transpose && kc == o.kc &&
+               dexc == o.dexc && ws == o.ws;
+    }
+};
+struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+    std::vector<cudaEvent_t> ev;  // profiling event-record nodes (pairs)
+    std::vector<int> cls;
+};
+
 struct Ctx {
     int dev = 0;
     long long launches = 0;
     Prof prof;
+    std::vector<GraphEntry> graphs;
+    GraphEntry* capturing = nullptr;
     cudaStream_t s = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     Err err;
@@ -305,6 +329,15 @@ static void prof_begin(Ctx& ctx, int cls)
 {
     Prof& P = ctx.prof;
     if (!P.on) return;
+    if (ctx.capturing) {  // event-record node inside the graph being captured
+        GraphEntry& G = *ctx.capturing;
+        cudaEvent_t a;
+        if (cudaEventCreate(&a) != cudaSuccess) return;
+        G.ev.push_back(a);
+        G.cls.push_back(cls);
+        cudaEventRecordWithFlags(a, ctx.s, cudaEventRecordExternal);
+        return;
+    }
     if (P.used + 2 > (int)P.ev.size()) {
         for (int q = 0; q < 256; q++) {
             cudaEvent_t e;
@@ -318,10 +351,42 @@ static void prof_begin(Ctx& ctx, int cls)
 static void prof_end(Ctx& ctx)
 {
     Prof& P = ctx.prof;
-    if (!P.on || P.cls.size() * 2 != (size_t)P.used + 2) return;
+    if (!P.on) return;
+    if (ctx.capturing) {
+        GraphEntry& G = *ctx.capturing;
+        if (G.ev.size() != 2 * G.cls.size() - 1) return;
+        cudaEvent_t b;
+        if (cudaEventCreate(&b) != cudaSuccess) return;
+        G.ev.push_back(b);
+        cudaEventRecordWithFlags(b, ctx.s, cudaEventRecordExternal);
+        return;
+    }
+    if (P.cls.size() * 2 != (size_t)P.used + 2) return;
     cudaEventRecord(P.ev[P.used + 1], ctx.s);
     P.used += 2;
 }
+// after a synchronize that followed a replay of G: add its event pairs
+static void prof_collect_graph(Ctx& ctx, const GraphEntry& G)
+{
+    Prof& P = ctx.prof;
+    if (!P.on) return;
+    for (size_t q = 0; q < G.cls.size() && 2 * q + 1 < G.ev.size(); q++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, G.ev[2 * q], G.ev[2 * q + 1]) == cudaSuccess) {
+            P.ms[G.cls[q]] += ms;
+            P.count[G.cls[q]]++;
+        }
+    }
+}
+static void destroy_graphs(Ctx& ctx)
+{
+    for (GraphEntry& G : ctx.graphs) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        for (cudaEvent_t e : G.ev) cudaEventDestroy(e);
+    }
+    ctx.graphs.clear();
+}
+
 static void prof_collect(Ctx& ctx)  // after a stream synchronize
 {
     Prof& P = ctx.prof;
@@ -334,6 +399,60 @@ static void prof_collect(Ctx& ctx)  // after a stream synchronize
     }
     P.cls.clear();
     P.used = 0;
+}
+
+// Replay the captured graph for `key`, capturing `body` first when needed.
+// Graphs hold kernel parameters (buffer pointers, operator constants) by
+// value; the red/black buffer parities return to their start after an even
+// number of sweeps per level, which the callers guarantee.  Returns the entry.
+template <class F>
+static int run_graph(Ctx& ctx, const GraphKey& key, GraphEntry** out, F&& body)
+{
+    GraphEntry* G = nullptr;
+    for (GraphEntry& e : ctx.graphs)
+        if (e.key == key) { G = &e; break; }
+    if (!G) {
+        if (ctx.graphs.size() >= 16) destroy_graphs(ctx);
+        ctx.graphs.emplace_back();
+        G = &ctx.graphs.back();
+        G->key = key;
+        cudaGraph_t graph = nullptr;
+        const long long l0 = ctx.launches;
+        if (cudaStreamBeginCapture(ctx.s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            ctx.graphs.pop_back();
+            ctx.err.msg = "stream capture failed to start";
+            return MPS_ERR_CUDA;
+        }
+        ctx.capturing = G;
+        int st = body();
+        ctx.capturing = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(ctx.s, &graph);
+        if (st || ce != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            for (cudaEvent_t e : G->ev) cudaEventDestroy(e);
+            ctx.graphs.pop_back();
+            cudaGetLastError();
+            if (!st) { ctx.err.msg = std::string("stream capture: ") + cudaGetErrorString(ce); st = MPS_ERR_CUDA; }
+            return st;
+        }
+        G->kernels = (int)(ctx.launches - l0);
+        ctx.launches = l0;
+        ce = cudaGraphInstantiate(&G->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+            for (cudaEvent_t e : G->ev) cudaEventDestroy(e);
+            ctx.graphs.pop_back();
+            ctx.err.msg = std::string("graph instantiate: ") + cudaGetErrorString(ce);
+            return MPS_ERR_CUDA;
+        }
+    }
+    if (cudaGraphLaunch(G->exec, ctx.s) != cudaSuccess) {
+        ctx.err.msg = "graph launch failed";
+        return MPS_ERR_CUDA;
+    }
+    ctx.launches += G->kernels;
+    *out = G;
+    return 0;
 }
 
 // ---- one colour pass ----
@@ -467,6 +586,7 @@ static void alloc_hier(Ctx& ctx, Hier<T>& H, bool& ok)
 static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts* o, int need64, int need32)
 {
     if (sig == ctx.sig) return 0;
+    destroy_graphs(ctx);
     ctx.ar.clear();
     ctx.sig = Signature();
     bool ok = true;
@@ -521,6 +641,7 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
 static int setup_krylov(Ctx& ctx, long long n, int m)
 {
     if (ctx.kar_n == n && ctx.kar_m == m) return 0;
+    destroy_graphs(ctx);
     ctx.kar.clear();
     ctx.kar_n = 0;
     ctx.kar_m = 0;
@@ -606,7 +727,17 @@ static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
     CKL();
     k_gj_prepare<<<nblk(2LL * n * n), TPB, 0, ctx.s>>>(n, ctx.dense, ctx.gjM);
     CKL();
-    k_gauss_jordan<<<1, 1024, 0, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus);
+    const size_t smem = sizeof(double) * 2 * (size_t)n * n;
+    if (smem <= 200 * 1024) {
+        static bool attr = false;
+        if (!attr) {
+            CK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            attr = true;
+        }
+        k_gauss_jordan<<<1, 1024, smem, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus, 1);
+    } else {
+        k_gauss_jordan<<<1, 1024, 0, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus, 0);
+    }
     CKL();
     return 0;
 }
@@ -855,22 +986,58 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     Split<double> no64;
     no64.c[0] = no64.c[1] = nullptr;
 
+    GraphKey gk;
+    gk.sig = sig;
+    gk.prec = mixed;
+    gk.nu1 = o->nu1;
+    gk.nu2 = o->nu2;
+    gk.nlev = nl;
+    gk.flux = o->flux;
+    gk.transpose = o->transpose;
+    gk.kc = sig.kuni ? k0 : 0.0;
+    gk.dexc = sig.has_reac ? 0.0 : dtinv;
+    gk.ws = ctx.ar.blocks.empty() ? nullptr : ctx.ar.blocks[0];
+    // graphs need the buffer parities to return after one iteration
+    const bool graphs = o->use_graph && ((o->nu1 + o->nu2) % 2 == 0);
+
     if (o->krylov == MPS_KRYLOV_NONE && !mixed) {
         // FP64 stationary V-cycle iteration on h64 (x lives in level-0 U)
         Hier<double>& H = ctx.h64;
         CK(cudaMemcpyAsync(H.U[0][0], ctx.x64, sizeof(double) * n2, cudaMemcpyDeviceToDevice, ctx.s));
         CK(cudaMemcpyAsync(H.F[0], ctx.b64, sizeof(double) * n2, cudaMemcpyDeviceToDevice, ctx.s));
-        H.ri[0] = H.bi[0] = 0;
+        for (int l = 0; l < nl; l++) H.ri[l] = H.bi[l] = 0;
+        auto residual = [&]() -> int {
+            if (sig.opclass == 0) return resid_norm(ctx, H.kop[0], ccur(H, L, 0), csplit<double>(H.F[0], L), no64);
+            return resid_norm(ctx, H.rop[0], ccur(H, L, 0), csplit<double>(H.F[0], L), no64);
+        };
+        auto iteration = [&]() -> int {
+            int s2 = vcycle(ctx, H, sig.opclass, o, false);
+            if (s2) return s2;
+            return residual();
+        };
+        if ((st = residual())) return st;
         for (;;) {
-            if (sig.opclass == 0) st = resid_norm(ctx, H.kop[0], ccur(H, L, 0), csplit<double>(H.F[0], L), no64);
-            else st = resid_norm(ctx, H.rop[0], ccur(H, L, 0), csplit<double>(H.F[0], L), no64);
-            if (st) return st;
             if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
             if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
             norms(ctx.hpin[0], ctx.hpin[1]);
             if (it == 0) inf.rel_res0 = rel;
             if (ref_norm_only ? it >= o->maxit : (conv() || it >= o->maxit)) break;
-            if ((st = vcycle(ctx, H, sig.opclass, o, false))) return st;
+            if (graphs) {
+                gk.kind = 1;
+                GraphEntry* G = nullptr;
+                for (;;) {  // each replay ends with the residual norms of the new iterate
+                    if ((st = run_graph(ctx, gk, &G, iteration))) return st;
+                    if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+                    prof_collect_graph(ctx, *G);
+                    vcycles++;
+                    it++;
+                    if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
+                    norms(ctx.hpin[0], ctx.hpin[1]);
+                    if (ref_norm_only ? it >= o->maxit : (conv() || it >= o->maxit)) break;
+                }
+                break;
+            }
+            if ((st = iteration())) return st;
             vcycles++;
             it++;
         }
@@ -882,31 +1049,54 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         // FP64 defect correction with FP32 V-cycles
         Hier<float>& H = ctx.h32;
         const int inner = o->inner_cycles > 0 ? o->inner_cycles : 2;
-        for (;;) {
+        for (int l = 0; l < nl; l++) H.ri[l] = H.bi[l] = 0;
+        gk.inner = inner;
+        auto residual = [&]() -> int {
             Split<float> r32 = split<float>(H.F[0], L);
             if (sig.opclass == 0)
-                st = resid_norm(ctx, ctx.kop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
-            else
-                st = resid_norm(ctx, ctx.rop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
-            if (st) return st;
-            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
-            if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
-            norms(ctx.hpin[0], ctx.hpin[1]);
-            if (it == 0) inf.rel_res0 = rel;
-            if (conv() || it >= o->maxit) break;
-            for (int c = 0; c < inner; c++) {
-                if ((st = vcycle(ctx, H, sig.opclass, o, c == 0))) return st;
-                vcycles++;
-            }
+                return resid_norm(ctx, ctx.kop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
+            return resid_norm(ctx, ctx.rop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
+        };
+        auto iteration = [&]() -> int {
+            int s2;
+            for (int c = 0; c < inner; c++)
+                if ((s2 = vcycle(ctx, H, sig.opclass, o, c == 0))) return s2;
             const unsigned ab = std::min<unsigned>(nblk(L.half), 4736);
             k_axpy<float, double><<<ab, TPB, 0, ctx.s>>>(L.half, 1.0, H.U[0][H.ri[0]], ctx.x64);
             CKL();
             k_axpy<float, double><<<ab, TPB, 0, ctx.s>>>(L.half, 1.0, H.U[0][H.bi[0]] + L.half, ctx.x64 + L.half);
             CKL();
+            return residual();
+        };
+        if ((st = residual())) return st;
+        for (;;) {
+            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+            if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
+            norms(ctx.hpin[0], ctx.hpin[1]);
+            if (it == 0) inf.rel_res0 = rel;
+            if (conv() || it >= o->maxit) break;
+            if (graphs) {
+                gk.kind = 2;
+                GraphEntry* G = nullptr;
+                for (;;) {  // each replay ends with the residual norms of the new iterate
+                    if ((st = run_graph(ctx, gk, &G, iteration))) return st;
+                    if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+                    prof_collect_graph(ctx, *G);
+                    vcycles += inner;
+                    it++;
+                    if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
+                    norms(ctx.hpin[0], ctx.hpin[1]);
+                    if (conv() || it >= o->maxit) break;
+                }
+                break;
+            }
+            if ((st = iteration())) return st;
+            vcycles += inner;
             it++;
         }
     } else {
         // FGMRES(m), right preconditioned by one V-cycle (FP32 when MIXED)
+        for (int l = 0; l < nl; l++) ctx.h32.ri[l] = ctx.h32.bi[l] = ctx.h64.ri[l] = ctx.h64.bi[l] = 0;
         const int m = o->restart;
         const long long n = n2;
         const unsigned db = ctx.mdot_blocks;
@@ -944,7 +1134,14 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                     Hier<float>& P = ctx.h32;
                     k_cast_field<float><<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, vj, P.F[0], 1.0, 0.0);
                     CKL();
-                    if ((st = vcycle(ctx, P, sig.opclass, o, true))) return st;
+                    if (graphs) {
+                        gk.kind = 3;
+                        GraphEntry* G = nullptr;
+                        if ((st = run_graph(ctx, gk, &G, [&]() { return vcycle(ctx, P, sig.opclass, o, true); })))
+                            return st;
+                    } else if ((st = vcycle(ctx, P, sig.opclass, o, true))) {
+                        return st;
+                    }
                     float* zj = (float*)ctx.Z + (size_t)j * n;
                     CK(cudaMemcpyAsync(zj, P.U[0][P.ri[0]], sizeof(float) * L.half, cudaMemcpyDeviceToDevice, ctx.s));
                     CK(cudaMemcpyAsync(zj + L.half, P.U[0][P.bi[0]] + L.half, sizeof(float) * L.half,
@@ -959,7 +1156,14 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 } else {
                     Hier<double>& P = ctx.h64;
                     CK(cudaMemcpyAsync(P.F[0], vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx.s));
-                    if ((st = vcycle(ctx, P, sig.opclass, o, true))) return st;
+                    if (graphs) {
+                        gk.kind = 4;
+                        GraphEntry* G = nullptr;
+                        if ((st = run_graph(ctx, gk, &G, [&]() { return vcycle(ctx, P, sig.opclass, o, true); })))
+                            return st;
+                    } else if ((st = vcycle(ctx, P, sig.opclass, o, true))) {
+                        return st;
+                    }
                     double* zj = (double*)ctx.Z + (size_t)j * n;
                     CK(cudaMemcpyAsync(zj, P.U[0][P.ri[0]], sizeof(double) * L.half, cudaMemcpyDeviceToDevice, ctx.s));
                     CK(cudaMemcpyAsync(zj + L.half, P.U[0][P.bi[0]] + L.half, sizeof(double) * L.half,
@@ -1132,6 +1336,7 @@ int mps_destroy(mps_handle h)
     Ctx& ctx = h->ctx;
     cudaSetDevice(ctx.dev);
     cudaStreamSynchronize(ctx.s);
+    destroy_graphs(ctx);
     ctx.ar.clear();
     ctx.kar.clear();
     ctx.inbuf.clear();
