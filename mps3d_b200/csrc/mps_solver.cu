@@ -729,11 +729,7 @@ static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
     CKL();
     const size_t smem = sizeof(double) * 2 * (size_t)n * n;
     if (smem <= 200 * 1024) {
-        static bool attr = false;
-        if (!attr) {
-            CK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-            attr = true;
-        }
+        CK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         k_gauss_jordan<<<1, 1024, smem, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus, 1);
     } else {
         k_gauss_jordan<<<1, 1024, 0, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus, 0);
