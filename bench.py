@@ -316,6 +316,8 @@ def run_ours(args, ws, rank, local):
     cells = n ** 3
     cf = 1 if prof.coeff_field == 1 else 0
     s32 = prof.precision_bytes or 4
+    if prof.count[capi.PROF_SMOOTH] == 0 or prof64.count[capi.PROF_SMOOTH] == 0:
+        raise RuntimeError("no finest-level colour-pass timings were recorded")
     cp_ms = prof.ms[capi.PROF_SMOOTH] / max(prof.count[capi.PROF_SMOOTH], 1)
     cp_bytes = colour_pass_bytes(cells, s32, cf)
     achieved = cp_bytes / (cp_ms * 1e-3) / 1e9

@@ -107,13 +107,14 @@ struct Prof {
 // that is baked into its kernel parameters
 struct GraphKey {
     Signature sig;
-    int kind = -1, prec = -1, inner = 0, nu1 = 0, nu2 = 0, nlev = 0, flux = 0, transpose = 0;
+    int kind = -1, prec = -1, inner = 0, nu1 = 0, nu2 = 0, nlev = 0, flux = 0, transpose = 0, prof = 0;
     double kc = 0, dexc = 0;
     const void* ws = nullptr;  // workspace identity (first arena block)
     bool operator==(const GraphKey& o) const
     {
         return sig == o.sig && kind == o.kind && prec == o.prec && inner == o.inner && nu1 == o.nu1 &&
-               nu2 == o.nu2 && nlev == o.nlev && flux == o.flux && transpose == o.transpose && kc == o.kc &&
+               nu2 == o.nu2 && nlev == o.nlev && flux == o.flux && transpose == o.transpose && prof == o.prof &&
+               kc == o.kc &&
                dexc == o.dexc && ws == o.ws;
     }
 };
@@ -993,6 +994,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     gk.kc = sig.kuni ? k0 : 0.0;
     gk.dexc = sig.has_reac ? 0.0 : dtinv;
     gk.ws = ctx.ar.blocks.empty() ? nullptr : ctx.ar.blocks[0];
+    gk.prof = ctx.prof.on;  // profiled graphs carry event-record nodes
     // graphs need the buffer parities to return after one iteration
     const bool graphs = o->use_graph && ((o->nu1 + o->nu2) % 2 == 0);
 
