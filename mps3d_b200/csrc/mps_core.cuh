@@ -120,22 +120,32 @@ struct NatDiv {
     int nx, ny;
 };
 
+// select one of two pointers without indexing a parameter array with a
+// run-time index (which would copy the array to local memory)
+template <class P>
+__host__ __device__ __forceinline__ P sel(const P* two, int c)
+{
+    return c ? two[1] : two[0];
+}
+
 template <class T>
 struct Split {  // a field in split layout: c[0] red half, c[1] black half
     T* c[2];
+    __device__ __forceinline__ T* half(int col) const { return col ? c[1] : c[0]; }
     __device__ __forceinline__ T get(const Lev& L, int i, int j, int k) const
     {
-        return c[scol(i, j, k)][soff(L, i, j, k)];
+        return half(scol(i, j, k))[soff(L, i, j, k)];
     }
 };
 template <class T>
 struct CSplit {
     const T* c[2];
+    __device__ __forceinline__ const T* half(int col) const { return col ? c[1] : c[0]; }
     __device__ __forceinline__ T get(const Lev& L, int i, int j, int k) const
     {
-        return __ldg(&c[scol(i, j, k)][soff(L, i, j, k)]);
+        return __ldg(&half(scol(i, j, k))[soff(L, i, j, k)]);
     }
-    __device__ __forceinline__ T at(int col, int off) const { return __ldg(&c[col][off]); }
+    __device__ __forceinline__ T at(int col, int off) const { return __ldg(&half(col)[off]); }
 };
 
 // neighbour along axis ax (0..2), direction s (-1/+1); returns false at a
@@ -175,117 +185,117 @@ struct ROp {
 template <class T>
 __device__ __forceinline__ T kval(const KOp<T>& op, const Lev& L, int i, int j, int k)
 {
-    return op.k[0] ? __ldg(&op.k[scol(i, j, k)][soff(L, i, j, k)]) : op.kc;
+    return op.k[0] ? __ldg(&sel(op.k, scol(i, j, k))[soff(L, i, j, k)]) : op.kc;
 }
 
-// diag and sum_n a_n u_n of row (i,j,k)
-template <class T, class U>
-__device__ __forceinline__ void row_eval(const KOp<T>& op, const Lev& L, const U& u, int i, int j,
-                                         int k, T& diag, T& off)
+// ---- row evaluation: diag and sum_n a_n u_n of row (i,j,k) ----
+// Branch-light and free of local memory: each face is handled by an
+// axis-templated helper (compile-time field indices, no references or
+// arrays), the neighbour's colour and split offset are computed directly,
+// periodic faces wrap, physical faces add their Dirichlet term.
+
+// neighbour index along AX in direction S, wrapped when periodic; false at a
+// physical boundary
+template <int AX, int S>
+__device__ __forceinline__ bool nbr_idx(const Lev& L, int p, int& q)
 {
-    const T kc = kval(op, L, i, j, k);
-    T d = op.dex[0] ? __ldg(&op.dex[scol(i, j, k)][soff(L, i, j, k)]) : op.dexc;
-    T o = T(0);
-#pragma unroll
-    for (int ax = 0; ax < 3; ax++) {
-        const int p = ax == 0 ? i : (ax == 1 ? j : k);
-#pragma unroll
-        for (int s = -1; s <= 1; s += 2) {
-            int a = i, b = j, c = k;
-            if (nbr(L, ax, s, a, b, c)) {
-                const int q = ax == 0 ? a : (ax == 1 ? b : c);
-                T w = T(0.5) * (kc + kval(op, L, a, b, c)) * (T)fcoef(L, ax, p, q);
-                d += w;
-                o -= w * u.get(L, a, b, c);
-            } else if (L.bc[2 * ax + (s > 0)] == BC_DIRC) {
-                d += kc * (T)dcoef(L, ax, p);
-            }
-        }
+    const int n = AX == 0 ? L.nx : (AX == 1 ? L.ny : L.nz);
+    q = p + S;
+    if (q < 0 || q >= n) {
+        if (!L.per[AX]) return false;
+        q = q < 0 ? n - 1 : 0;
     }
-    diag = d;
-    off = o;
+    return true;
 }
 
-template <class T, class U>
-__device__ __forceinline__ void row_eval(const ROp<T>& op, const Lev& L, const U& u, int i, int j,
-                                         int k, T& diag, T& off)
+template <int AX>
+__device__ __forceinline__ double fcoef_ax(const Lev& L, int p, int q)
 {
-    const int c = scol(i, j, k);
-    const long long o0 = soff(L, i, j, k);
-    T d = __ldg(&op.r[0][c][o0]);
-    T o = T(0);
-#pragma unroll
-    for (int ax = 0; ax < 3; ax++) {
-#pragma unroll
-        for (int s = -1; s <= 1; s += 2) {
-            int a = i, b = j, cc = k;
-            if (nbr(L, ax, s, a, b, cc)) {
-                T w = __ldg(&op.r[1 + 2 * ax + (s > 0)][c][o0]);
-                o += w * u.get(L, a, b, cc);
-            }
-        }
+    const int n = AX == 0 ? L.nx : (AX == 1 ? L.ny : L.nz);
+    return p == n - 1 ? L.cl[AX] : (q == n - 1 ? L.cp[AX] : L.cr[AX]);
+}
+template <int AX>
+__device__ __forceinline__ double dcoef_ax(const Lev& L, int p)
+{
+    const int n = AX == 0 ? L.nx : (AX == 1 ? L.ny : L.nz);
+    return p == n - 1 ? L.dlast[AX] : L.dr[AX];
+}
+
+template <class T, int AX, int S, class U>
+__device__ __forceinline__ void kface(const KOp<T>& op, const Lev& L, const U& u, int i, int j, int k, T kc,
+                                      T& d, T& acc)
+{
+    const int p = AX == 0 ? i : (AX == 1 ? j : k);
+    int q;
+    if (nbr_idx<AX, S>(L, p, q)) {
+        const int a = AX == 0 ? q : i, b = AX == 1 ? q : j, c = AX == 2 ? q : k;
+        const int cn = (a + b + c) & 1;
+        const int on = (a >> 1) + L.P * (b + L.ny * c);
+        const T kn = op.k[0] ? __ldg(&sel(op.k, cn)[on]) : op.kc;
+        const T w = T(0.5) * (kc + kn) * (T)fcoef_ax<AX>(L, p, q);
+        d += w;
+        acc += w * u.at(cn, on);
+    } else if (L.bc[2 * AX + (S > 0 ? 1 : 0)] == BC_DIRC) {
+        d += kc * (T)dcoef_ax<AX>(L, p);
     }
-    diag = d;
-    off = o;
-}
-
-// interior fast path: the six neighbours of (i,j,k) have the other colour and
-// sit at 32-bit offsets o+q-1, o+q (x), o-+P (y), o-+P*ny (z) of the other
-// half, q = i&1; all faces have the regular coefficient cr.
-__device__ __forceinline__ bool is_fast(const Lev& L, int i, int j, int k)
-{
-    return i >= L.fast_lo[0] && i <= L.fast_hi[0] && j >= L.fast_lo[1] && j <= L.fast_hi[1] &&
-           k >= L.fast_lo[2] && k <= L.fast_hi[2];
 }
 
 template <class T, class U>
-__device__ __forceinline__ void row_eval_fast(const KOp<T>& op, const Lev& L, const U& u, int i, int j, int k,
-                                              T& diag, T& off)
+__device__ __forceinline__ void row_eval(const KOp<T>& op, const Lev& L, const U& u, int i, int j, int k,
+                                         T& diag, T& off)
 {
-    const int cc = (i + j + k) & 1, oc = cc ^ 1;
+    const int cc = (i + j + k) & 1;
     const int o = (i >> 1) + L.P * (j + L.ny * k);
-    const int q = i & 1, sy = L.P, sz = L.P * L.ny;
-    const int n0 = o + q - 1, n1 = o + q, n2 = o - sy, n3 = o + sy, n4 = o - sz, n5 = o + sz;
-    const T cx = (T)L.cr[0], cy = (T)L.cr[1], cz = (T)L.cr[2];
-    const T d0 = op.dex[0] ? __ldg(&op.dex[cc][o]) : op.dexc;
-    const T u0 = u.at(oc, n0), u1 = u.at(oc, n1), u2 = u.at(oc, n2), u3 = u.at(oc, n3), u4 = u.at(oc, n4),
-            u5 = u.at(oc, n5);
-    if (op.k[0]) {
-        const T* ko = op.k[oc];
-        const T kc = __ldg(&op.k[cc][o]);
-        const T w0 = (kc + __ldg(&ko[n0])) * cx, w1 = (kc + __ldg(&ko[n1])) * cx;
-        const T w2 = (kc + __ldg(&ko[n2])) * cy, w3 = (kc + __ldg(&ko[n3])) * cy;
-        const T w4 = (kc + __ldg(&ko[n4])) * cz, w5 = (kc + __ldg(&ko[n5])) * cz;
-        diag = d0 + T(0.5) * (((w0 + w1) + (w2 + w3)) + (w4 + w5));
-        off = T(-0.5) * (((w0 * u0 + w1 * u1) + (w2 * u2 + w3 * u3)) + (w4 * u4 + w5 * u5));
-    } else {
-        const T kc = op.kc;
-        diag = d0 + T(2) * kc * ((cx + cy) + cz);
-        off = -kc * ((cx * (u0 + u1) + cy * (u2 + u3)) + cz * (u4 + u5));
+    const T kc = op.k[0] ? __ldg(&sel(op.k, cc)[o]) : op.kc;
+    T d = op.dex[0] ? __ldg(&sel(op.dex, cc)[o]) : op.dexc;
+    T acc = T(0);
+    kface<T, 0, -1>(op, L, u, i, j, k, kc, d, acc);
+    kface<T, 0, 1>(op, L, u, i, j, k, kc, d, acc);
+    kface<T, 1, -1>(op, L, u, i, j, k, kc, d, acc);
+    kface<T, 1, 1>(op, L, u, i, j, k, kc, d, acc);
+    kface<T, 2, -1>(op, L, u, i, j, k, kc, d, acc);
+    kface<T, 2, 1>(op, L, u, i, j, k, kc, d, acc);
+    diag = d;
+    off = -acc;
+}
+
+template <class T, int AX, int S, class U>
+__device__ __forceinline__ void rface(const ROp<T>& op, const Lev& L, const U& u, int i, int j, int k, int cc,
+                                      int o, T& acc)
+{
+    const int p = AX == 0 ? i : (AX == 1 ? j : k);
+    int q;
+    if (nbr_idx<AX, S>(L, p, q)) {
+        const int a = AX == 0 ? q : i, b = AX == 1 ? q : j, c = AX == 2 ? q : k;
+        const int cn = (a + b + c) & 1;
+        const int on = (a >> 1) + L.P * (b + L.ny * c);
+        acc += __ldg(&sel(op.r[1 + 2 * AX + (S > 0 ? 1 : 0)], cc)[o]) * u.at(cn, on);
     }
 }
 
 template <class T, class U>
-__device__ __forceinline__ void row_eval_fast(const ROp<T>& op, const Lev& L, const U& u, int i, int j, int k,
-                                              T& diag, T& off)
+__device__ __forceinline__ void row_eval(const ROp<T>& op, const Lev& L, const U& u, int i, int j, int k,
+                                         T& diag, T& off)
 {
-    const int cc = (i + j + k) & 1, oc = cc ^ 1;
+    const int cc = (i + j + k) & 1;
     const int o = (i >> 1) + L.P * (j + L.ny * k);
-    const int q = i & 1, sy = L.P, sz = L.P * L.ny;
-    diag = __ldg(&op.r[0][cc][o]);
-    off = ((__ldg(&op.r[1][cc][o]) * u.at(oc, o + q - 1) + __ldg(&op.r[2][cc][o]) * u.at(oc, o + q)) +
-           (__ldg(&op.r[3][cc][o]) * u.at(oc, o - sy) + __ldg(&op.r[4][cc][o]) * u.at(oc, o + sy))) +
-          (__ldg(&op.r[5][cc][o]) * u.at(oc, o - sz) + __ldg(&op.r[6][cc][o]) * u.at(oc, o + sz));
+    T acc = T(0);
+    rface<T, 0, -1>(op, L, u, i, j, k, cc, o, acc);
+    rface<T, 0, 1>(op, L, u, i, j, k, cc, o, acc);
+    rface<T, 1, -1>(op, L, u, i, j, k, cc, o, acc);
+    rface<T, 1, 1>(op, L, u, i, j, k, cc, o, acc);
+    rface<T, 2, -1>(op, L, u, i, j, k, cc, o, acc);
+    rface<T, 2, 1>(op, L, u, i, j, k, cc, o, acc);
+    diag = __ldg(&sel(op.r[0], cc)[o]);
+    off = acc;
 }
 
-// dispatch: fast path in the interior, general path at boundaries, periodic
-// seams and next to a non-uniform last cell
+// all stencil kernels evaluate rows through this entry point
 template <class T, class Op, class U>
 __device__ __forceinline__ void row_any(const Op& op, const Lev& L, const U& u, int i, int j, int k, T& diag,
                                         T& off)
 {
-    if (is_fast(L, i, j, k)) row_eval_fast(op, L, u, i, j, k, diag, off);
-    else row_eval(op, L, u, i, j, k, diag, off);
+    row_eval(op, L, u, i, j, k, diag, off);
 }
 
 // red-black Gauss-Seidel point update u_c = (f_c - offdiag)/diag

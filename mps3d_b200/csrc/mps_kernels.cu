@@ -220,7 +220,7 @@ __global__ void k_find_bvec(Lev L, const double* __restrict__ vel, const double*
     }
     v = v + (sterm ? sterm[t] : 0.0);
     v = v + source[gi];
-    b.c[scol(i, j, k)][soff(L, i, j, k)] = v;
+    b.half(scol(i, j, k))[soff(L, i, j, k)] = v;
 }
 
 __global__ void k_restrict_field(Lev F, CSplit<double> in, Lev C, Split<double> out, int geom)
@@ -255,7 +255,7 @@ __global__ void k_restrict_field(Lev F, CSplit<double> in, Lev C, Split<double> 
             }
         }
     }
-    out.c[scol(I, J, K)][soff(C, I, J, K)] = geom ? s / vol : s * (1.0 / vol);
+    out.half(scol(I, J, K))[soff(C, I, J, K)] = geom ? s / vol : s * (1.0 / vol);
 }
 
 __global__ void k_multidot(long long n, int m, const double* const* __restrict__ V, const double* __restrict__ w,

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> 
         }
     }
     const int ci = I, cj = J, ck = K;
-    fc.c[scol(ci, cj, ck)][soff(C, ci, cj, ck)] = geom ? s / vol : s * (T(1) / vol);
+    fc.half(scol(ci, cj, ck))[soff(C, ci, cj, ck)] = geom ? s / vol : s * (T(1) / vol);
 }
 
 // coarse ghost rule for the correction (update_boundary_ghostvalues applied
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
         const T y0 = x00 + ty * (x10 - x00), y1 = x01 + ty * (x11 - x01);
         v = y0 + tz * (y1 - y0);
     }
-    T* p = &u.c[scol(i, j, k)][soff(F, i, j, k)];
+    T* p = &u.half(scol(i, j, k))[soff(F, i, j, k)];
     *p = *p + v;
 }
 
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(512) k_coarse_solve(Lev C, const double* __res
         double acc = 0.0;
         for (int q = 0; q < n; q++) acc += AinvT[(long long)q * n + r] * fs[q];
         int i = r % C.nx, j = (r / C.nx) % C.ny, k = r / (C.nx * C.ny);
-        u.c[scol(i, j, k)][soff(C, i, j, k)] = (T)acc;
+        u.half(scol(i, j, k))[soff(C, i, j, k)] = (T)acc;
     }
 }
 
@@ -211,7 +211,7 @@ __device__ __forceinline__ void dense_row(const KOp<T>& op, const Lev& L, int i,
 {
     const int r = i + L.nx * (j + L.ny * k);
     const double kc = (double)kval(op, L, i, j, k);
-    double d = op.dex[0] ? (double)op.dex[scol(i, j, k)][soff(L, i, j, k)] : (double)op.dexc;
+    double d = op.dex[0] ? (double)sel(op.dex, scol(i, j, k))[soff(L, i, j, k)] : (double)op.dexc;
     for (int ax = 0; ax < 3; ax++)
         for (int s = -1; s <= 1; s += 2) {
             int a = i, b = j, c = k;
@@ -233,12 +233,12 @@ __device__ __forceinline__ void dense_row(const ROp<T>& op, const Lev& L, int i,
     const int r = i + L.nx * (j + L.ny * k);
     const int c0 = scol(i, j, k);
     const long long o0 = soff(L, i, j, k);
-    A[(long long)r * n + r] += (double)op.r[0][c0][o0];
+    A[(long long)r * n + r] += (double)sel(op.r[0], c0)[o0];
     for (int ax = 0; ax < 3; ax++)
         for (int s = -1; s <= 1; s += 2) {
             int a = i, b = j, c = k;
             if (nbr(L, ax, s, a, b, c))
-                A[(long long)r * n + (a + L.nx * (b + L.ny * c))] += (double)op.r[1 + 2 * ax + (s > 0)][c0][o0];
+                A[(long long)r * n + (a + L.nx * (b + L.ny * c))] += (double)sel(op.r[1 + 2 * ax + (s > 0)], c0)[o0];
         }
 }
 template <class T, class Op>
@@ -324,11 +324,11 @@ __global__ void __launch_bounds__(TPB) k_resid_norm(Lev L, Op op, CSplit<T> u, C
         if (t < total && decode(L, t, c, i, j, k)) {
             T diag, off;
             row_any<T>(op, L, u, i, j, k, diag, off);
-            T fv = __ldg(&f.c[c][t]);
-            T r = fv - (diag * __ldg(&u.c[c][t]) + off);
+            T fv = __ldg(&f.half(c)[t]);
+            T r = fv - (diag * __ldg(&u.half(c)[t]) + off);
             rr += (double)r * (double)r;
             ff += (double)fv * (double)fv;
-            if (rout.c[0]) rout.c[c][t] = (R)r;
+            if (rout.c[0]) rout.half(c)[t] = (R)r;
         }
     }
     double a = block_sum(rr, sh);
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(TPB) k_apply(Lev L, Op op, CSplit<Tu> u, Split
         if (decode(L, t, c, i, j, k)) {
             T diag, off;
             row_eval(op, L, u, i, j, k, diag, off);
-            out.c[c][t] = (double)(diag * (T)__ldg(&u.c[c][t]) + off);
+            out.half(c)[t] = (double)(diag * (T)__ldg(&u.half(c)[t]) + off);
         }
     }
 }
@@ -368,7 +368,7 @@ __global__ void k_pack(Lev L, const double* __restrict__ g, Split<T> out, double
     unsigned i = rem - j * nx;
     long long gi = (long long)(i + 1) + (long long)(nx + 2) * ((long long)(j + 1) + (long long)(ny + 2) * (k + 1));
     double v = g ? g[gi] * scale + shift : shift;
-    out.c[scol(i, j, k)][soff(L, i, j, k)] = (T)v;
+    out.half(scol(i, j, k))[soff(L, i, j, k)] = (T)v;
 }
 
 template <class T>
@@ -504,8 +504,8 @@ __global__ void k_build_rows(Lev L, CSplit<double> vx, CSplit<double> vy, CSplit
     d = d - (has_reac ? reac.get(L, i, j, k) : 0.0) + dtinv;
     const int cc = scol(i, j, k);
     const long long o = soff(L, i, j, k);
-    ((T*)out_rows.r[0][cc])[o] = (T)d;
-    for (int q = 0; q < 6; q++) ((T*)out_rows.r[1 + q][cc])[o] = (T)co[q];
+    ((T*)sel(out_rows.r[0], cc))[o] = (T)d;
+    for (int q = 0; q < 6; q++) ((T*)sel(out_rows.r[1 + q], cc))[o] = (T)co[q];
 }
 
 template <class T>
