@@ -21,22 +21,29 @@ namespace mps {
 enum { BC_DIRC = 1, BC_FLUX = 2, BC_ZGRD = 3, BC_PERI = 4, BC_DZGD = 5 };
 enum { F_LEFT = 0, F_RIGHT, F_BOTTOM, F_TOP, F_BACK, F_FRONT };
 
-// unsigned division by a run-time invariant d (n < 2^31): q = (n*M) >> s
+// unsigned division by a run-time invariant d with a 32-bit multiply-high
+// (Granlund-Montgomery): q = (t + ((n - t) >> 1)) >> (l - 1), t = mulhi(M, n),
+// l = ceil(log2 d), M = floor(2^32 (2^l - d) / d) + 1; exact for all 32-bit n
 struct FastDiv {
-    unsigned long long M;
-    int s;
+    unsigned M;
+    int l;
     unsigned d;
     __host__ void init(unsigned dv)
     {
         d = dv;
-        int l = 0;
+        l = 0;
         while ((1ull << l) < dv) l++;
-        s = 32 + l;
-        M = ((1ull << s) + dv - 1) / dv;
+        M = (unsigned)(((1ull << 32) * ((1ull << l) - dv)) / dv + 1);
     }
     __host__ __device__ __forceinline__ unsigned div(unsigned n) const
     {
-        return (unsigned)(((unsigned long long)n * M) >> s);
+        if (d == 1) return n;
+#ifdef __CUDA_ARCH__
+        const unsigned t = __umulhi(M, n);
+#else
+        const unsigned t = (unsigned)(((unsigned long long)M * n) >> 32);
+#endif
+        return (t + ((n - t) >> 1)) >> (l - 1);
     }
 };
 
@@ -57,9 +64,7 @@ struct Lev {
     int bc[6];        // BC codes LEFT..FRONT
     double w[3], wl[3];
     double cr[3], cl[3], cp[3], dr[3], dlast[3];
-    int fast_lo[3], fast_hi[3];  // index range per axis where a row has six
-                                 // neighbours of the other colour at regular
-                                 // spacing (interior fast path)
+    int uniform;      // all cells of the level have the regular widths
     FastDiv divP, divNy;
     unsigned rows;    // ny*nz
 };
@@ -290,12 +295,125 @@ __device__ __forceinline__ void row_eval(const ROp<T>& op, const Lev& L, const U
     off = acc;
 }
 
-// all stencil kernels evaluate rows through this entry point
+// ---- uniform levels (every level of the reference hierarchy, and the
+// finest level always): the six neighbours of an interior cell have the other
+// colour at offsets o+q-1, o+q (x, q = i&1), o-+P (y), o-+P*ny (z) of the
+// other half; boundary cells patch the offset of a missing face (periodic
+// wrap: the wrapped cell; physical face: the cell itself with weight 0 and
+// the Dirichlet term on the diagonal).
+struct Nb6 {
+    int o[6];   // offsets
+    int c[6];   // colours
+    int m[6];   // 1 = face present
+    int dirc;   // bit f set: physical Dirichlet face f
+};
+
+__device__ __forceinline__ void nb6(const Lev& L, int i, int j, int k, int cc, int o, Nb6& N)
+{
+    const int oc = cc ^ 1, q = i & 1, sy = L.P, sz = L.P * L.ny;
+    N.o[0] = o + q - 1; N.o[1] = o + q; N.o[2] = o - sy; N.o[3] = o + sy; N.o[4] = o - sz; N.o[5] = o + sz;
+#pragma unroll
+    for (int f = 0; f < 6; f++) { N.c[f] = oc; N.m[f] = 1; }
+    N.dirc = 0;
+    const int row = j + L.ny * k;
+    if (i == 0) {
+        if (L.per[0]) { const int a = L.nx - 1; N.c[0] = (a + j + k) & 1; N.o[0] = (a >> 1) + L.P * row; }
+        else { N.m[0] = 0; N.o[0] = o; N.c[0] = cc; N.dirc |= (L.bc[0] == BC_DIRC) << 0; }
+    }
+    if (i == L.nx - 1) {
+        if (L.per[0]) { N.c[1] = (j + k) & 1; N.o[1] = L.P * row; }
+        else { N.m[1] = 0; N.o[1] = o; N.c[1] = cc; N.dirc |= (L.bc[1] == BC_DIRC) << 1; }
+    }
+    if (j == 0) {
+        if (L.per[1]) { const int b = L.ny - 1; N.c[2] = (i + b + k) & 1; N.o[2] = (i >> 1) + L.P * (b + L.ny * k); }
+        else { N.m[2] = 0; N.o[2] = o; N.c[2] = cc; N.dirc |= (L.bc[2] == BC_DIRC) << 2; }
+    }
+    if (j == L.ny - 1) {
+        if (L.per[1]) { N.c[3] = (i + k) & 1; N.o[3] = (i >> 1) + L.P * (L.ny * k); }
+        else { N.m[3] = 0; N.o[3] = o; N.c[3] = cc; N.dirc |= (L.bc[3] == BC_DIRC) << 3; }
+    }
+    if (k == 0) {
+        if (L.per[2]) { const int c = L.nz - 1; N.c[4] = (i + j + c) & 1; N.o[4] = (i >> 1) + L.P * (j + L.ny * c); }
+        else { N.m[4] = 0; N.o[4] = o; N.c[4] = cc; N.dirc |= (L.bc[4] == BC_DIRC) << 4; }
+    }
+    if (k == L.nz - 1) {
+        if (L.per[2]) { N.c[5] = (i + j) & 1; N.o[5] = (i >> 1) + L.P * j; }
+        else { N.m[5] = 0; N.o[5] = o; N.c[5] = cc; N.dirc |= (L.bc[5] == BC_DIRC) << 5; }
+    }
+}
+
+template <class T, class U>
+__device__ __forceinline__ void row_eval_uni(const KOp<T>& op, const Lev& L, const U& u, int i, int j, int k,
+                                             T& diag, T& off)
+{
+    const int cc = (i + j + k) & 1;
+    const int o = (i >> 1) + L.P * (j + L.ny * k);
+    Nb6 N;
+    nb6(L, i, j, k, cc, o, N);
+    const T cf[3] = {(T)L.cr[0], (T)L.cr[1], (T)L.cr[2]};
+    T d = op.dex[0] ? __ldg(&sel(op.dex, cc)[o]) : op.dexc;
+    T acc = T(0);
+    if (op.k[0]) {
+        const T kc = __ldg(&sel(op.k, cc)[o]);
+        T wsum = T(0);
+#pragma unroll
+        for (int f = 0; f < 6; f++) {
+            const T kn = __ldg(&sel(op.k, N.c[f])[N.o[f]]);
+            const T w = N.m[f] ? (kc + kn) * cf[f >> 1] : T(0);
+            wsum += w;
+            acc += w * u.at(N.c[f], N.o[f]);
+        }
+        d += T(0.5) * wsum;
+        acc *= T(0.5);
+        if (N.dirc) {
+#pragma unroll
+            for (int f = 0; f < 6; f++)
+                if ((N.dirc >> f) & 1) d += T(2) * kc * cf[f >> 1];
+        }
+    } else {
+        const T kc = op.kc;
+        T wsum = T(0);
+#pragma unroll
+        for (int f = 0; f < 6; f++) {
+            const T w = N.m[f] ? cf[f >> 1] : T(0);
+            wsum += w;
+            acc += w * u.at(N.c[f], N.o[f]);
+        }
+        if (N.dirc) {
+#pragma unroll
+            for (int f = 0; f < 6; f++)
+                if ((N.dirc >> f) & 1) wsum += T(2) * cf[f >> 1];
+        }
+        d += kc * wsum;
+        acc *= kc;
+    }
+    diag = d;
+    off = -acc;
+}
+
+template <class T, class U>
+__device__ __forceinline__ void row_eval_uni(const ROp<T>& op, const Lev& L, const U& u, int i, int j, int k,
+                                             T& diag, T& off)
+{
+    const int cc = (i + j + k) & 1;
+    const int o = (i >> 1) + L.P * (j + L.ny * k);
+    Nb6 N;
+    nb6(L, i, j, k, cc, o, N);
+    T acc = T(0);
+#pragma unroll
+    for (int f = 0; f < 6; f++) acc += __ldg(&sel(op.r[1 + f], cc)[o]) * u.at(N.c[f], N.o[f]);
+    diag = __ldg(&sel(op.r[0], cc)[o]);
+    off = acc;
+}
+
+// all stencil kernels evaluate rows through this entry point (the branch is
+// uniform across a launch)
 template <class T, class Op, class U>
 __device__ __forceinline__ void row_any(const Op& op, const Lev& L, const U& u, int i, int j, int k, T& diag,
                                         T& off)
 {
-    row_eval(op, L, u, i, j, k, diag, off);
+    if (L.uniform) row_eval_uni(op, L, u, i, j, k, diag, off);
+    else row_eval(op, L, u, i, j, k, diag, off);
 }
 
 // red-black Gauss-Seidel point update u_c = (f_c - offdiag)/diag
@@ -304,6 +422,12 @@ template <class T>
 __device__ __forceinline__ T gs_value(T f, T diag, T off)
 {
     return (f - off) / diag;
+}
+// FP32 V-cycles are a preconditioner: the approximate divide (2 ulp) is used
+template <>
+__device__ __forceinline__ float gs_value<float>(float f, float diag, float off)
+{
+    return __fdividef(f - off, diag);
 }
 
 // Scharfetter-Gummel face weights (find_sg_exponential_flux,

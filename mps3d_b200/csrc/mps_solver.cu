@@ -211,11 +211,8 @@ static Lev make_lev(int nx, int ny, int nz, const double w[3], const double wl[3
         L.cp[a] = 1.0 / (dl * ww);
         L.dr[a] = 2.0 / (ww * ww);
         L.dlast[a] = 2.0 / (wwl * wwl);
-        // fast path: not on a boundary/seam cell, not the last cell or its
-        // neighbour when the last cell's width differs
-        L.fast_lo[a] = 1;
-        L.fast_hi[a] = n[a] - 2 - (wwl != ww ? 1 : 0);
     }
+    L.uniform = (w[0] == wl[0] && w[1] == wl[1] && w[2] == wl[2]) ? 1 : 0;
     L.divP.init((unsigned)L.P);
     L.divNy.init((unsigned)ny);
     L.rows = (unsigned)ny * (unsigned)nz;
