@@ -151,6 +151,8 @@ struct CSplit {
         return __ldg(&half(scol(i, j, k))[soff(L, i, j, k)]);
     }
     __device__ __forceinline__ T at(int col, int off) const { return __ldg(&half(col)[off]); }
+    __device__ __forceinline__ const T* ptr(int col) const { return half(col); }
+    __device__ __forceinline__ T ld(const T* p, int off) const { return __ldg(&p[off]); }
 };
 
 // neighbour along axis ax (0..2), direction s (-1/+1); returns false at a
@@ -298,47 +300,66 @@ __device__ __forceinline__ void row_eval(const ROp<T>& op, const Lev& L, const U
 // ---- uniform levels (every level of the reference hierarchy, and the
 // finest level always): the six neighbours of an interior cell have the other
 // colour at offsets o+q-1, o+q (x, q = i&1), o-+P (y), o-+P*ny (z) of the
-// other half; boundary cells patch the offset of a missing face (periodic
-// wrap: the wrapped cell; physical face: the cell itself with weight 0 and
-// the Dirichlet term on the diagonal).
+// other half, read through one base pointer per field.  Boundary cells patch
+// the offset of a missing face: a physical face keeps a valid offset with
+// weight 0 and adds its Dirichlet term to the diagonal; a periodic face
+// points at the wrapped cell.  When a periodic size is odd the wrapped cell
+// has the same colour (a "seam"): that face is left out of the main loop and
+// added in a rare fix-up from the same-colour arrays.
 struct Nb6 {
-    int o[6];   // offsets
-    int c[6];   // colours
-    int m[6];   // 1 = face present
-    int dirc;   // bit f set: physical Dirichlet face f
+    int o[6];   // offsets into the half of the neighbour's colour
+    int m[6];   // 1 = face in the main (other-colour) loop
+    int dirc;   // bit f: physical Dirichlet face f
+    int seam;   // bit f: periodic face whose neighbour has the same colour
 };
 
 __device__ __forceinline__ void nb6(const Lev& L, int i, int j, int k, int cc, int o, Nb6& N)
 {
-    const int oc = cc ^ 1, q = i & 1, sy = L.P, sz = L.P * L.ny;
+    const int q = i & 1, sy = L.P, sz = L.P * L.ny;
     N.o[0] = o + q - 1; N.o[1] = o + q; N.o[2] = o - sy; N.o[3] = o + sy; N.o[4] = o - sz; N.o[5] = o + sz;
 #pragma unroll
-    for (int f = 0; f < 6; f++) { N.c[f] = oc; N.m[f] = 1; }
+    for (int f = 0; f < 6; f++) N.m[f] = 1;
     N.dirc = 0;
+    N.seam = 0;
     const int row = j + L.ny * k;
     if (i == 0) {
-        if (L.per[0]) { const int a = L.nx - 1; N.c[0] = (a + j + k) & 1; N.o[0] = (a >> 1) + L.P * row; }
-        else { N.m[0] = 0; N.o[0] = o; N.c[0] = cc; N.dirc |= (L.bc[0] == BC_DIRC) << 0; }
+        if (L.per[0]) {
+            const int a = L.nx - 1;
+            N.o[0] = (a >> 1) + L.P * row;
+            if (((a + j + k) & 1) == cc) { N.seam |= 1; N.m[0] = 0; }
+        } else { N.m[0] = 0; N.o[0] = o; N.dirc |= (L.bc[0] == BC_DIRC) << 0; }
     }
     if (i == L.nx - 1) {
-        if (L.per[0]) { N.c[1] = (j + k) & 1; N.o[1] = L.P * row; }
-        else { N.m[1] = 0; N.o[1] = o; N.c[1] = cc; N.dirc |= (L.bc[1] == BC_DIRC) << 1; }
+        if (L.per[0]) {
+            N.o[1] = L.P * row;
+            if (((j + k) & 1) == cc) { N.seam |= 2; N.m[1] = 0; }
+        } else { N.m[1] = 0; N.o[1] = o; N.dirc |= (L.bc[1] == BC_DIRC) << 1; }
     }
     if (j == 0) {
-        if (L.per[1]) { const int b = L.ny - 1; N.c[2] = (i + b + k) & 1; N.o[2] = (i >> 1) + L.P * (b + L.ny * k); }
-        else { N.m[2] = 0; N.o[2] = o; N.c[2] = cc; N.dirc |= (L.bc[2] == BC_DIRC) << 2; }
+        if (L.per[1]) {
+            const int b = L.ny - 1;
+            N.o[2] = (i >> 1) + L.P * (b + L.ny * k);
+            if (((i + b + k) & 1) == cc) { N.seam |= 4; N.m[2] = 0; }
+        } else { N.m[2] = 0; N.o[2] = o; N.dirc |= (L.bc[2] == BC_DIRC) << 2; }
     }
     if (j == L.ny - 1) {
-        if (L.per[1]) { N.c[3] = (i + k) & 1; N.o[3] = (i >> 1) + L.P * (L.ny * k); }
-        else { N.m[3] = 0; N.o[3] = o; N.c[3] = cc; N.dirc |= (L.bc[3] == BC_DIRC) << 3; }
+        if (L.per[1]) {
+            N.o[3] = (i >> 1) + L.P * (L.ny * k);
+            if (((i + k) & 1) == cc) { N.seam |= 8; N.m[3] = 0; }
+        } else { N.m[3] = 0; N.o[3] = o; N.dirc |= (L.bc[3] == BC_DIRC) << 3; }
     }
     if (k == 0) {
-        if (L.per[2]) { const int c = L.nz - 1; N.c[4] = (i + j + c) & 1; N.o[4] = (i >> 1) + L.P * (j + L.ny * c); }
-        else { N.m[4] = 0; N.o[4] = o; N.c[4] = cc; N.dirc |= (L.bc[4] == BC_DIRC) << 4; }
+        if (L.per[2]) {
+            const int c = L.nz - 1;
+            N.o[4] = (i >> 1) + L.P * (j + L.ny * c);
+            if (((i + j + c) & 1) == cc) { N.seam |= 16; N.m[4] = 0; }
+        } else { N.m[4] = 0; N.o[4] = o; N.dirc |= (L.bc[4] == BC_DIRC) << 4; }
     }
     if (k == L.nz - 1) {
-        if (L.per[2]) { N.c[5] = (i + j) & 1; N.o[5] = (i >> 1) + L.P * j; }
-        else { N.m[5] = 0; N.o[5] = o; N.c[5] = cc; N.dirc |= (L.bc[5] == BC_DIRC) << 5; }
+        if (L.per[2]) {
+            N.o[5] = (i >> 1) + L.P * j;
+            if (((i + j) & 1) == cc) { N.seam |= 32; N.m[5] = 0; }
+        } else { N.m[5] = 0; N.o[5] = o; N.dirc |= (L.bc[5] == BC_DIRC) << 5; }
     }
 }
 
@@ -346,30 +367,40 @@ template <class T, class U>
 __device__ __forceinline__ void row_eval_uni(const KOp<T>& op, const Lev& L, const U& u, int i, int j, int k,
                                              T& diag, T& off)
 {
-    const int cc = (i + j + k) & 1;
+    const int cc = (i + j + k) & 1, oc = cc ^ 1;
     const int o = (i >> 1) + L.P * (j + L.ny * k);
     Nb6 N;
     nb6(L, i, j, k, cc, o, N);
     const T cf[3] = {(T)L.cr[0], (T)L.cr[1], (T)L.cr[2]};
     T d = op.dex[0] ? __ldg(&sel(op.dex, cc)[o]) : op.dexc;
+    const T* uo = u.ptr(oc);
     T acc = T(0);
     if (op.k[0]) {
+        const T* ko = sel(op.k, oc);
         const T kc = __ldg(&sel(op.k, cc)[o]);
         T wsum = T(0);
 #pragma unroll
         for (int f = 0; f < 6; f++) {
-            const T kn = __ldg(&sel(op.k, N.c[f])[N.o[f]]);
+            const T kn = __ldg(&ko[N.o[f]]);
             const T w = N.m[f] ? (kc + kn) * cf[f >> 1] : T(0);
             wsum += w;
-            acc += w * u.at(N.c[f], N.o[f]);
+            acc += w * u.ld(uo, N.o[f]);
+        }
+        if (N.seam | N.dirc) {
+            const T* ks = sel(op.k, cc);
+            const T* us = u.ptr(cc);
+#pragma unroll
+            for (int f = 0; f < 6; f++) {
+                if ((N.seam >> f) & 1) {
+                    const T w = (kc + __ldg(&ks[N.o[f]])) * cf[f >> 1];
+                    wsum += w;
+                    acc += w * u.ld(us, N.o[f]);
+                }
+                if ((N.dirc >> f) & 1) wsum += T(4) * kc * cf[f >> 1];
+            }
         }
         d += T(0.5) * wsum;
         acc *= T(0.5);
-        if (N.dirc) {
-#pragma unroll
-            for (int f = 0; f < 6; f++)
-                if ((N.dirc >> f) & 1) d += T(2) * kc * cf[f >> 1];
-        }
     } else {
         const T kc = op.kc;
         T wsum = T(0);
@@ -377,12 +408,18 @@ __device__ __forceinline__ void row_eval_uni(const KOp<T>& op, const Lev& L, con
         for (int f = 0; f < 6; f++) {
             const T w = N.m[f] ? cf[f >> 1] : T(0);
             wsum += w;
-            acc += w * u.at(N.c[f], N.o[f]);
+            acc += w * u.ld(uo, N.o[f]);
         }
-        if (N.dirc) {
+        if (N.seam | N.dirc) {
+            const T* us = u.ptr(cc);
 #pragma unroll
-            for (int f = 0; f < 6; f++)
+            for (int f = 0; f < 6; f++) {
+                if ((N.seam >> f) & 1) {
+                    wsum += cf[f >> 1];
+                    acc += cf[f >> 1] * u.ld(us, N.o[f]);
+                }
                 if ((N.dirc >> f) & 1) wsum += T(2) * cf[f >> 1];
+            }
         }
         d += kc * wsum;
         acc *= kc;
@@ -395,13 +432,25 @@ template <class T, class U>
 __device__ __forceinline__ void row_eval_uni(const ROp<T>& op, const Lev& L, const U& u, int i, int j, int k,
                                              T& diag, T& off)
 {
-    const int cc = (i + j + k) & 1;
+    const int cc = (i + j + k) & 1, oc = cc ^ 1;
     const int o = (i >> 1) + L.P * (j + L.ny * k);
     Nb6 N;
     nb6(L, i, j, k, cc, o, N);
+    const T* uo = u.ptr(oc);
     T acc = T(0);
+    // missing physical faces have zero row coefficients; seam faces read the
+    // same colour
 #pragma unroll
-    for (int f = 0; f < 6; f++) acc += __ldg(&sel(op.r[1 + f], cc)[o]) * u.at(N.c[f], N.o[f]);
+    for (int f = 0; f < 6; f++) {
+        const T a = __ldg(&sel(op.r[1 + f], cc)[o]);
+        acc += ((N.seam >> f) & 1) ? T(0) : a * u.ld(uo, N.o[f]);
+    }
+    if (N.seam) {
+        const T* us = u.ptr(cc);
+#pragma unroll
+        for (int f = 0; f < 6; f++)
+            if ((N.seam >> f) & 1) acc += __ldg(&sel(op.r[1 + f], cc)[o]) * u.ld(us, N.o[f]);
+    }
     diag = __ldg(&sel(op.r[0], cc)[o]);
     off = acc;
 }

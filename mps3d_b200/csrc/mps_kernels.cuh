@@ -13,6 +13,8 @@ template <class T>
 struct ZeroU {  // accessor of a field known to be zero
     __device__ __forceinline__ T get(const Lev&, int, int, int) const { return T(0); }
     __device__ __forceinline__ T at(int, int) const { return T(0); }
+    __device__ __forceinline__ const T* ptr(int) const { return nullptr; }
+    __device__ __forceinline__ T ld(const T*, int) const { return T(0); }
 };
 template <class T>
 struct OtherOnlyU {  // colour c known zero, the other colour read from memory
@@ -23,6 +25,8 @@ struct OtherOnlyU {  // colour c known zero, the other colour read from memory
         return scol(i, j, k) == c ? T(0) : __ldg(&other[soff(L, i, j, k)]);
     }
     __device__ __forceinline__ T at(int col, int off) const { return col == c ? T(0) : __ldg(&other[off]); }
+    __device__ __forceinline__ const T* ptr(int col) const { return col == c ? nullptr : other; }
+    __device__ __forceinline__ T ld(const T* p, int off) const { return p ? __ldg(&p[off]) : T(0); }
 };
 
 // ---------------------------------------------------------------------
