@@ -65,7 +65,7 @@ struct Lev {
     double w[3], wl[3];
     double cr[3], cl[3], cp[3], dr[3], dlast[3];
     int uniform;      // all cells of the level have the regular widths
-    FastDiv divP, divNy;
+    FastDiv divP, divNy, divG;  // by P, ny, P/4
     unsigned rows;    // ny*nz
 };
 

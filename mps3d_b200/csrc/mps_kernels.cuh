@@ -50,6 +50,205 @@ __global__ void __launch_bounds__(TPB) k_colour(Lev L, Op op, int c, U u, T* __r
 }
 
 // ---------------------------------------------------------------------
+// colour pass on a uniform level, four consecutive cells of one colour per
+// thread (16-byte vector loads).  Row (j,k), group g: split offsets
+// o0..o0+3 with o0 = 4g + P*(j+ny*k); i = 2(4g+e)+q, q = (j+k+c)&1.  The x
+// neighbours of the group are the other colour at o0+q-1 .. o0+q+3 (one
+// vector plus one scalar), the y/z neighbours one vector each.  Elements past
+// the end of the row (pads) are written as 0.  Same semantics as k_colour.
+// ---------------------------------------------------------------------
+template <class T>
+struct Vec4 {
+    T v[4];
+};
+template <class T>
+__device__ __forceinline__ Vec4<T> ld4(const T* p)
+{
+    Vec4<T> r;
+    if constexpr (sizeof(T) == 4) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    } else {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        r.v[0] = a.x; r.v[1] = a.y; r.v[2] = b.x; r.v[3] = b.y;
+    }
+    return r;
+}
+template <class T>
+__device__ __forceinline__ void st4(T* p, const Vec4<T>& r)
+{
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2(r.v[0], r.v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(r.v[2], r.v[3]);
+    }
+}
+template <class T>
+__device__ __forceinline__ Vec4<T> zero4()
+{
+    Vec4<T> r;
+#pragma unroll
+    for (int e = 0; e < 4; e++) r.v[e] = T(0);
+    return r;
+}
+
+// field accessors for the vector kernel: a pointer per colour half, or zero
+template <class T>
+struct Fld {
+    const T* c0;
+    const T* c1;
+    __device__ __forceinline__ const T* half(int col) const { return col ? c1 : c0; }
+};
+
+// the two row neighbours along y or z of the group (AX = 1 or 2, S = -1/+1):
+// vector of u and k values and the face status
+template <class T, int AX, int S>
+__device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int q, int cc, const T* uo, const T* us,
+                                        const T* ko, const T* ks, bool kfield, Vec4<T>& u4, Vec4<T>& k4, int& mask,
+                                        int& dirc)
+{
+    const int n = AX == 1 ? L.ny : L.nz;
+    const int p = AX == 1 ? j : k;
+    int pq = p + S;
+    mask = 1;
+    dirc = 0;
+    const T* ub = uo;
+    const T* kb = ko;
+    if (pq < 0 || pq >= n) {
+        if (!L.per[AX]) {  // physical face: no neighbour
+            mask = 0;
+            dirc = L.bc[2 * AX + (S > 0 ? 1 : 0)] == BC_DIRC;
+            u4 = zero4<T>();
+            k4 = zero4<T>();
+            return;
+        }
+        pq = pq < 0 ? n - 1 : 0;
+        // the wrapped row's colour for this group: (i + j' + k') & 1 with i parity q (of colour cc)
+        const int jj = AX == 1 ? pq : j, kk = AX == 2 ? pq : k;
+        const int ncol = ((2 * h0 + ((j + k + cc) & 1)) + jj + kk) & 1;
+        if (ncol == cc) { ub = us; kb = ks; }
+    }
+    const int jj = AX == 1 ? pq : j, kk = AX == 2 ? pq : k;
+    const int off = h0 + L.P * (jj + L.ny * kk);
+    u4 = ub ? ld4(ub + off) : zero4<T>();
+    k4 = kfield ? ld4(kb + off) : zero4<T>();
+    (void)q;
+}
+
+template <class T, class U>
+__global__ void __launch_bounds__(TPB) k_colour4(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
+                                                 const T* __restrict__ f)
+{
+    const unsigned G = (unsigned)L.P >> 2;  // groups per row
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned row = L.divG.div(t);
+    if (row >= L.rows) return;
+    const int g = (int)(t - row * G);
+    const int k = (int)L.divNy.div(row);
+    const int j = (int)row - k * L.ny;
+    const int cc = c, oc = c ^ 1;
+    const int q = (j + k + c) & 1;
+    const int h0 = 4 * g;
+    const int o0 = h0 + L.P * (int)row;
+    const bool kfield = op.k[0] != nullptr;
+    const T* uo = u.ptr(oc);
+    const T* us = u.ptr(cc);
+    const T* ko = kfield ? sel(op.k, oc) : nullptr;
+    const T* ks = kfield ? sel(op.k, cc) : nullptr;
+    const T cx = (T)L.cr[0], cy = (T)L.cr[1], cz = (T)L.cr[2];
+
+    // own values
+    const Vec4<T> f4 = ld4(f + o0);
+    const Vec4<T> kc4 = kfield ? ld4(ks + o0) : zero4<T>();
+    Vec4<T> d4;
+    if (op.dex[0]) d4 = ld4(sel(op.dex, cc) + o0);
+    else {
+#pragma unroll
+        for (int e = 0; e < 4; e++) d4.v[e] = op.dexc;
+    }
+
+    // x neighbours: A = other colour at o0..o0+3, S = o0+4 (q=1) or o0-1 (q=0)
+    const Vec4<T> ax = uo ? ld4(uo + o0) : zero4<T>();
+    const Vec4<T> akx = kfield ? ld4(ko + o0) : zero4<T>();
+    int so = q ? o0 + 4 : o0 - 1;
+    bool sok = q ? (h0 + 4 < L.P) : (h0 > 0);
+    T sx = T(0), skx = T(0);
+    if (sok) {
+        sx = u.ld(uo, so);
+        skx = kfield ? __ldg(ko + so) : T(0);
+    }
+
+    // y/z neighbours
+    Vec4<T> uym, kym, uyp, kyp, uzm, kzm, uzp, kzp;
+    int mym, myp, mzm, mzp, dym, dyp, dzm, dzp;
+    yz_face<T, 1, -1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uym, kym, mym, dym);
+    yz_face<T, 1, 1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uyp, kyp, myp, dyp);
+    yz_face<T, 2, -1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uzm, kzm, mzm, dzm);
+    yz_face<T, 2, 1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uzp, kzp, mzp, dzp);
+
+    Vec4<T> res;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int i = 2 * (h0 + e) + q;
+        // x-: other colour at h0+e+q-1 ; x+: at h0+e+q
+        T uxm, kxm, uxp, kxp;
+        if (q) {
+            uxm = ax.v[e]; kxm = akx.v[e];
+            uxp = e < 3 ? ax.v[e + 1] : sx; kxp = e < 3 ? akx.v[e + 1] : skx;
+        } else {
+            uxm = e > 0 ? ax.v[e - 1] : sx; kxm = e > 0 ? akx.v[e - 1] : skx;
+            uxp = ax.v[e]; kxp = akx.v[e];
+        }
+        T mxm = T(1), mxp = T(1);
+        T dxm = T(0), dxp = T(0);
+        if (i == 0) {  // x- boundary / periodic wrap
+            if (L.per[0]) {
+                const int a = L.nx - 1;
+                const int ncol = (a + j + k) & 1;
+                const int wo = (a >> 1) + L.P * (int)row;
+                if (ncol == cc) { uxm = u.ld(us, wo); kxm = kfield ? __ldg(ks + wo) : T(0); }
+                else { uxm = u.ld(uo, wo); kxm = kfield ? __ldg(ko + wo) : T(0); }
+            } else {
+                mxm = T(0);
+                dxm = L.bc[0] == BC_DIRC ? T(1) : T(0);
+            }
+        }
+        if (i == L.nx - 1) {  // x+ boundary / periodic wrap
+            if (L.per[0]) {
+                const int ncol = (j + k) & 1;
+                const int wo = L.P * (int)row;
+                if (ncol == cc) { uxp = u.ld(us, wo); kxp = kfield ? __ldg(ks + wo) : T(0); }
+                else { uxp = u.ld(uo, wo); kxp = kfield ? __ldg(ko + wo) : T(0); }
+            } else {
+                mxp = T(0);
+                dxp = L.bc[1] == BC_DIRC ? T(1) : T(0);
+            }
+        }
+        const T kc = kfield ? kc4.v[e] : op.kc;
+        T diag, acc;
+        if (kfield) {
+            const T w0 = mxm * (kc + kxm) * cx, w1 = mxp * (kc + kxp) * cx;
+            const T w2 = (T)mym * (kc + kym.v[e]) * cy, w3 = (T)myp * (kc + kyp.v[e]) * cy;
+            const T w4 = (T)mzm * (kc + kzm.v[e]) * cz, w5 = (T)mzp * (kc + kzp.v[e]) * cz;
+            const T bnd = T(2) * kc * ((dxm + dxp) * cx + (T)(dym + dyp) * cy + (T)(dzm + dzp) * cz);
+            diag = d4.v[e] + T(0.5) * (((w0 + w1) + (w2 + w3)) + (w4 + w5)) + bnd;
+            acc = T(0.5) * (((w0 * uxm + w1 * uxp) + (w2 * uym.v[e] + w3 * uyp.v[e])) +
+                            (w4 * uzm.v[e] + w5 * uzp.v[e]));
+        } else {
+            const T sw = (mxm + mxp) * cx + (T)(mym + myp) * cy + (T)(mzm + mzp) * cz +
+                         T(2) * ((dxm + dxp) * cx + (T)(dym + dyp) * cy + (T)(dzm + dzp) * cz);
+            diag = d4.v[e] + kc * sw;
+            acc = kc * ((cx * (mxm * uxm + mxp * uxp) + cy * (uym.v[e] * (T)mym + uyp.v[e] * (T)myp)) +
+                        cz * (uzm.v[e] * (T)mzm + uzp.v[e] * (T)mzp));
+        }
+        res.v[e] = i < L.nx ? gs_value(f4.v[e], diag, -acc) : T(0);
+    }
+    st4(out + o0, res);
+}
+
+// ---------------------------------------------------------------------
 // residual r = f - A u on the fine level fused with the restriction to the
 // coarse level: coarse value = mean of r over the children {2I,2I+1}^3 that
 // exist (restriction, mgridsteps.f90:11-53, applied to the residual at :531).

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/mps_linsolve.h"
@@ -215,6 +216,7 @@ static Lev make_lev(int nx, int ny, int nz, const double w[3], const double wl[3
     L.uniform = (w[0] == wl[0] && w[1] == wl[1] && w[2] == wl[2]) ? 1 : 0;
     L.divP.init((unsigned)L.P);
     L.divNy.init((unsigned)ny);
+    L.divG.init((unsigned)(L.P / 4));
     L.rows = (unsigned)ny * (unsigned)nz;
     return L;
 }
@@ -464,6 +466,26 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     if (c == 0) out = H.U[l][H.ri[l] ^ 1];
     else out = H.U[l][H.bi[l] ^ 1] + L.half;
     if (l == 0) prof_begin(ctx, MPS_PROF_SMOOTH);
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (L.uniform) {
+            const unsigned nb4 = nblk((long long)(L.P / 4) * L.rows);
+            if (zero_state == 2) {
+                k_colour4<T, ZeroU<T>><<<nb4, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh);
+            } else if (zero_state == 1) {
+                OtherOnlyU<T> u;
+                u.c = c;
+                u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
+                k_colour4<T, OtherOnlyU<T>><<<nb4, TPB, 0, ctx.s>>>(L, op, c, u, out, fh);
+            } else {
+                k_colour4<T, CSplit<T>><<<nb4, TPB, 0, ctx.s>>>(L, op, c, ccur(H, L, l), out, fh);
+            }
+            if (l == 0) prof_end(ctx);
+            CKL();
+            if (c == 0) H.ri[l] ^= 1;
+            else H.bi[l] ^= 1;
+            return 0;
+        }
+    }
     if (zero_state == 2) {  // whole state zero
         k_colour<T, Op, ZeroU<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh);
     } else if (zero_state == 1) {  // colour c zero, other colour valid
