@@ -57,17 +57,25 @@ __global__ void __launch_bounds__(TPB) k_colour(Lev L, Op op, int c, U u, T* __r
 // vector plus one scalar), the y/z neighbours one vector each.  Elements past
 // the end of the row (pads) are written as 0.  Same semantics as k_colour.
 // ---------------------------------------------------------------------
-template <class T>
-struct Vec4 {
-    T v[4];
+template <class T, int W>
+struct VecW {
+    T v[W];
 };
-template <class T>
-__device__ __forceinline__ Vec4<T> ld4(const T* p)
+template <class T, int W>
+__device__ __forceinline__ VecW<T, W> ldv(const T* p)
 {
-    Vec4<T> r;
-    if constexpr (sizeof(T) == 4) {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-        r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    VecW<T, W> r;
+    if constexpr (sizeof(T) * W == 16) {
+        if constexpr (sizeof(T) == 4) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+            r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+        } else {
+            const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+            r.v[0] = a.x; r.v[1] = a.y;
+        }
+    } else if constexpr (sizeof(T) * W == 8) {
+        const float2 a = __ldg(reinterpret_cast<const float2*>(p));
+        r.v[0] = a.x; r.v[1] = a.y;
     } else {
         const double2 a = __ldg(reinterpret_cast<const double2*>(p));
         const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
@@ -75,39 +83,35 @@ __device__ __forceinline__ Vec4<T> ld4(const T* p)
     }
     return r;
 }
-template <class T>
-__device__ __forceinline__ void st4(T* p, const Vec4<T>& r)
+template <class T, int W>
+__device__ __forceinline__ void stv(T* p, const VecW<T, W>& r)
 {
-    if constexpr (sizeof(T) == 4) {
-        *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+    if constexpr (sizeof(T) * W == 16) {
+        if constexpr (sizeof(T) == 4) *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+        else *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
+    } else if constexpr (sizeof(T) * W == 8) {
+        *reinterpret_cast<float2*>(p) = make_float2(r.v[0], r.v[1]);
     } else {
         reinterpret_cast<double2*>(p)[0] = make_double2(r.v[0], r.v[1]);
         reinterpret_cast<double2*>(p)[1] = make_double2(r.v[2], r.v[3]);
     }
 }
-template <class T>
-__device__ __forceinline__ Vec4<T> zero4()
+template <class T, int W>
+__device__ __forceinline__ VecW<T, W> zerov()
 {
-    Vec4<T> r;
+    VecW<T, W> r;
 #pragma unroll
-    for (int e = 0; e < 4; e++) r.v[e] = T(0);
+    for (int e = 0; e < W; e++) r.v[e] = T(0);
     return r;
 }
 
-// field accessors for the vector kernel: a pointer per colour half, or zero
-template <class T>
-struct Fld {
-    const T* c0;
-    const T* c1;
-    __device__ __forceinline__ const T* half(int col) const { return col ? c1 : c0; }
-};
-
-// the two row neighbours along y or z of the group (AX = 1 or 2, S = -1/+1):
-// vector of u and k values and the face status
-template <class T, int AX, int S>
-__device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int q, int cc, const T* uo, const T* us,
-                                        const T* ko, const T* ks, bool kfield, Vec4<T>& u4, Vec4<T>& k4, int& mask,
-                                        int& dirc)
+// the row neighbour along y or z of a group (AX = 1 or 2, S = -1/+1): vectors
+// of u and k values and the face status (wrapped row for periodic faces,
+// same-colour arrays across an odd periodic seam)
+template <class T, int W, int AX, int S>
+__device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int cc, const T* uo, const T* us,
+                                        const T* ko, const T* ks, bool kfield, VecW<T, W>& u4, VecW<T, W>& k4,
+                                        int& mask, int& dirc)
 {
     const int n = AX == 1 ? L.ny : L.nz;
     const int p = AX == 1 ? j : k;
@@ -120,37 +124,41 @@ __device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int 
         if (!L.per[AX]) {  // physical face: no neighbour
             mask = 0;
             dirc = L.bc[2 * AX + (S > 0 ? 1 : 0)] == BC_DIRC;
-            u4 = zero4<T>();
-            k4 = zero4<T>();
+            u4 = zerov<T, W>();
+            k4 = zerov<T, W>();
             return;
         }
         pq = pq < 0 ? n - 1 : 0;
-        // the wrapped row's colour for this group: (i + j' + k') & 1 with i parity q (of colour cc)
         const int jj = AX == 1 ? pq : j, kk = AX == 2 ? pq : k;
         const int ncol = ((2 * h0 + ((j + k + cc) & 1)) + jj + kk) & 1;
         if (ncol == cc) { ub = us; kb = ks; }
     }
     const int jj = AX == 1 ? pq : j, kk = AX == 2 ? pq : k;
     const int off = h0 + L.P * (jj + L.ny * kk);
-    u4 = ub ? ld4(ub + off) : zero4<T>();
-    k4 = kfield ? ld4(kb + off) : zero4<T>();
-    (void)q;
+    u4 = ub ? ldv<T, W>(ub + off) : zerov<T, W>();
+    k4 = kfield ? ldv<T, W>(kb + off) : zerov<T, W>();
 }
 
-template <class T, class U>
-__global__ void __launch_bounds__(TPB) k_colour4(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
-                                                 const T* __restrict__ f)
+// colour pass on a uniform level, W consecutive cells of one colour per thread
+// (vector loads).  Row (j,k), group g: split offsets o0..o0+W-1 with
+// o0 = W g + P (j + ny k); i = 2(W g + e) + q, q = (j+k+c)&1.  The x
+// neighbours of the group are the other colour at o0+q-1 .. o0+q+W-1 (one
+// vector plus one scalar), the y/z neighbours one vector each.  Elements past
+// the end of the row (pads) are written as 0.  Same results as k_colour.
+template <class T, int W, class U>
+__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
+                                                    const T* __restrict__ f, FastDiv divG)
 {
-    const unsigned G = (unsigned)L.P >> 2;  // groups per row
+    const unsigned G = (unsigned)L.P / W;  // groups per row
     const unsigned t = blockIdx.x * TPB + threadIdx.x;
-    const unsigned row = L.divG.div(t);
+    const unsigned row = divG.div(t);
     if (row >= L.rows) return;
     const int g = (int)(t - row * G);
     const int k = (int)L.divNy.div(row);
     const int j = (int)row - k * L.ny;
     const int cc = c, oc = c ^ 1;
     const int q = (j + k + c) & 1;
-    const int h0 = 4 * g;
+    const int h0 = W * g;
     const int o0 = h0 + L.P * (int)row;
     const bool kfield = op.k[0] != nullptr;
     const T* uo = u.ptr(oc);
@@ -159,93 +167,95 @@ __global__ void __launch_bounds__(TPB) k_colour4(Lev L, KOp<T> op, int c, U u, T
     const T* ks = kfield ? sel(op.k, cc) : nullptr;
     const T cx = (T)L.cr[0], cy = (T)L.cr[1], cz = (T)L.cr[2];
 
-    // own values
-    const Vec4<T> f4 = ld4(f + o0);
-    const Vec4<T> kc4 = kfield ? ld4(ks + o0) : zero4<T>();
-    Vec4<T> d4;
-    if (op.dex[0]) d4 = ld4(sel(op.dex, cc) + o0);
-    else {
-#pragma unroll
-        for (int e = 0; e < 4; e++) d4.v[e] = op.dexc;
+    VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
+    const VecW<T, W> kc4 = kfield ? ldv<T, W>(ks + o0) : zerov<T, W>();
+    int dcount_y = 0, dcount_z = 0;
+    // y and z faces, accumulated one at a time
+#define MPS_YZ(AXV, SV, CF, DC)                                                                               \
+    {                                                                                                         \
+        VecW<T, W> un, kn;                                                                                    \
+        int m, dd;                                                                                            \
+        yz_face<T, W, AXV, SV>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);                       \
+        DC += dd;                                                                                             \
+        if (m) {                                                                                              \
+            _Pragma("unroll") for (int e = 0; e < W; e++)                                                     \
+            {                                                                                                 \
+                const T w = kfield ? (kc4.v[e] + kn.v[e]) * (CF) : (CF);                                      \
+                wsum.v[e] += w;                                                                               \
+                acc.v[e] += w * un.v[e];                                                                      \
+            }                                                                                                 \
+        }                                                                                                     \
     }
+    MPS_YZ(1, -1, cy, dcount_y)
+    MPS_YZ(1, 1, cy, dcount_y)
+    MPS_YZ(2, -1, cz, dcount_z)
+    MPS_YZ(2, 1, cz, dcount_z)
+#undef MPS_YZ
 
-    // x neighbours: A = other colour at o0..o0+3, S = o0+4 (q=1) or o0-1 (q=0)
-    const Vec4<T> ax = uo ? ld4(uo + o0) : zero4<T>();
-    const Vec4<T> akx = kfield ? ld4(ko + o0) : zero4<T>();
-    int so = q ? o0 + 4 : o0 - 1;
-    bool sok = q ? (h0 + 4 < L.P) : (h0 > 0);
+    // x neighbours: A = other colour at o0..o0+W-1, S = o0+W (q=1) or o0-1 (q=0)
+    const VecW<T, W> ax = uo ? ldv<T, W>(uo + o0) : zerov<T, W>();
+    const VecW<T, W> akx = kfield ? ldv<T, W>(ko + o0) : zerov<T, W>();
+    const int so = q ? o0 + W : o0 - 1;
+    const bool sok = q ? (h0 + W < L.P) : (h0 > 0);
     T sx = T(0), skx = T(0);
     if (sok) {
         sx = u.ld(uo, so);
         skx = kfield ? __ldg(ko + so) : T(0);
     }
-
-    // y/z neighbours
-    Vec4<T> uym, kym, uyp, kyp, uzm, kzm, uzp, kzp;
-    int mym, myp, mzm, mzp, dym, dyp, dzm, dzp;
-    yz_face<T, 1, -1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uym, kym, mym, dym);
-    yz_face<T, 1, 1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uyp, kyp, myp, dyp);
-    yz_face<T, 2, -1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uzm, kzm, mzm, dzm);
-    yz_face<T, 2, 1>(L, j, k, h0, q, cc, uo, us, ko, ks, kfield, uzp, kzp, mzp, dzp);
-
-    Vec4<T> res;
+    const VecW<T, W> f4 = ldv<T, W>(f + o0);
+    VecW<T, W> res;
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
+    for (int e = 0; e < W; e++) {
         const int i = 2 * (h0 + e) + q;
-        // x-: other colour at h0+e+q-1 ; x+: at h0+e+q
         T uxm, kxm, uxp, kxp;
         if (q) {
             uxm = ax.v[e]; kxm = akx.v[e];
-            uxp = e < 3 ? ax.v[e + 1] : sx; kxp = e < 3 ? akx.v[e + 1] : skx;
+            uxp = e < W - 1 ? ax.v[e + 1] : sx; kxp = e < W - 1 ? akx.v[e + 1] : skx;
         } else {
             uxm = e > 0 ? ax.v[e - 1] : sx; kxm = e > 0 ? akx.v[e - 1] : skx;
             uxp = ax.v[e]; kxp = akx.v[e];
         }
         T mxm = T(1), mxp = T(1);
-        T dxm = T(0), dxp = T(0);
+        int dx = 0;
         if (i == 0) {  // x- boundary / periodic wrap
             if (L.per[0]) {
                 const int a = L.nx - 1;
-                const int ncol = (a + j + k) & 1;
                 const int wo = (a >> 1) + L.P * (int)row;
-                if (ncol == cc) { uxm = u.ld(us, wo); kxm = kfield ? __ldg(ks + wo) : T(0); }
-                else { uxm = u.ld(uo, wo); kxm = kfield ? __ldg(ko + wo) : T(0); }
+                const T* ub = (((a + j + k) & 1) == cc) ? us : uo;
+                const T* kb = (((a + j + k) & 1) == cc) ? ks : ko;
+                uxm = u.ld(ub, wo);
+                kxm = kfield ? __ldg(kb + wo) : T(0);
             } else {
                 mxm = T(0);
-                dxm = L.bc[0] == BC_DIRC ? T(1) : T(0);
+                dx += L.bc[0] == BC_DIRC;
             }
         }
         if (i == L.nx - 1) {  // x+ boundary / periodic wrap
             if (L.per[0]) {
-                const int ncol = (j + k) & 1;
                 const int wo = L.P * (int)row;
-                if (ncol == cc) { uxp = u.ld(us, wo); kxp = kfield ? __ldg(ks + wo) : T(0); }
-                else { uxp = u.ld(uo, wo); kxp = kfield ? __ldg(ko + wo) : T(0); }
+                const T* ub = (((j + k) & 1) == cc) ? us : uo;
+                const T* kb = (((j + k) & 1) == cc) ? ks : ko;
+                uxp = u.ld(ub, wo);
+                kxp = kfield ? __ldg(kb + wo) : T(0);
             } else {
                 mxp = T(0);
-                dxp = L.bc[1] == BC_DIRC ? T(1) : T(0);
+                dx += L.bc[1] == BC_DIRC;
             }
         }
         const T kc = kfield ? kc4.v[e] : op.kc;
-        T diag, acc;
-        if (kfield) {
-            const T w0 = mxm * (kc + kxm) * cx, w1 = mxp * (kc + kxp) * cx;
-            const T w2 = (T)mym * (kc + kym.v[e]) * cy, w3 = (T)myp * (kc + kyp.v[e]) * cy;
-            const T w4 = (T)mzm * (kc + kzm.v[e]) * cz, w5 = (T)mzp * (kc + kzp.v[e]) * cz;
-            const T bnd = T(2) * kc * ((dxm + dxp) * cx + (T)(dym + dyp) * cy + (T)(dzm + dzp) * cz);
-            diag = d4.v[e] + T(0.5) * (((w0 + w1) + (w2 + w3)) + (w4 + w5)) + bnd;
-            acc = T(0.5) * (((w0 * uxm + w1 * uxp) + (w2 * uym.v[e] + w3 * uyp.v[e])) +
-                            (w4 * uzm.v[e] + w5 * uzp.v[e]));
-        } else {
-            const T sw = (mxm + mxp) * cx + (T)(mym + myp) * cy + (T)(mzm + mzp) * cz +
-                         T(2) * ((dxm + dxp) * cx + (T)(dym + dyp) * cy + (T)(dzm + dzp) * cz);
-            diag = d4.v[e] + kc * sw;
-            acc = kc * ((cx * (mxm * uxm + mxp * uxp) + cy * (uym.v[e] * (T)mym + uyp.v[e] * (T)myp)) +
-                        cz * (uzm.v[e] * (T)mzm + uzp.v[e] * (T)mzp));
-        }
-        res.v[e] = i < L.nx ? gs_value(f4.v[e], diag, -acc) : T(0);
+        const T d0 = op.dex[0] ? __ldg(sel(op.dex, cc) + o0 + e) : op.dexc;
+        T w0, w1;
+        if (kfield) { w0 = mxm * (kc + kxm) * cx; w1 = mxp * (kc + kxp) * cx; }
+        else { w0 = mxm * cx; w1 = mxp * cx; }
+        const T ws = wsum.v[e] + (w0 + w1);
+        const T ac = acc.v[e] + (w0 * uxm + w1 * uxp);
+        const T bnd = T(2) * ((T)dx * cx + (T)dcount_y * cy + (T)dcount_z * cz);
+        T diag, off;
+        if (kfield) { diag = d0 + T(0.5) * ws + kc * bnd; off = T(-0.5) * ac; }
+        else { diag = d0 + kc * (ws + bnd); off = -kc * ac; }
+        res.v[e] = i < L.nx ? gs_value(f4.v[e], diag, off) : T(0);
     }
-    st4(out + o0, res);
+    stv<T, W>(out + o0, res);
 }
 
 // ---------------------------------------------------------------------

@@ -468,16 +468,20 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     if (l == 0) prof_begin(ctx, MPS_PROF_SMOOTH);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (L.uniform) {
-            const unsigned nb4 = nblk((long long)(L.P / 4) * L.rows);
+            // vector kernel: 4 cells per thread in FP32, 2 in FP64
+            constexpr int W = sizeof(T) == 4 ? 4 : 2;
+            FastDiv dg;
+            dg.init((unsigned)(L.P / W));
+            const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
             if (zero_state == 2) {
-                k_colour4<T, ZeroU<T>><<<nb4, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh);
+                k_colourv<T, W, ZeroU<T>><<<nbv, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh, dg);
             } else if (zero_state == 1) {
                 OtherOnlyU<T> u;
                 u.c = c;
                 u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
-                k_colour4<T, OtherOnlyU<T>><<<nb4, TPB, 0, ctx.s>>>(L, op, c, u, out, fh);
+                k_colourv<T, W, OtherOnlyU<T>><<<nbv, TPB, 0, ctx.s>>>(L, op, c, u, out, fh, dg);
             } else {
-                k_colour4<T, CSplit<T>><<<nb4, TPB, 0, ctx.s>>>(L, op, c, ccur(H, L, l), out, fh);
+                k_colourv<T, W, CSplit<T>><<<nbv, TPB, 0, ctx.s>>>(L, op, c, ccur(H, L, l), out, fh, dg);
             }
             if (l == 0) prof_end(ctx);
             CKL();
