@@ -136,7 +136,7 @@ __host__ __device__ __forceinline__ P sel(const P* two, int c)
 template <class T>
 struct Split {  // a field in split layout: c[0] red half, c[1] black half
     T* c[2];
-    __device__ __forceinline__ T* half(int col) const { return col ? c[1] : c[0]; }
+    __host__ __device__ __forceinline__ T* half(int col) const { return col ? c[1] : c[0]; }
     __device__ __forceinline__ T get(const Lev& L, int i, int j, int k) const
     {
         return half(scol(i, j, k))[soff(L, i, j, k)];
@@ -145,7 +145,7 @@ struct Split {  // a field in split layout: c[0] red half, c[1] black half
 template <class T>
 struct CSplit {
     const T* c[2];
-    __device__ __forceinline__ const T* half(int col) const { return col ? c[1] : c[0]; }
+    __host__ __device__ __forceinline__ const T* half(int col) const { return col ? c[1] : c[0]; }
     __device__ __forceinline__ T get(const Lev& L, int i, int j, int k) const
     {
         return __ldg(&half(scol(i, j, k))[soff(L, i, j, k)]);

@@ -17,97 +17,73 @@ __global__ void k_gj_prepare(int n, const double* A, double* M)
 
 __global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* Mg, double* AinvT, int* status, int smem)
 {
+    // 32 x 32 threads: lanes stride columns, warps stride rows
     extern __shared__ double Ms[];
-    double* M = smem ? Ms : Mg;
-    if (smem) {
-        for (long long t = threadIdx.x; t < 2LL * n * n; t += blockDim.x) Ms[t] = Mg[t];
-        __syncthreads();
-    }
-    __shared__ double sval[32];
-    __shared__ int sidx[32];
     __shared__ double fac[1024];
-    __shared__ double s_scale;
-    __shared__ int s_piv;
     __shared__ unsigned char sing[1024];
-    const long long ld = 2LL * n;
+    __shared__ int s_piv;
+    __shared__ double s_scale;
+    const int ld = 2 * n;
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    double* M = smem ? Ms : Mg;
+    if (smem)
+        for (int t = tid; t < 2 * n * n; t += nt) Ms[t] = Mg[t];
     for (int r = tid; r < n; r += nt) sing[r] = 0;
     __syncthreads();
-
-    // scale of the matrix for the singular-pivot threshold
-    double mx = 0.0;
-    for (long long t = tid; t < (long long)n * n; t += nt) {
-        long long r = t / n, c = t - r * n;
-        mx = fmax(mx, fabs(M[r * ld + c]));
-    }
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
-    if ((tid & 31) == 0) sval[tid >> 5] = mx;
-    __syncthreads();
-    if (tid == 0) {
-        double m = 0.0;
-        for (int w = 0; w < (nt >> 5); w++) m = fmax(m, sval[w]);
-        s_scale = m;
+    // scale of the matrix for the singular-pivot threshold (warp 0)
+    if (wid == 0) {
+        double mx = 0.0;
+        for (int r = 0; r < n; r++)
+            for (int c = lane; c < n; c += 32) mx = fmax(mx, fabs(M[r * ld + c]));
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+        if (lane == 0) s_scale = mx;
     }
     __syncthreads();
     const double tiny = 1e-13 * s_scale;
-
     for (int p = 0; p < n; p++) {
-        // pivot search in column p, rows p..n-1
-        double best = -1.0;
-        int bi = p;
-        for (int r = p + tid; r < n; r += nt) {
-            double v = fabs(M[(long long)r * ld + p]);
-            if (v > best) { best = v; bi = r; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            double ov = __shfl_down_sync(0xffffffffu, best, o);
-            int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-        }
-        if ((tid & 31) == 0) { sval[tid >> 5] = best; sidx[tid >> 5] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            double b = -1.0;
-            int ix = p;
-            for (int w = 0; w < (nt >> 5); w++)
-                if (sval[w] > b || (sval[w] == b && sidx[w] < ix)) { b = sval[w]; ix = sidx[w]; }
-            s_piv = (b > tiny) ? ix : -1;
+        // pivot: largest |M[r][p]|, r >= p (warp 0)
+        if (wid == 0) {
+            double best = -1.0;
+            int bi = p;
+            for (int r = p + lane; r < n; r += 32) {
+                const double v = fabs(M[r * ld + p]);
+                if (v > best) { best = v; bi = r; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) {
+                s_piv = best > tiny ? bi : -1;
+                if (best <= tiny) { atomicOr(status, 1); sing[p] = 1; }
+            }
         }
         __syncthreads();
         const int piv = s_piv;
-        if (piv < 0) {
-            // singular direction: skip the column; the inverse row is zeroed at
-            // the end so the solve returns the particular solution with this
-            // unknown at zero
-            if (tid == 0) { atomicOr(status, 1); sing[p] = 1; }
-            __syncthreads();
-            continue;
-        }
+        if (piv < 0) continue;  // singular direction: left for the zeroed inverse row
         if (piv != p)
-            for (long long c = tid; c < ld; c += nt) {
-                double a = M[(long long)p * ld + c];
-                M[(long long)p * ld + c] = M[(long long)piv * ld + c];
-                M[(long long)piv * ld + c] = a;
+            for (int c = tid; c < ld; c += nt) {
+                const double a = M[p * ld + c];
+                M[p * ld + c] = M[piv * ld + c];
+                M[piv * ld + c] = a;
             }
         __syncthreads();
-        const double inv = 1.0 / M[(long long)p * ld + p];
+        const double inv = 1.0 / M[p * ld + p];
+        for (int r = tid; r < n; r += nt) fac[r] = (r == p) ? 0.0 : M[r * ld + p];
         __syncthreads();
-        for (long long c = tid; c < ld; c += nt) M[(long long)p * ld + c] *= inv;
+        for (int c = p + tid; c < ld; c += nt) M[p * ld + c] *= inv;
         __syncthreads();
-        for (int r = tid; r < n; r += nt) fac[r] = (r == p) ? 0.0 : M[(long long)r * ld + p];
-        __syncthreads();
-        const long long width = ld - p;
-        for (long long t = tid; t < (long long)n * width; t += nt) {
-            long long r = t / width, c = p + (t - r * width);
-            double f = fac[r];
-            if (f != 0.0) M[r * ld + c] -= f * M[(long long)p * ld + c];
+        for (int r = wid; r < n; r += nw) {
+            const double f = fac[r];
+            if (f != 0.0)
+                for (int c = p + lane; c < ld; c += 32) M[r * ld + c] -= f * M[p * ld + c];
         }
         __syncthreads();
     }
-    for (long long t = tid; t < (long long)n * n; t += nt) {
-        long long r = t / n, c = t - r * n;
-        AinvT[c * n + r] = sing[r] ? 0.0 : M[r * ld + n + c];
-    }
+    for (int r = wid; r < n; r += nw)
+        for (int c = lane; c < n; c += 32) AinvT[(long long)c * n + r] = sing[r] ? 0.0 : M[r * ld + n + c];
 }
 
 // ---------------------------------------------------------------------

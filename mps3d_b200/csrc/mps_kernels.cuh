@@ -9,6 +9,27 @@ namespace mps {
 
 constexpr int TPB = 256;
 
+struct RedBuf {
+    double* partial;      // [2 * maxblocks]
+    unsigned* counter;    // zero-initialised
+    double* out;          // [2]: sum r^2, sum f^2
+};
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    __syncthreads();
+    return s;  // valid in thread 0
+}
+
 template <class T>
 struct ZeroU {  // accessor of a field known to be zero
     __device__ __forceinline__ T get(const Lev&, int, int, int) const { return T(0); }
@@ -139,27 +160,18 @@ __device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int 
     k4 = kfield ? ldv<T, W>(kb + off) : zerov<T, W>();
 }
 
-// colour pass on a uniform level, W consecutive cells of one colour per thread
+// Row evaluation of W consecutive cells of one colour on a uniform level
 // (vector loads).  Row (j,k), group g: split offsets o0..o0+W-1 with
 // o0 = W g + P (j + ny k); i = 2(W g + e) + q, q = (j+k+c)&1.  The x
 // neighbours of the group are the other colour at o0+q-1 .. o0+q+W-1 (one
-// vector plus one scalar), the y/z neighbours one vector each.  Elements past
-// the end of the row (pads) are written as 0.  Same results as k_colour.
+// vector plus one scalar), the y/z neighbours one vector each.  Returns
+// diag and offdiag (sum_n a_n u_n) per element; elements with i >= nx are
+// padding.
 template <class T, int W, class U>
-__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
-                                                    const T* __restrict__ f, FastDiv divG)
+__device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c, const U& u, int row, int j,
+                                           int k, int h0, int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
 {
-    const unsigned G = (unsigned)L.P / W;  // groups per row
-    const unsigned t = blockIdx.x * TPB + threadIdx.x;
-    const unsigned row = divG.div(t);
-    if (row >= L.rows) return;
-    const int g = (int)(t - row * G);
-    const int k = (int)L.divNy.div(row);
-    const int j = (int)row - k * L.ny;
     const int cc = c, oc = c ^ 1;
-    const int q = (j + k + c) & 1;
-    const int h0 = W * g;
-    const int o0 = h0 + L.P * (int)row;
     const bool kfield = op.k[0] != nullptr;
     const T* uo = u.ptr(oc);
     const T* us = u.ptr(cc);
@@ -202,8 +214,6 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, 
         sx = u.ld(uo, so);
         skx = kfield ? __ldg(ko + so) : T(0);
     }
-    const VecW<T, W> f4 = ldv<T, W>(f + o0);
-    VecW<T, W> res;
 #pragma unroll
     for (int e = 0; e < W; e++) {
         const int i = 2 * (h0 + e) + q;
@@ -220,11 +230,10 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, 
         if (i == 0) {  // x- boundary / periodic wrap
             if (L.per[0]) {
                 const int a = L.nx - 1;
-                const int wo = (a >> 1) + L.P * (int)row;
-                const T* ub = (((a + j + k) & 1) == cc) ? us : uo;
-                const T* kb = (((a + j + k) & 1) == cc) ? ks : ko;
-                uxm = u.ld(ub, wo);
-                kxm = kfield ? __ldg(kb + wo) : T(0);
+                const int wo = (a >> 1) + L.P * row;
+                const bool same = ((a + j + k) & 1) == cc;
+                uxm = u.ld(same ? us : uo, wo);
+                kxm = kfield ? __ldg((same ? ks : ko) + wo) : T(0);
             } else {
                 mxm = T(0);
                 dx += L.bc[0] == BC_DIRC;
@@ -232,11 +241,10 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, 
         }
         if (i == L.nx - 1) {  // x+ boundary / periodic wrap
             if (L.per[0]) {
-                const int wo = L.P * (int)row;
-                const T* ub = (((j + k) & 1) == cc) ? us : uo;
-                const T* kb = (((j + k) & 1) == cc) ? ks : ko;
-                uxp = u.ld(ub, wo);
-                kxp = kfield ? __ldg(kb + wo) : T(0);
+                const int wo = L.P * row;
+                const bool same = ((j + k) & 1) == cc;
+                uxp = u.ld(same ? us : uo, wo);
+                kxp = kfield ? __ldg((same ? ks : ko) + wo) : T(0);
             } else {
                 mxp = T(0);
                 dx += L.bc[1] == BC_DIRC;
@@ -250,12 +258,150 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, 
         const T ws = wsum.v[e] + (w0 + w1);
         const T ac = acc.v[e] + (w0 * uxm + w1 * uxp);
         const T bnd = T(2) * ((T)dx * cx + (T)dcount_y * cy + (T)dcount_z * cz);
-        T diag, off;
-        if (kfield) { diag = d0 + T(0.5) * ws + kc * bnd; off = T(-0.5) * ac; }
-        else { diag = d0 + kc * (ws + bnd); off = -kc * ac; }
-        res.v[e] = i < L.nx ? gs_value(f4.v[e], diag, off) : T(0);
+        if (kfield) { diag.v[e] = d0 + T(0.5) * ws + kc * bnd; off.v[e] = T(-0.5) * ac; }
+        else { diag.v[e] = d0 + kc * (ws + bnd); off.v[e] = -kc * ac; }
     }
-    stv<T, W>(out + o0, res);
+}
+
+// decode the group index of a vector launch
+struct GroupIdx {
+    int row, j, k, h0, q, o0;
+};
+template <int W>
+__device__ __forceinline__ bool group_decode(const Lev& L, const FastDiv& divG, int c, GroupIdx& G)
+{
+    const unsigned ng = (unsigned)L.P / W;
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned row = divG.div(t);
+    if (row >= L.rows) return false;
+    G.row = (int)row;
+    G.k = (int)L.divNy.div(row);
+    G.j = (int)row - G.k * L.ny;
+    G.h0 = W * (int)(t - row * ng);
+    G.q = (G.j + G.k + c) & 1;
+    G.o0 = G.h0 + L.P * (int)row;
+    return true;
+}
+
+// colour pass on a uniform level: W cells of colour c per thread.  Elements
+// past the end of the row (pads) are written as 0.  Same results as k_colour.
+template <class T, int W, class U>
+__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
+                                                    const T* __restrict__ f, FastDiv divG)
+{
+    GroupIdx G;
+    if (!group_decode<W>(L, divG, c, G)) return;
+    VecW<T, W> diag, off;
+    group_rows<T, W, U>(L, op, c, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
+    const VecW<T, W> f4 = ldv<T, W>(f + G.o0);
+    VecW<T, W> res;
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int i = 2 * (G.h0 + e) + G.q;
+        res.v[e] = i < L.nx ? gs_value(f4.v[e], diag.v[e], off.v[e]) : T(0);
+    }
+    stv<T, W>(out + G.o0, res);
+}
+
+// residual of colour c on a uniform level, W cells per thread: r = f - A u
+// (u, f of type T), optional r out (type R, split half c), and the sums of
+// r^2 and f^2 reduced deterministically (accumulate = add to rb.out, for the
+// second colour)
+template <class T, int W, class R>
+__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_residv(Lev L, KOp<T> op, int c, CSplit<T> u,
+                                                                       const T* __restrict__ f, R* __restrict__ rout,
+                                                                       RedBuf rb, int accumulate, FastDiv divG)
+{
+    __shared__ double sh[32];
+    double rr = 0.0, ff = 0.0;
+    GroupIdx G;
+    if (group_decode<W>(L, divG, c, G)) {
+        VecW<T, W> diag, off;
+        group_rows<T, W, CSplit<T>>(L, op, c, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
+        const VecW<T, W> f4 = ldv<T, W>(f + G.o0);
+        const VecW<T, W> u4 = ldv<T, W>(u.half(c) + G.o0);
+        VecW<R, W> r4;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+            const int i = 2 * (G.h0 + e) + G.q;
+            const T r = f4.v[e] - (diag.v[e] * u4.v[e] + off.v[e]);
+            const bool ok = i < L.nx;
+            r4.v[e] = ok ? (R)r : R(0);
+            if (ok) {
+                rr += (double)r * (double)r;
+                ff += (double)f4.v[e] * (double)f4.v[e];
+            }
+        }
+        if (rout) stv<R, W>(rout + G.o0, r4);
+    }
+    const double a = block_sum(rr, sh);
+    const double b = block_sum(ff, sh);
+    if (!rb.partial) return;
+    // finish: last block sums the partials in block order
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        rb.partial[2 * blockIdx.x] = a;
+        rb.partial[2 * blockIdx.x + 1] = b;
+        __threadfence();
+        last = (atomicAdd(rb.counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for (unsigned qd = threadIdx.x; qd < gridDim.x; qd += blockDim.x) {
+        sa += ((volatile double*)rb.partial)[2 * qd];
+        sb += ((volatile double*)rb.partial)[2 * qd + 1];
+    }
+    sa = block_sum(sa, sh);
+    sb = block_sum(sb, sh);
+    if (threadIdx.x == 0) {
+        rb.out[0] = accumulate ? rb.out[0] + sa : sa;
+        rb.out[1] = accumulate ? rb.out[1] + sb : sb;
+        *rb.counter = 0u;
+    }
+}
+
+// restriction of a residual held in split layout (type T) to the coarse
+// right-hand side: mean (volume-weighted for the geometric hierarchy) over
+// the children; with red_only the black children count as 0 (the residual of
+// the colour updated last vanishes up to rounding)
+template <class T>
+__global__ void __launch_bounds__(TPB) k_restrict_res(Lev F, CSplit<T> r, Lev C, Split<T> fc, int geom, int red_only)
+{
+    unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned ncx = C.nx, ncy = C.ny;
+    if (t >= ncx * ncy * (unsigned)C.nz) return;
+    unsigned K = t / (ncx * ncy);
+    unsigned rem = t - K * ncx * ncy;
+    unsigned J = rem / ncx;
+    unsigned I = rem - J * ncx;
+    const int cI[3] = {(int)I, (int)J, (int)K};
+    int lo[3], cnt[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const int nf = lev_n(F, a), nc = lev_n(C, a);
+        lo[a] = nf == nc ? cI[a] : 2 * cI[a];
+        cnt[a] = nf == nc ? 1 : ((geom && cI[a] == nc - 1) ? nf - 2 * (nc - 1) : 2);
+    }
+    T s = T(0), vol = T(0);
+    for (int dk = 0; dk < cnt[2]; dk++) {
+        const int k = lo[2] + dk;
+        const T wz = geom ? (T)cwidth(F, 2, k) : T(1);
+        for (int dj = 0; dj < cnt[1]; dj++) {
+            const int j = lo[1] + dj;
+            const T wy = geom ? (T)cwidth(F, 1, j) : T(1);
+            for (int di = 0; di < cnt[0]; di++) {
+                const int i = lo[0] + di;
+                const T wx = geom ? (T)cwidth(F, 0, i) : T(1);
+                const T v = wx * wy * wz;
+                const int col = (i + j + k) & 1;
+                if (!red_only || col == 0) s += v * r.get(F, i, j, k);
+                vol += v;
+            }
+        }
+    }
+    fc.half(scol(I, J, K))[soff(C, I, J, K)] = s / vol;
 }
 
 // ---------------------------------------------------------------------
@@ -348,15 +494,22 @@ __device__ __forceinline__ T coarse_at(const Lev& C, const CSplit<T>& e, int I, 
 // per fine cell.
 // ---------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X)
+__global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, int only_col)
 {
-    unsigned t = blockIdx.x * TPB + threadIdx.x;
-    const unsigned nx = F.nx, ny = F.ny;
-    if (t >= nx * ny * (unsigned)F.nz) return;
-    unsigned k = t / (nx * ny);
-    unsigned rem = t - k * nx * ny;
-    unsigned j = rem / nx;
-    unsigned i = rem - j * nx;
+    unsigned i, j, k;
+    if (only_col < 0) {  // all cells, natural order
+        unsigned t = blockIdx.x * TPB + threadIdx.x;
+        const unsigned nx = F.nx, ny = F.ny;
+        if (t >= nx * ny * (unsigned)F.nz) return;
+        k = t / (nx * ny);
+        unsigned rem = t - k * nx * ny;
+        j = rem / nx;
+        i = rem - j * nx;
+    } else {  // the cells of one colour, split order (coalesced on that half)
+        int ii, jj, kk;
+        if (!decode(F, blockIdx.x * TPB + threadIdx.x, only_col, ii, jj, kk)) return;
+        i = ii; j = jj; k = kk;
+    }
     T v;
     if (!X.geom) {
         int I = i >> 1, J = j >> 1, K = k >> 1;
@@ -476,27 +629,6 @@ __global__ void k_gj_prepare(int n, const double* A, double* M);
 // deterministically (per-block partials, the last block sums them in
 // block order).  Optionally writes r (converted to R) to a split field.
 // ---------------------------------------------------------------------
-struct RedBuf {
-    double* partial;      // [2 * maxblocks]
-    unsigned* counter;    // zero-initialised
-    double* out;          // [2]: sum r^2, sum f^2
-};
-
-__device__ __forceinline__ double block_sum(double v, double* sh)
-{
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) sh[w] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x < 32) {
-        s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    }
-    __syncthreads();
-    return s;  // valid in thread 0
-}
-
 __device__ __forceinline__ void finish_two(RedBuf rb, double a, double b, double* sh)
 {
     __shared__ bool last;

@@ -79,6 +79,7 @@ template <class T>
 struct Hier {
     T* U[MAXL][2] = {};  // two full split buffers (2*half) per level
     T* F[MAXL] = {};     // right-hand side (split)
+    T* R[MAXL] = {};     // residual scratch (split)
     int ri[MAXL] = {}, bi[MAXL] = {};
     KOp<T> kop[MAXL];
     ROp<T> rop[MAXL];
@@ -455,6 +456,11 @@ static int run_graph(Ctx& ctx, const GraphKey& key, GraphEntry** out, F&& body)
     return 0;
 }
 
+static bool odd_periodic(const Lev& L)
+{
+    return (L.per[0] && (L.nx & 1)) || (L.per[1] && (L.ny & 1)) || (L.per[2] && (L.nz & 1));
+}
+
 // ---- one colour pass ----
 template <class T, class Op>
 static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zero_state)
@@ -535,14 +541,46 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         CK(cudaMemsetAsync(H.U[l][H.bi[l]] + L.half, 0, sizeof(T) * L.half, ctx.s));
     }
     if (l == 0) prof_begin(ctx, MPS_PROF_RESTRICT);
-    k_resid_restrict<T, Op><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
-        L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom);
+    bool done = false;
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (L.uniform) {
+            // residual of the red colour (vector kernel) + restriction; after a
+            // black pass the black residual vanishes except across odd periodic seams
+            constexpr int W = sizeof(T) == 4 ? 4 : 2;
+            FastDiv dg;
+            dg.init((unsigned)(L.P / W));
+            const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
+            RedBuf none;
+            none.partial = nullptr;
+            none.counter = nullptr;
+            none.out = nullptr;
+            const bool both = o->nu1 == 0 || odd_periodic(L);
+            for (int c = 0; c < (both ? 2 : 1); c++) {
+                k_residv<T, W, T><<<nbv, TPB, 0, ctx.s>>>(L, ops[l], c, ccur(H, L, l), H.F[l] + (c ? L.half : 0),
+                                                           H.R[l] + (c ? L.half : 0), none, 0, dg);
+                CKL();
+            }
+            k_restrict_res<T><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
+                L, csplit<T>(H.R[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, both ? 0 : 1);
+            done = true;
+        }
+    }
+    if (!done)
+        k_resid_restrict<T, Op><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
+            L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom);
     if (l == 0) prof_end(ctx);
     CKL();
     if ((st = vcycle_rec(ctx, H, ops, l + 1, o, true))) return st;
     if (l == 0) prof_begin(ctx, MPS_PROF_PROLONG);
-    k_prolong_correct<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
-        L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l]);
+    // the first post-smoothing pass overwrites the red cells from the black
+    // ones, so only black cells need the correction (unless an odd periodic
+    // seam makes red cells read red neighbours)
+    if (o->nu2 >= 1 && !odd_periodic(L))
+        k_prolong_correct<T><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, cur(H, L, l), C,
+                                                                               ccur(H, C, l + 1), ctx.xf[l], 1);
+    else
+        k_prolong_correct<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
+            L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l], -1);
     if (l == 0) prof_end(ctx);
     CKL();
     for (int s = 0; s < o->nu2; s++) {
@@ -565,6 +603,21 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
 {
     const Lev& L = ctx.lev[0];
     prof_begin(ctx, MPS_PROF_RESID);
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (L.uniform) {  // vector kernel, one launch per colour, norms accumulated
+            constexpr int W = sizeof(T) == 4 ? 4 : 2;
+            FastDiv dg;
+            dg.init((unsigned)(L.P / W));
+            const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
+            for (int c = 0; c < 2; c++) {
+                k_residv<T, W, R><<<nbv, TPB, 0, ctx.s>>>(L, op, c, u, f.half(c), rout.c[0] ? rout.half(c) : nullptr,
+                                                           ctx.rb, c, dg);
+                CKL();
+            }
+            prof_end(ctx);
+            return 0;
+        }
+    }
     k_resid_norm<T, Op, R><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, op, u, f, rout, ctx.rb);
     prof_end(ctx);
     CKL();
@@ -598,8 +651,9 @@ static void alloc_hier(Ctx& ctx, Hier<T>& H, bool& ok)
         H.U[l][0] = (T*)ctx.ar.get(b);
         H.U[l][1] = (T*)ctx.ar.get(b);
         H.F[l] = (T*)ctx.ar.get(b);
+        H.R[l] = (T*)ctx.ar.get(b);
         H.ri[l] = H.bi[l] = 0;
-        ok = ok && H.U[l][0] && H.U[l][1] && H.F[l];
+        ok = ok && H.U[l][0] && H.U[l][1] && H.F[l] && H.R[l];
     }
     const Lev& C = ctx.lev[ctx.nlev - 1];
     const long long n = (long long)C.nx * C.ny * C.nz;
