@@ -310,12 +310,30 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, 
 template <class T, int W, class R>
 __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_residv(Lev L, KOp<T> op, int c, CSplit<T> u,
                                                                        const T* __restrict__ f, R* __restrict__ rout,
-                                                                       RedBuf rb, int accumulate, FastDiv divG)
+                                                                       RedBuf rb, int accumulate, FastDiv divG,
+                                                                       int seam_only)
 {
     __shared__ double sh[32];
     double rr = 0.0, ff = 0.0;
-    GroupIdx G;
-    if (group_decode<W>(L, divG, c, G)) {
+    const unsigned ngroups = (unsigned)(L.P / W) * L.rows;
+    // grid-stride: a few hundred blocks keep the norm reduction's tail short
+    for (unsigned base = blockIdx.x * TPB; base < ngroups; base += gridDim.x * TPB) {
+        GroupIdx G;
+        const unsigned t = base + threadIdx.x;
+        const unsigned row = divG.div(t);
+        if (row >= L.rows) continue;
+        G.row = (int)row;
+        G.k = (int)L.divNy.div(row);
+        G.j = (int)row - G.k * L.ny;
+        G.h0 = W * (int)(t - row * (unsigned)(L.P / W));
+        G.q = (G.j + G.k + c) & 1;
+        G.o0 = G.h0 + L.P * (int)row;
+        if (seam_only) {  // only groups touching an odd periodic seam
+            const bool sx = L.per[0] && (L.nx & 1) && (G.h0 == 0 || 2 * (G.h0 + W) + 1 >= L.nx);
+            const bool sy = L.per[1] && (L.ny & 1) && (G.j == 0 || G.j == L.ny - 1);
+            const bool sz = L.per[2] && (L.nz & 1) && (G.k == 0 || G.k == L.nz - 1);
+            if (!(sx || sy || sz)) continue;
+        }
         VecW<T, W> diag, off;
         group_rows<T, W, CSplit<T>>(L, op, c, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
         const VecW<T, W> f4 = ldv<T, W>(f + G.o0);
@@ -384,6 +402,26 @@ __global__ void __launch_bounds__(TPB) k_restrict_res(Lev F, CSplit<T> r, Lev C,
         lo[a] = nf == nc ? cI[a] : 2 * cI[a];
         cnt[a] = nf == nc ? 1 : ((geom && cI[a] == nc - 1) ? nf - 2 * (nc - 1) : 2);
     }
+    // seam children keep their (non-zero) black residual
+    const bool seamx = F.per[0] && (F.nx & 1), seamy = F.per[1] && (F.ny & 1), seamz = F.per[2] && (F.nz & 1);
+    if (cnt[0] == 2 && cnt[1] == 2 && cnt[2] == 2 && (!geom || F.uniform)) {
+        // regular 2x2x2 block of equal cells
+        T s = T(0);
+#pragma unroll
+        for (int dk = 0; dk < 2; dk++)
+#pragma unroll
+            for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+                for (int di = 0; di < 2; di++) {
+                    const int i = lo[0] + di, j = lo[1] + dj, k = lo[2] + dk;
+                    const bool black = ((di + dj + dk + lo[0] + lo[1] + lo[2]) & 1) != 0;
+                    const bool seam = (seamx && (i == 0 || i == F.nx - 1)) || (seamy && (j == 0 || j == F.ny - 1)) ||
+                                      (seamz && (k == 0 || k == F.nz - 1));
+                    if (!red_only || !black || seam) s += r.get(F, i, j, k);
+                }
+        fc.half(scol(I, J, K))[soff(C, I, J, K)] = s * T(0.125);
+        return;
+    }
     T s = T(0), vol = T(0);
     for (int dk = 0; dk < cnt[2]; dk++) {
         const int k = lo[2] + dk;
@@ -396,7 +434,9 @@ __global__ void __launch_bounds__(TPB) k_restrict_res(Lev F, CSplit<T> r, Lev C,
                 const T wx = geom ? (T)cwidth(F, 0, i) : T(1);
                 const T v = wx * wy * wz;
                 const int col = (i + j + k) & 1;
-                if (!red_only || col == 0) s += v * r.get(F, i, j, k);
+                const bool seam = (seamx && (i == 0 || i == F.nx - 1)) || (seamy && (j == 0 || j == F.ny - 1)) ||
+                                  (seamz && (k == 0 || k == F.nz - 1));
+                if (!red_only || col == 0 || seam) s += v * r.get(F, i, j, k);
                 vol += v;
             }
         }
@@ -505,6 +545,14 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
         unsigned rem = t - k * nx * ny;
         j = rem / nx;
         i = rem - j * nx;
+    } else if (only_col == 2) {  // red cells on the odd periodic seam planes
+        int ii, jj, kk;
+        if (!decode(F, blockIdx.x * TPB + threadIdx.x, 0, ii, jj, kk)) return;
+        const bool seam = (F.per[0] && (F.nx & 1) && (ii == 0 || ii == F.nx - 1)) ||
+                          (F.per[1] && (F.ny & 1) && (jj == 0 || jj == F.ny - 1)) ||
+                          (F.per[2] && (F.nz & 1) && (kk == 0 || kk == F.nz - 1));
+        if (!seam) return;
+        i = ii; j = jj; k = kk;
     } else {  // the cells of one colour, split order (coalesced on that half)
         int ii, jj, kk;
         if (!decode(F, blockIdx.x * TPB + threadIdx.x, only_col, ii, jj, kk)) return;

@@ -554,10 +554,15 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             none.partial = nullptr;
             none.counter = nullptr;
             none.out = nullptr;
-            const bool both = o->nu1 == 0 || odd_periodic(L);
-            for (int c = 0; c < (both ? 2 : 1); c++) {
-                k_residv<T, W, T><<<nbv, TPB, 0, ctx.s>>>(L, ops[l], c, ccur(H, L, l), H.F[l] + (c ? L.half : 0),
-                                                           H.R[l] + (c ? L.half : 0), none, 0, dg);
+            // nu1 == 0: both colours in full; odd periodic seams: the black
+            // residual only on the seam planes (elsewhere it vanishes)
+            const bool both = o->nu1 == 0;
+            const bool seams = !both && odd_periodic(L);
+            const unsigned nbg = std::min<unsigned>(nbv, 148 * 8);
+            for (int c = 0; c < ((both || seams) ? 2 : 1); c++) {
+                k_residv<T, W, T><<<c == 1 && seams ? nbg : nbv, TPB, 0, ctx.s>>>(
+                    L, ops[l], c, ccur(H, L, l), H.F[l] + (c ? L.half : 0), H.R[l] + (c ? L.half : 0), none, 0, dg,
+                    (c == 1 && seams) ? 1 : 0);
                 CKL();
             }
             k_restrict_res<T><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
@@ -575,10 +580,15 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     // the first post-smoothing pass overwrites the red cells from the black
     // ones, so only black cells need the correction (unless an odd periodic
     // seam makes red cells read red neighbours)
-    if (o->nu2 >= 1 && !odd_periodic(L))
+    if (o->nu2 >= 1) {
         k_prolong_correct<T><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, cur(H, L, l), C,
                                                                                ccur(H, C, l + 1), ctx.xf[l], 1);
-    else
+        if (odd_periodic(L)) {  // red cells on the seams are read by the next red pass
+            CKL();
+            k_prolong_correct<T><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, cur(H, L, l), C,
+                                                                                   ccur(H, C, l + 1), ctx.xf[l], 2);
+        }
+    } else
         k_prolong_correct<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
             L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l], -1);
     if (l == 0) prof_end(ctx);
@@ -608,10 +618,10 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             constexpr int W = sizeof(T) == 4 ? 4 : 2;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
-            const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
+            const unsigned nbv = std::min<unsigned>(nblk((long long)(L.P / W) * L.rows), 148 * 8);
             for (int c = 0; c < 2; c++) {
                 k_residv<T, W, R><<<nbv, TPB, 0, ctx.s>>>(L, op, c, u, f.half(c), rout.c[0] ? rout.half(c) : nullptr,
-                                                           ctx.rb, c, dg);
+                                                           ctx.rb, c, dg, 0);
                 CKL();
             }
             prof_end(ctx);
