@@ -46,7 +46,8 @@ enum mps_status {
     MPS_ERR_BAD_ARG = 4,
     MPS_ERR_TIMEOUT = 5,       /* a bounded device-side wait expired */
     MPS_ERR_CUDA = 6,
-    MPS_ERR_NOMEM = 7
+    MPS_ERR_NOMEM = 7,
+    MPS_ERR_TOO_LARGE = 8      /* grid beyond MPS_NOALLOC_MAX_CELLS (mps_apply_A_noalloc) */
 };
 
 /* ---- boundary-condition codes (discretepde.f90; PERI is an extension) ---- */
@@ -184,6 +185,32 @@ int mps_get_profile(mps_handle h, mps_profile* p, int reset);
  * wrap), device pointers. */
 int mps_fill_ghosts_dev(mps_handle h, const mps_grid* g, const int bc_code[6],
                         const double* const bcval[6], double* soln, void* stream);
+
+/* AX = A soln like mps_apply_A_dev, for callers that must not allocate device
+ * memory.  No counterpart in the reference: its find_AX works on arrays the
+ * caller already owns, so it never needed one.  Callers that cannot allocate
+ * are, for example, a time-stepping code whose memory pool (its own or
+ * torch's caching allocator) already holds the free HBM, so that cudaMalloc
+ * would fail, and a code that keeps the device busy on its own streams, which
+ * cudaFree would stall by waiting for the whole device.
+ *
+ * No handle: the call works on the current device and calls no cudaMalloc,
+ * cudaFree or allocating library routine.  Its scratch is one static device
+ * array of MPS_NOALLOC_SCRATCH_BYTES (32 MiB) that every device which loads
+ * this library holds until the process exits.  The first call on a device
+ * looks up that array's address on the device; make that first call before
+ * any stream capture begins.  Sizes: round_up(lx, 16) * ly * lz must not
+ * exceed MPS_NOALLOC_MAX_CELLS (64^3), else MPS_ERR_TOO_LARGE and nothing is
+ * launched.  The work is queued on `stream` (NULL = the default stream) and
+ * AX is ready when the stream reaches that point.  All calls share the one
+ * array, so two calls that overlap on the GPU (other streams, other host
+ * threads) race and corrupt each other's results: serialise them.  opts may
+ * be NULL (upwind flux, no transpose); only its flux and transpose are read. */
+#define MPS_NOALLOC_MAX_CELLS 262144
+#define MPS_NOALLOC_SCRATCH_BYTES (16LL * 8LL * MPS_NOALLOC_MAX_CELLS)
+int mps_apply_A_noalloc(const mps_grid* g, int timederiv, double dt, const double* vel,
+                        const double* dcoeff, const double* reac, const int bc_code[6],
+                        const double* soln, double* AX, const mps_solver_opts* opts, void* stream);
 
 #ifdef __cplusplus
 }

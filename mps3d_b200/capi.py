@@ -22,8 +22,12 @@ MPS_ERR_BAD_ARG = 4
 MPS_ERR_TIMEOUT = 5
 MPS_ERR_CUDA = 6
 MPS_ERR_NOMEM = 7
+MPS_ERR_TOO_LARGE = 8
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN", 3: "BREAKDOWN", 4: "BAD_ARG", 5: "TIMEOUT", 6: "CUDA",
-                7: "NOMEM"}
+                7: "NOMEM", 8: "TOO_LARGE"}
+# mps_apply_A_noalloc: round_up(lx, 16) * ly * lz limit and its static scratch
+NOALLOC_MAX_CELLS = 262144
+NOALLOC_SCRATCH_BYTES = 16 * 8 * NOALLOC_MAX_CELLS
 
 HIER_CELL, HIER_GEOM = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
@@ -35,7 +39,7 @@ TOL_RMS_ABS, TOL_REL_L2 = 0, 1
 EXPORTS = [
     "mps_default_opts", "mps_version", "mps_create", "mps_destroy", "mps_stream", "mps_last_error",
     "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once", "mps_apply_A_dev", "mps_find_bvec_dev",
-    "mps_fill_ghosts_dev", "mps_set_profile", "mps_get_profile",
+    "mps_fill_ghosts_dev", "mps_set_profile", "mps_get_profile", "mps_apply_A_noalloc",
 ]
 
 PROF_SMOOTH, PROF_RESTRICT, PROF_PROLONG, PROF_RESID, PROF_NCLASS = 0, 1, 2, 3, 8
@@ -107,8 +111,10 @@ def load(build_if_missing: bool = False):
     L.mps_fill_ghosts_dev.argtypes = [vp, C.POINTER(Grid), ip, C.POINTER(vp), vp, vp]
     L.mps_set_profile.argtypes = [vp, C.c_int]
     L.mps_get_profile.argtypes = [vp, C.POINTER(Profile), C.c_int]
+    L.mps_apply_A_noalloc.argtypes = [C.POINTER(Grid), C.c_int, C.c_double, vp, vp, vp, ip, vp, vp, C.POINTER(Opts),
+                                      vp]
     for name in ("mps_set_profile", "mps_get_profile", "mps_create", "mps_destroy", "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once",
-                 "mps_apply_A_dev", "mps_find_bvec_dev", "mps_fill_ghosts_dev"):
+                 "mps_apply_A_dev", "mps_find_bvec_dev", "mps_fill_ghosts_dev", "mps_apply_A_noalloc"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

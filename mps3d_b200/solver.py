@@ -163,6 +163,27 @@ def apply_A_dev(dp: DeviceProblem, soln, handle: Optional[capi.Handle] = None, t
     return out
 
 
+def apply_A_noalloc(dp: DeviceProblem, soln, out=None, transpose=False, stream=None):
+    """AX = A soln through mps_apply_A_noalloc: no handle and no device allocation
+    inside the call (its scratch is the library's static device array).  The
+    caller provides ``out`` (interior (lz,ly,lx) float64 on the device) when it
+    must not allocate either; the work is queued on ``stream`` (default: torch's
+    current stream) and is not waited for."""
+    import torch
+
+    p = dp.prob
+    if out is None:
+        out = torch.empty(p.shape, dtype=torch.float64, device=soln.device)
+    o = make_opts(flux=p.flux, transpose=transpose)
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    st = capi.load().mps_apply_A_noalloc(C.byref(_grid(p)), int(p.timederiv), float(p.dt), dp.ptr(dp.vel),
+                                         dp.ptr(dp.dcoeff), dp.ptr(dp.reac), _bc(p), dp.ptr(soln), dp.ptr(out),
+                                         C.byref(o), C.c_void_p(s))
+    if st != 0:
+        raise capi.SolverError(st, "mps_apply_A_noalloc: " + capi.STATUS_NAMES.get(st, str(st)))
+    return out
+
+
 def find_bvec_dev(dp: DeviceProblem, handle: Optional[capi.Handle] = None, mgridsterm=None):
     import torch
 
