@@ -249,6 +249,120 @@ def vcycle_bytes(levels_cells, s, coeff_field, nu=4):
     return tot
 
 
+def timed_solves(dp, xg, h, steps, ws, init=None, **kw):
+    """ms per solve (CUDA events on the solving stream, max over ranks) and the last info."""
+    import torch
+
+    from mps3d_b200 import solver
+
+    def one():
+        if init is None:
+            xg.zero_()
+        else:
+            xg.copy_(init)
+        _, info = solver.linsolve_dev(dp, xg, handle=h, **kw)
+        if info["status"] != 0:
+            raise RuntimeError(f"solve failed: {info} {h.last_error()}")
+        return info
+
+    for _ in range(3):
+        one()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        info = one()
+    e1.record()
+    torch.cuda.synchronize()
+    return dist_max(e0.elapsed_time(e1), ws) / steps, info
+
+
+def bench_sg_step(args, ws, h, phi_fine, dev):
+    """Implicit SG electron step, 129^3: the potential is the 257^3 plasma
+    Poisson solution injected onto 129^3; FGMRES(30) preconditioned by an FP32
+    (mixed) or FP64 V-cycle, to 1e-10 relative residual."""
+    import torch
+
+    from mps3d_b200 import solver, workloads as W
+
+    p3 = W.electron_sg_step(129, phi=W.inject_potential(phi_fine.cpu().numpy(), 129))
+    dp3 = solver.DeviceProblem(p3, device=f"cuda:{dev}")
+    x3 = torch.zeros(p3.ghost_shape, dtype=torch.float64, device=f"cuda:{dev}")
+    out = {"workload": "implicit electron drift-diffusion step 129^3, Scharfetter-Gummel faces, dt 1e-11 s, "
+                       "periodic x/y, ZGRD z; potential = 257^3 plasma Poisson solution injected",
+           "unit": "solves/s", "tol_rel_residual": 1e-10}
+    for prec in ("mixed", "fp64"):
+        ms, info = timed_solves(dp3, x3, h, args.steps, ws, precision=prec, krylov="fgmres", restart=30,
+                                tol=1e-10, maxit=60)
+        out[prec] = {"value": ws * 1e3 / ms, "ms_per_solve": ms, "iters": info["iters"],
+                     "rel_res": info["rel_res"]}
+    return out
+
+
+def bench_batch(args, ws, h, dev):
+    """64 independent constant-coefficient Poisson solves, cubic sizes drawn
+    from {33,49,65,97,129}, Dirichlet 0, U[-1,1] right-hand sides, to 1e-10
+    relative residual: one batched mixed-precision call (every V-cycle step
+    of all problems in one launch, the iteration loop in one CUDA graph)
+    against 64 sequential FP64 solves (one handle per size, so no
+    reallocation between them)."""
+    import torch
+
+    from mps3d_b200 import capi, solver, workloads as W
+
+    ps = W.batch_poisson(64)
+    dps = [solver.DeviceProblem(p, device=f"cuda:{dev}") for p in ps]
+    xs = [torch.zeros(p.ghost_shape, dtype=torch.float64, device=f"cuda:{dev}") for p in ps]
+    cells = sum(p.lx * p.ly * p.lz for p in ps)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def batched(prec):
+        for x in xs:
+            x.zero_()
+        return solver.linsolve_batched_dev(dps, xs, handle=h, tol=1e-10, precision=prec, maxit=60)
+
+    handles = {}
+
+    def sequential(prec):
+        infos = []
+        for dp, x in zip(dps, xs):
+            n = dp.prob.lx
+            if n not in handles:
+                handles[n] = capi.Handle(dev)
+            x.zero_()
+            _, info = solver.linsolve_dev(dp, x, handle=handles[n], tol=1e-10, precision=prec, maxit=60)
+            infos.append(info)
+        return infos
+
+    out = {"workload": "64 Poisson problems, unit cube, cubic sizes from {33,49,65,97,129} (seeded), Dirichlet 0, "
+                       "U[-1,1] right-hand sides, 1e-10 relative residual",
+           "cells": cells, "unit": "solves/s"}
+    for name, fn, prec in (("batched_mixed", batched, "mixed"), ("batched_fp64", batched, "fp64"),
+                           ("sequential_fp64", sequential, "fp64"), ("sequential_mixed", sequential, "mixed")):
+        for _ in range(3):
+            infos = fn(prec)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        for _ in range(args.steps):
+            infos = fn(prec)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = dist_max(e0.elapsed_time(e1), ws) / args.steps
+        bad = [i for i in infos if i["status"] != 0]
+        if bad:
+            raise RuntimeError(f"{name}: {len(bad)} problems failed: {bad[0]}")
+        out[name] = {"value": ws * 64 * 1e3 / ms, "ms_per_batch": ms,
+                     "max_rel_res": max(i["rel_res"] for i in infos),
+                     "iters": sorted({i["iters"] for i in infos})}
+    out["batched_mixed_over_sequential_fp64"] = out["batched_mixed"]["value"] / out["sequential_fp64"]["value"]
+    for hh in handles.values():
+        hh.close()
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -382,6 +496,12 @@ def run_ours(args, ws, rank, local):
                          f"twin of the {n}^3 problem ({cores} OpenMP threads), {t_cycle:.3f} s/cycle x {need} "
                          f"cycles to 1e-10 at the measured rate"}
 
+    # ---- secondary configurations (figures beside the headline line) ----
+    others = {}
+    if not args.skip_others and n == 257:
+        others["sg_step_129"] = bench_sg_step(args, ws, h, x, dev)
+        others["batch64"] = bench_batch(args, ws, h, dev)
+
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "colour_pass_traffic.json")
     if os.path.exists(tpath):
@@ -410,6 +530,7 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "final_rel_residual": inf_mixed[-1]["rel_res"],
+        "other_configs": others,
     }
     if e2e is not None:
         out["e2e_vs_device_max_rel_diff"] = dx
@@ -429,6 +550,7 @@ def main():
     ap.add_argument("--cpu-cycles", type=int, default=3)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-others", action="store_true", help="only the headline configuration")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     try:

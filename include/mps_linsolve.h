@@ -186,6 +186,38 @@ int mps_get_profile(mps_handle h, mps_profile* p, int reset);
 int mps_fill_ghosts_dev(mps_handle h, const mps_grid* g, const int bc_code[6],
                         const double* const bcval[6], double* soln, void* stream);
 
+/* One independent problem of a batched call (device pointers, as for
+ * mps_linsolve_dev). */
+typedef struct mps_problem {
+    mps_grid g;
+    int timederiv;
+    double dt;
+    const double* vel;      /* NULL or all zero: batched solves take the diffusion class */
+    const double* dcoeff;
+    const double* reac;
+    const double* source;
+    int bc_code[6];
+    const double* bcval[6];
+    const double* mgridsterm;
+    double* soln;           /* in: initial guess, out: solution (ghosted) */
+} mps_problem;
+
+#define MPS_BATCH_MAX 4096
+
+/* Solve nprob independent problems of any sizes together: one set-up per
+ * problem, then every V-cycle step of all problems as one launch, the outer
+ * iterations inside one CUDA graph whose loop ends on the device when every
+ * problem has converged (or reached maxit).  Replaces a loop of
+ * mps_linsolve_dev calls, i.e. a loop over the reference's per-equation solve
+ * loops (poissoneq.f90:427-450 and its siblings) for independent systems.
+ * opts apply to every problem: stationary iteration (krylov NONE),
+ * precision MIXED (FP32 V-cycles, FP64 residual and update) or FP64,
+ * nu1 >= 1 and nu1+nu2 even.  infos[p] (may be NULL) gets each problem's
+ * result; the return value is MPS_OK unless a problem failed to set up
+ * (its status) or produced NaN (MPS_ERR_NAN). */
+int mps_linsolve_batched_dev(mps_handle h, int nprob, const mps_problem* probs,
+                             const mps_solver_opts* opts, mps_solve_info* infos, void* stream);
+
 /* AX = A soln like mps_apply_A_dev, for callers that must not allocate device
  * memory.  No counterpart in the reference: its find_AX works on arrays the
  * caller already owns, so it never needed one.  Callers that cannot allocate

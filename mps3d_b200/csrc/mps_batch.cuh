@@ -1,0 +1,899 @@
+// Batched solves: many independent problems advanced together.
+//
+// Each problem keeps its own level hierarchy, built by the single-problem
+// set-up (solve_impl with prepare_only).  The iteration then runs as a fixed
+// list of batched steps -- one kernel launch per colour pass, transfer,
+// coarsest solve, outer residual, correction and convergence check -- that
+// cover every problem taking part in the step.  A launch is a persistent,
+// grid-stride loop over tasks: a task is one block-sized tile of one problem,
+// found by a binary search over the step's task prefix; the block copies that
+// problem's descriptor (its level, operator and buffers) into shared memory
+// and runs the same device function as the single-problem kernel.  Problems
+// whose hierarchies are shallower simply take no part in the deeper steps;
+// converged problems are skipped at run time through a per-problem flag.
+//
+// The outer iteration (defect correction: FP64 residual, V-cycles in T, FP64
+// update) is one CUDA graph whose body is a WHILE conditional node: the check
+// kernel at the end of the body clears the condition once no problem is
+// active.  Every problem leaves the active set after at most maxit
+// iterations, and the check kernel also counts the body's executions and
+// stops at maxit + 2, so the loop always ends.
+//
+// The launch shape (blocks of the grid-stride loop, per level depth) is
+// picked by timing candidate grids on the batch's own finest-to-coarsest
+// colour passes at the first call with a given batch structure.
+
+namespace mps {
+
+// per-problem iteration state (device)
+struct BState {
+    int active, iters, status, pad;
+    double rel, rms, rel0;
+};
+
+enum BKind { B_COLOUR = 0, B_RESTRICT, B_COARSE, B_PROLONG, B_OUTER, B_AXPY };
+
+template <class T>
+struct DColour {
+    Lev L;
+    KOp<T> op;
+    const T* u0;  // state: red half
+    const T* u1;  // state: black half (already offset by half)
+    T* out;       // this colour's half of the other buffer
+    const T* f;   // this colour's half of the right-hand side
+};
+template <class T>
+struct DRestrict {
+    Lev F, C;
+    KOp<T> op;
+    const T* u0;
+    const T* u1;
+    const T* f;  // fine right-hand side (split base)
+    T* fc;       // coarse right-hand side (split base)
+    int geom;
+};
+template <class T>
+struct DCoarse {
+    Lev C;
+    const double* AinvT;
+    const T* f;
+    T* u0;
+    T* u1;
+};
+template <class T>
+struct DProlong {
+    Lev F, C;
+    Xfer X;
+    T* u0;
+    T* u1;
+    const T* e0;
+    const T* e1;
+};
+template <class T>
+struct DOuter {
+    Lev L;
+    KOp<double> op;
+    const double* x;  // split base
+    const double* b;  // split base
+    T* r;             // split base (finest right-hand side of the T hierarchy)
+};
+template <class T>
+struct DAxpy {
+    long long half;
+    const T* e0;
+    const T* e1;
+    double* x;
+};
+
+
+__device__ __forceinline__ int find_seg(const int* __restrict__ task0, int nseg, int task)
+{
+    int lo = 0, hi = nseg;  // task0[lo] <= task < task0[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&task0[mid]) <= task) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <class D>
+__device__ __forceinline__ void load_desc(const D* __restrict__ desc, int seg, unsigned char* sbuf)
+{
+    const unsigned* src = reinterpret_cast<const unsigned*>(desc + seg);
+    unsigned* dst = reinterpret_cast<unsigned*>(sbuf);
+    for (int w = threadIdx.x; w < (int)(sizeof(D) / 4); w += blockDim.x) dst[w] = __ldg(&src[w]);
+}
+
+// grid-stride loop over the tasks of one batched step; body(desc, t, problem)
+#define BATCH_LOOP(D, desc, task0, pid, nseg, total, active, ...)                                               \
+    __shared__ __align__(16) unsigned char sbuf_[sizeof(D)];                                                   \
+    for (int task = blockIdx.x; task < (total); task += gridDim.x) {                                           \
+        const int seg = find_seg(task0, nseg, task);                                                           \
+        const int prob = __ldg(&(pid)[seg]);                                                                   \
+        if (!((volatile const int*)&(active)[prob].active)[0]) continue;                                       \
+        __syncthreads();                                                                                       \
+        load_desc<D>(desc, seg, sbuf_);                                                                        \
+        __syncthreads();                                                                                       \
+        const D& d = *reinterpret_cast<const D*>(sbuf_);                                                       \
+        const unsigned t = (unsigned)(task - __ldg(&(task0)[seg])) * TPB + threadIdx.x;                        \
+        (void)t;                                                                                               \
+        __VA_ARGS__                                                                                            \
+    }
+
+template <class T>
+__global__ void __launch_bounds__(TPB) kb_colour(const DColour<T>* __restrict__ desc, const int* __restrict__ task0,
+                                                 const int* __restrict__ pid, int nseg, int total,
+                                                 const BState* active, int c, int zs)
+{
+    BATCH_LOOP(DColour<T>, desc, task0, pid, nseg, total, active, {
+        if (zs == 2) {
+            colour_body<T, KOp<T>, ZeroU<T>>(d.L, d.op, c, ZeroU<T>(), d.out, d.f, t);
+        } else if (zs == 1) {
+            OtherOnlyU<T> u;
+            u.c = c;
+            u.other = c == 0 ? d.u1 : d.u0;
+            colour_body<T, KOp<T>, OtherOnlyU<T>>(d.L, d.op, c, u, d.out, d.f, t);
+        } else {
+            CSplit<T> u;
+            u.c[0] = d.u0;
+            u.c[1] = d.u1;
+            colour_body<T, KOp<T>, CSplit<T>>(d.L, d.op, c, u, d.out, d.f, t);
+        }
+    })
+}
+
+template <class T>
+__global__ void __launch_bounds__(TPB) kb_restrict(const DRestrict<T>* __restrict__ desc,
+                                                   const int* __restrict__ task0, const int* __restrict__ pid,
+                                                   int nseg, int total, const BState* active)
+{
+    BATCH_LOOP(DRestrict<T>, desc, task0, pid, nseg, total, active, {
+        CSplit<T> u, f;
+        u.c[0] = d.u0;
+        u.c[1] = d.u1;
+        f.c[0] = d.f;
+        f.c[1] = d.f + d.F.half;
+        Split<T> fc;
+        fc.c[0] = d.fc;
+        fc.c[1] = d.fc + d.C.half;
+        resid_restrict_body<T, KOp<T>>(d.F, d.op, u, f, d.C, fc, d.geom, t);
+    })
+}
+
+template <class T>
+__global__ void __launch_bounds__(TPB) kb_coarse(const DCoarse<T>* __restrict__ desc, const int* __restrict__ task0,
+                                                 const int* __restrict__ pid, int nseg, int total,
+                                                 const BState* active)
+{
+    __shared__ double fs[1024];
+    BATCH_LOOP(DCoarse<T>, desc, task0, pid, nseg, total, active, {
+        CSplit<T> f;
+        f.c[0] = d.f;
+        f.c[1] = d.f + d.C.half;
+        Split<T> u;
+        u.c[0] = d.u0;
+        u.c[1] = d.u1;
+        coarse_solve_body<T>(d.C, d.AinvT, f, u, fs);
+        __syncthreads();
+    })
+}
+
+template <class T>
+__global__ void __launch_bounds__(TPB) kb_prolong(const DProlong<T>* __restrict__ desc, const int* __restrict__ task0,
+                                                  const int* __restrict__ pid, int nseg, int total,
+                                                  const BState* active)
+{
+    BATCH_LOOP(DProlong<T>, desc, task0, pid, nseg, total, active, {
+        Split<T> u;
+        u.c[0] = d.u0;
+        u.c[1] = d.u1;
+        CSplit<T> e;
+        e.c[0] = d.e0;
+        e.c[1] = d.e1;
+        prolong_body<T>(d.F, u, d.C, e, d.X, -1, t);
+    })
+}
+
+// r = b - A x in FP64 over both colours, r stored as T; per-task partial sums
+// of r.r and b.b (deterministic: the check kernel adds them in task order)
+template <class T>
+__global__ void __launch_bounds__(TPB) kb_outer(const DOuter<T>* __restrict__ desc, const int* __restrict__ task0,
+                                                const int* __restrict__ pid, int nseg, int total,
+                                                const BState* active, double* __restrict__ partial)
+{
+    __shared__ double sh[32];
+    BATCH_LOOP(DOuter<T>, desc, task0, pid, nseg, total, active, {
+        double rr = 0.0, bb = 0.0;
+        const unsigned n = (unsigned)d.L.P * d.L.rows;
+        CSplit<double> x;
+        x.c[0] = d.x;
+        x.c[1] = d.x + d.L.half;
+        for (int c = 0; c < 2; c++) {
+            int i, j, k;
+            if (t < n && decode(d.L, t, c, i, j, k)) {
+                double diag, off;
+                row_any<double>(d.op, d.L, x, i, j, k, diag, off);
+                const double bv = __ldg(&d.b[c * d.L.half + t]);
+                const double r = bv - (diag * __ldg(&x.c[c][t]) + off);
+                rr += r * r;
+                bb += bv * bv;
+                d.r[c * d.L.half + t] = (T)r;
+            }
+        }
+        const double a = block_sum(rr, sh);
+        const double b = block_sum(bb, sh);
+        if (threadIdx.x == 0) {
+            partial[2 * task] = a;
+            partial[2 * task + 1] = b;
+        }
+    })
+}
+
+template <class T>
+__global__ void __launch_bounds__(TPB) kb_axpy(const DAxpy<T>* __restrict__ desc, const int* __restrict__ task0,
+                                               const int* __restrict__ pid, int nseg, int total,
+                                               const BState* active)
+{
+    BATCH_LOOP(DAxpy<T>, desc, task0, pid, nseg, total, active, {
+        if ((long long)t < 2 * d.half) {
+            const T e = (long long)t < d.half ? d.e0[t] : d.e1[(long long)t - d.half];
+            d.x[t] = d.x[t] + (double)e;
+        }
+    })
+}
+
+// one block per problem: sum the outer step's partials, update the state;
+// the last block to finish sets the loop condition (when inside the graph)
+__global__ void __launch_bounds__(TPB) kb_check(const int* __restrict__ task0, const int* __restrict__ pid,
+                                                const double* __restrict__ partial, BState* st,
+                                                const long long* __restrict__ ncell, int nprob, double tol,
+                                                int tol_kind, int maxit, int count_iter, unsigned* counter,
+                                                int* loops, int loop_cap, cudaGraphConditionalHandle hc,
+                                                int use_handle)
+{
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const int s = blockIdx.x;
+    const int p = pid[s];
+    const bool act = ((volatile int*)&st[p].active)[0] != 0;
+    double a = 0.0, b = 0.0;
+    if (act)
+        for (int q = task0[s] + threadIdx.x; q < task0[s + 1]; q += blockDim.x) {
+            a += partial[2 * q];
+            b += partial[2 * q + 1];
+        }
+    a = block_sum(a, sh);
+    b = block_sum(b, sh);
+    if (threadIdx.x == 0) {
+        if (act) {
+            BState& S = st[p];
+            if (count_iter) S.iters += 1;
+            const double rel = b > 0.0 ? sqrt(a) / sqrt(b) : sqrt(a);
+            const double rms = sqrt(a / (double)ncell[p]);
+            if (!count_iter) S.rel0 = rel;
+            S.rel = rel;
+            S.rms = rms;
+            const bool conv = tol_kind == MPS_TOL_RMS_ABS ? rms <= tol : rel <= tol;
+            if (!(a <= 1.0e308)) { S.status = MPS_ERR_NAN; S.active = 0; }
+            else if (conv) { S.status = MPS_OK; S.active = 0; }
+            else if (S.iters >= maxit) { S.status = MPS_ERR_NOT_CONVERGED; S.active = 0; }
+        }
+        __threadfence();
+        const unsigned prev = atomicAdd(counter, 1u);
+        last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    int any = 0;
+    for (int q = threadIdx.x; q < nprob; q += blockDim.x) any |= ((volatile int*)&st[q].active)[0];
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        const int l = *loops + 1;
+        *loops = l;
+        if (l >= loop_cap) any = 0;
+        if (use_handle) cudaGraphSetConditional(hc, any ? 1u : 0u);
+    }
+}
+
+#undef BATCH_LOOP
+
+// ----------------------------------------------------------------------
+// host side
+struct BStep {
+    int kind = 0, c = 0, zs = 0, depth = 0;
+    size_t desc_off = 0;  // bytes into the descriptor buffer
+    size_t task_off = 0;  // ints into the task buffer: task0[nseg+1], then pid[nseg]
+    int nseg = 0, total = 0, grid = 0;
+};
+
+struct BatchState {
+    std::vector<std::unique_ptr<Ctx>> sub;
+    // device buffers (one allocation each, grown on demand)
+    unsigned char* ddesc = nullptr;
+    size_t ddesc_cap = 0;
+    int* dtask = nullptr;
+    size_t dtask_cap = 0;
+    double* dpart = nullptr;
+    size_t dpart_cap = 0;
+    BState* dst = nullptr;
+    long long* dncell = nullptr;
+    unsigned* dcounter = nullptr;
+    int* dloops = nullptr;
+    int cap_prob = 0;
+    // captured loop
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> graph_key;
+    int body_kernels = 0;
+    // autotuned grid per (precision, depth), keyed by the batch structure
+    std::vector<long long> tune_key;
+    std::vector<int> tune_grid;
+};
+
+static int sub_init(Ctx& parent, Ctx& sc)
+{
+    sc.dev = parent.dev;
+    sc.s = parent.s;
+    if (cudaEventCreate(&sc.e0) != cudaSuccess || cudaEventCreate(&sc.e1) != cudaSuccess ||
+        cudaMallocHost((void**)&sc.hpin, sizeof(double) * 512) != cudaSuccess ||
+        cudaMalloc((void**)&sc.dmax, sizeof(unsigned long long) * 8) != cudaSuccess)
+        return MPS_ERR_CUDA;
+    return MPS_OK;
+}
+
+static void sub_free(Ctx& sc)
+{
+    destroy_graphs(sc);
+    sc.ar.clear();
+    sc.kar.clear();
+    sc.inbuf.clear();
+    for (cudaEvent_t e : sc.prof.ev) cudaEventDestroy(e);
+    if (sc.dtab) cudaFree(sc.dtab);
+    if (sc.dmax) cudaFree(sc.dmax);
+    if (sc.hpin) cudaFreeHost(sc.hpin);
+    if (sc.e0) cudaEventDestroy(sc.e0);
+    if (sc.e1) cudaEventDestroy(sc.e1);
+    sc.dtab = nullptr;
+    sc.dmax = nullptr;
+    sc.hpin = nullptr;
+    sc.e0 = sc.e1 = nullptr;
+}
+
+static void batch_release_graph(BatchState& B)
+{
+    if (B.exec) cudaGraphExecDestroy(B.exec);
+    if (B.graph) cudaGraphDestroy(B.graph);
+    B.exec = nullptr;
+    B.graph = nullptr;
+    B.graph_key.clear();
+}
+
+static void destroy_batch(Ctx& ctx)
+{
+    if (!ctx.batch) return;
+    BatchState& B = *ctx.batch;
+    batch_release_graph(B);
+    for (auto& sc : B.sub) sub_free(*sc);
+    B.sub.clear();
+    cudaFree(B.ddesc);
+    cudaFree(B.dtask);
+    cudaFree(B.dpart);
+    cudaFree(B.dst);
+    cudaFree(B.dncell);
+    cudaFree(B.dcounter);
+    cudaFree(B.dloops);
+    delete ctx.batch;
+    ctx.batch = nullptr;
+}
+
+// the step list and descriptors of one batch, built by replaying each
+// problem's V-cycle bookkeeping (buffer parities) on the host
+template <class T>
+struct BatchPlan {
+    std::vector<BStep> pre, body;
+    std::vector<unsigned char> desc;
+    std::vector<int> task;
+    int maxdepth = 0;
+
+    template <class D>
+    size_t add_desc(const D& d)
+    {
+        const size_t off = (desc.size() + 15) / 16 * 16;
+        desc.resize(off + sizeof(D));
+        std::memcpy(desc.data() + off, &d, sizeof(D));
+        return off;
+    }
+};
+
+template <class T>
+static Hier<T>& batch_hier(Ctx& sc);
+template <>
+Hier<float>& batch_hier<float>(Ctx& sc) { return sc.h32; }
+template <>
+Hier<double>& batch_hier<double>(Ctx& sc) { return sc.h64; }
+
+template <class T>
+static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o, int inner)
+{
+    const int np = (int)B.sub.size();
+    int D = 0;
+    for (auto& sc : B.sub) D = std::max(D, sc->nlev - 1);
+    P.maxdepth = D;
+    std::vector<std::array<int, MAXL>> ri(np), bi(np);
+    for (int p = 0; p < np; p++) {
+        ri[p].fill(0);
+        bi[p].fill(0);
+    }
+    // one step over the participating problems: make(p) fills the descriptor
+    auto step = [&](std::vector<BStep>& list, int kind, int depth, int c, int zs, auto want, auto make,
+                    auto tasks) {
+        using D = decltype(make(0));
+        BStep s;
+        s.kind = kind;
+        s.depth = depth;
+        s.c = c;
+        s.zs = zs;
+        std::vector<int> t0, pid;
+        std::vector<D> ds;
+        int total = 0;
+        for (int p = 0; p < np; p++) {
+            if (!want(p)) continue;
+            t0.push_back(total);
+            pid.push_back(p);
+            ds.push_back(make(p));
+            total += tasks(p);
+        }
+        if (pid.empty()) return;
+        t0.push_back(total);
+        s.nseg = (int)pid.size();
+        s.total = total;
+        s.desc_off = (P.desc.size() + 15) / 16 * 16;
+        P.desc.resize(s.desc_off + sizeof(D) * ds.size());
+        std::memcpy(P.desc.data() + s.desc_off, ds.data(), sizeof(D) * ds.size());
+        s.task_off = P.task.size();
+        P.task.insert(P.task.end(), t0.begin(), t0.end());
+        P.task.insert(P.task.end(), pid.begin(), pid.end());
+        list.push_back(s);
+    };
+    auto nb = [](long long n) { return (int)((n + TPB - 1) / TPB); };
+    auto cur0 = [&](int p, int d) { return batch_hier<T>(*B.sub[p]).U[d][ri[p][d]]; };
+    auto cur1 = [&](int p, int d) {
+        return batch_hier<T>(*B.sub[p]).U[d][bi[p][d]] + B.sub[p]->lev[d].half;
+    };
+    auto colour = [&](std::vector<BStep>& list, int d, int c, int zs) {
+        step(
+            list, B_COLOUR, d, c, zs, [&](int p) { return d < B.sub[p]->nlev - 1; },
+            [&](int p) {
+                Ctx& sc = *B.sub[p];
+                Hier<T>& H = batch_hier<T>(sc);
+                const Lev& L = sc.lev[d];
+                DColour<T> x;
+                x.L = L;
+                x.op = H.kop[d];
+                x.u0 = cur0(p, d);
+                x.u1 = cur1(p, d);
+                x.out = c == 0 ? H.U[d][ri[p][d] ^ 1] : H.U[d][bi[p][d] ^ 1] + L.half;
+                x.f = H.F[d] + (c ? L.half : 0);
+                if (c == 0) ri[p][d] ^= 1;
+                else bi[p][d] ^= 1;
+                return x;
+            },
+            [&](int p) { return nb(B.sub[p]->lev[d].half); });
+    };
+    auto vcycle = [&](std::vector<BStep>& list, bool zero) {
+        for (int d = 0; d < D; d++) {
+            const bool z = d > 0 || zero;
+            for (int s = 0; s < o->nu1; s++) {
+                colour(list, d, 0, z && s == 0 ? 2 : 0);
+                colour(list, d, 1, z && s == 0 ? 1 : 0);
+            }
+            step(
+                list, B_RESTRICT, d, 0, 0, [&](int p) { return d < B.sub[p]->nlev - 1; },
+                [&](int p) {
+                    Ctx& sc = *B.sub[p];
+                    Hier<T>& H = batch_hier<T>(sc);
+                    DRestrict<T> x;
+                    x.F = sc.lev[d];
+                    x.C = sc.lev[d + 1];
+                    x.op = H.kop[d];
+                    x.u0 = cur0(p, d);
+                    x.u1 = cur1(p, d);
+                    x.f = H.F[d];
+                    x.fc = H.F[d + 1];
+                    x.geom = sc.xf[d].geom;
+                    return x;
+                },
+                [&](int p) {
+                    const Lev& C = B.sub[p]->lev[d + 1];
+                    return nb((long long)C.nx * C.ny * C.nz);
+                });
+        }
+        step(
+            list, B_COARSE, D, 0, 0, [&](int) { return true; },
+            [&](int p) {
+                Ctx& sc = *B.sub[p];
+                Hier<T>& H = batch_hier<T>(sc);
+                const int d = sc.nlev - 1;
+                DCoarse<T> x;
+                x.C = sc.lev[d];
+                x.AinvT = H.AinvT;
+                x.f = H.F[d];
+                x.u0 = cur0(p, d);
+                x.u1 = cur1(p, d);
+                return x;
+            },
+            [&](int) { return 1; });
+        for (int d = D - 1; d >= 0; d--) {
+            step(
+                list, B_PROLONG, d, 0, 0, [&](int p) { return d < B.sub[p]->nlev - 1; },
+                [&](int p) {
+                    Ctx& sc = *B.sub[p];
+                    DProlong<T> x;
+                    x.F = sc.lev[d];
+                    x.C = sc.lev[d + 1];
+                    x.X = sc.xf[d];
+                    x.u0 = cur0(p, d);
+                    x.u1 = cur1(p, d);
+                    x.e0 = cur0(p, d + 1);
+                    x.e1 = cur1(p, d + 1);
+                    return x;
+                },
+                [&](int p) {
+                    const Lev& F = B.sub[p]->lev[d];
+                    return nb((long long)F.nx * F.ny * F.nz);
+                });
+            for (int s = 0; s < o->nu2; s++) {
+                colour(list, d, 0, 0);
+                colour(list, d, 1, 0);
+            }
+        }
+    };
+    auto outer = [&](std::vector<BStep>& list) {
+        step(
+            list, B_OUTER, 0, 0, 0, [&](int) { return true; },
+            [&](int p) {
+                Ctx& sc = *B.sub[p];
+                DOuter<T> x;
+                x.L = sc.lev[0];
+                x.op = sc.kop64;
+                x.x = sc.x64;
+                x.b = sc.b64;
+                x.r = batch_hier<T>(sc).F[0];
+                return x;
+            },
+            [&](int p) { return nb(B.sub[p]->lev[0].half); });
+    };
+    outer(P.pre);
+    for (int c = 0; c < inner; c++) vcycle(P.body, c == 0);
+    step(
+        P.body, B_AXPY, 0, 0, 0, [&](int) { return true; },
+        [&](int p) {
+            Ctx& sc = *B.sub[p];
+            DAxpy<T> x;
+            x.half = sc.lev[0].half;
+            x.e0 = cur0(p, 0);
+            x.e1 = cur1(p, 0);
+            x.x = sc.x64;
+            return x;
+        },
+        [&](int p) { return nb(2 * B.sub[p]->lev[0].half); });
+    outer(P.body);
+}
+
+template <class T>
+static void launch_step(cudaStream_t s, const BStep& st, const unsigned char* ddesc, const int* dtask,
+                        const BState* active, double* dpart)
+{
+    const int* t0 = dtask + st.task_off;
+    const int* pid = t0 + st.nseg + 1;
+    const unsigned g = (unsigned)std::max(1, std::min(st.grid, st.total));
+    const void* dp = ddesc + st.desc_off;
+    switch (st.kind) {
+    case B_COLOUR:
+        kb_colour<T><<<g, TPB, 0, s>>>((const DColour<T>*)dp, t0, pid, st.nseg, st.total, active, st.c, st.zs);
+        break;
+    case B_RESTRICT:
+        kb_restrict<T><<<g, TPB, 0, s>>>((const DRestrict<T>*)dp, t0, pid, st.nseg, st.total, active);
+        break;
+    case B_COARSE:
+        kb_coarse<T><<<g, TPB, 0, s>>>((const DCoarse<T>*)dp, t0, pid, st.nseg, st.total, active);
+        break;
+    case B_PROLONG:
+        kb_prolong<T><<<g, TPB, 0, s>>>((const DProlong<T>*)dp, t0, pid, st.nseg, st.total, active);
+        break;
+    case B_OUTER:
+        kb_outer<T><<<g, TPB, 0, s>>>((const DOuter<T>*)dp, t0, pid, st.nseg, st.total, active, dpart);
+        break;
+    case B_AXPY:
+        kb_axpy<T><<<g, TPB, 0, s>>>((const DAxpy<T>*)dp, t0, pid, st.nseg, st.total, active);
+        break;
+    }
+}
+
+// the batch structure a graph (and a tuning result) is valid for
+template <class T>
+static std::vector<long long> batch_key(BatchState& B, const BatchPlan<T>& P, const mps_solver_opts* o, int inner)
+{
+    std::vector<long long> k;
+    k.push_back(sizeof(T));
+    k.push_back(o->nu1);
+    k.push_back(o->nu2);
+    k.push_back(inner);
+    k.push_back((long long)B.sub.size());
+    for (auto& sc : B.sub) {
+        k.push_back(sc->nlev);
+        for (int l = 0; l < sc->nlev; l++) {
+            k.push_back(sc->lev[l].nx);
+            k.push_back(sc->lev[l].ny);
+            k.push_back(sc->lev[l].nz);
+        }
+    }
+    k.push_back((long long)P.desc.size());
+    k.push_back((long long)P.task.size());
+    return k;
+}
+
+static const int kTuneGrids[] = {148, 296, 592, 1184, 2368, 4736};
+
+// time the candidate grids on the colour pass of every depth (the passes
+// read and write only the V-cycle state, which the first pass of a solve
+// overwrites without reading)
+template <class T>
+static int autotune(Ctx& ctx, BatchState& B, BatchPlan<T>& P, const unsigned char* ddesc, const int* dtask)
+{
+    const int D = P.maxdepth;
+    B.tune_grid.assign(D + 1, 1184);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (int d = 0; d < D; d++) {
+        const BStep* st = nullptr;
+        for (const BStep& s : P.body)
+            if (s.kind == B_COLOUR && s.depth == d && s.zs == 0) { st = &s; break; }
+        if (!st) continue;
+        float best = 1e30f;
+        for (int g : kTuneGrids) {
+            if (g > std::max(st->total, 148)) break;
+            BStep s2 = *st;
+            s2.grid = g;
+            launch_step<T>(ctx.s, s2, ddesc, dtask, B.dst, B.dpart);  // warm
+            CK(cudaEventRecord(a, ctx.s));
+            for (int r = 0; r < 3; r++) launch_step<T>(ctx.s, s2, ddesc, dtask, B.dst, B.dpart);
+            CK(cudaEventRecord(b, ctx.s));
+            CK(cudaEventSynchronize(b));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, a, b));
+            if (ms < best * 0.97f) { best = ms; B.tune_grid[d] = g; }
+        }
+    }
+    B.tune_grid[D] = B.tune_grid[0];
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+template <class T>
+static void assign_grids(BatchState& B, BatchPlan<T>& P)
+{
+    auto grid_of = [&](const BStep& s) {
+        if (s.kind == B_COARSE) return std::min(s.total, 4736);
+        if (s.kind == B_OUTER || s.kind == B_AXPY) return B.tune_grid[0];
+        return B.tune_grid[std::min(s.depth, (int)B.tune_grid.size() - 1)];
+    };
+    for (BStep& s : P.pre) s.grid = grid_of(s);
+    for (BStep& s : P.body) s.grid = grid_of(s);
+}
+
+template <class T>
+static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_solver_opts* o, mps_solve_info* infos)
+{
+    if (!ctx.batch) ctx.batch = new BatchState();
+    BatchState& B = *ctx.batch;
+    const int inner = o->inner_cycles > 0 ? o->inner_cycles : 2;
+    // ---- per-problem contexts and set-up ----
+    if ((int)B.sub.size() != np) {
+        batch_release_graph(B);
+        for (auto& sc : B.sub) sub_free(*sc);
+        B.sub.clear();
+        for (int p = 0; p < np; p++) {
+            B.sub.emplace_back(new Ctx());
+            if (sub_init(ctx, *B.sub.back())) { ctx.err.msg = "batched: sub-context set-up failed"; return MPS_ERR_CUDA; }
+        }
+    }
+    CK(cudaEventRecord(ctx.e0, ctx.s));
+    const long long launches0 = ctx.launches;
+    for (int p = 0; p < np; p++) {
+        Ctx& sc = *B.sub[p];
+        const mps_problem& q = probs[p];
+        Inputs in;
+        in.vel = q.vel;
+        in.dcoeff = q.dcoeff;
+        in.reac = q.reac;
+        in.source = q.source;
+        for (int f = 0; f < 6; f++) in.bcval[f] = q.bcval[f];
+        in.sterm = q.mgridsterm;
+        in.soln = q.soln;
+        mps_solve_info inf;
+        sc.launches = 0;
+        int st = solve_impl(sc, &q.g, q.timederiv, q.dt, in, q.bc_code, o, &inf, 0, 1);
+        ctx.launches += sc.launches;
+        if (st) {
+            ctx.err.msg = "batched problem " + std::to_string(p) + ": " + sc.err.msg;
+            if (infos) { std::memset(&infos[p], 0, sizeof(mps_solve_info)); infos[p].status = st; }
+            return st;
+        }
+        if (sc.sig.opclass != 0) {
+            ctx.err.msg = "batched problem " + std::to_string(p) +
+                          ": batched solves take the diffusion class (no convection, upwind flux, no transpose)";
+            return MPS_ERR_BAD_ARG;
+        }
+    }
+    // ---- plan, device tables ----
+    BatchPlan<T> P;
+    plan_batch<T>(B, P, o, inner);
+    auto grow = [&](auto*& ptr, size_t& cap, size_t n, size_t elem) -> int {
+        if (n <= cap) return 0;
+        batch_release_graph(B);
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+        if (cudaMalloc((void**)&ptr, std::max<size_t>(n, 1) * elem) != cudaSuccess) return MPS_ERR_CUDA;
+        cap = n;
+        return 0;
+    };
+    int maxtasks = 0;
+    for (const BStep& s : P.body)
+        if (s.kind == B_OUTER) maxtasks = std::max(maxtasks, s.total);
+    if (grow(B.ddesc, B.ddesc_cap, P.desc.size(), 1) || grow(B.dtask, B.dtask_cap, P.task.size(), sizeof(int)) ||
+        grow(B.dpart, B.dpart_cap, 2 * (size_t)maxtasks, sizeof(double))) {
+        ctx.err.msg = "batched: device tables";
+        return MPS_ERR_NOMEM;
+    }
+    if (np > B.cap_prob) {
+        batch_release_graph(B);
+        cudaFree(B.dst);
+        cudaFree(B.dncell);
+        cudaFree(B.dcounter);
+        cudaFree(B.dloops);
+        B.dst = nullptr; B.dncell = nullptr; B.dcounter = nullptr; B.dloops = nullptr;
+        B.cap_prob = 0;
+        if (cudaMalloc((void**)&B.dst, sizeof(BState) * np) != cudaSuccess ||
+            cudaMalloc((void**)&B.dncell, sizeof(long long) * np) != cudaSuccess ||
+            cudaMalloc((void**)&B.dcounter, sizeof(unsigned)) != cudaSuccess ||
+            cudaMalloc((void**)&B.dloops, sizeof(int)) != cudaSuccess) {
+            ctx.err.msg = "batched: state";
+            return MPS_ERR_NOMEM;
+        }
+        CK(cudaMemsetAsync(B.dcounter, 0, sizeof(unsigned), ctx.s));
+        B.cap_prob = np;
+    }
+    std::vector<BState> hs(np);
+    std::vector<long long> hn(np);
+    for (int p = 0; p < np; p++) {
+        hs[p] = BState{1, 0, MPS_OK, 0, 0.0, 0.0, 0.0};
+        hn[p] = (long long)probs[p].g.lx * probs[p].g.ly * probs[p].g.lz;
+    }
+    CK(cudaMemcpyAsync(B.ddesc, P.desc.data(), P.desc.size(), cudaMemcpyHostToDevice, ctx.s));
+    CK(cudaMemcpyAsync(B.dtask, P.task.data(), sizeof(int) * P.task.size(), cudaMemcpyHostToDevice, ctx.s));
+    CK(cudaMemcpyAsync(B.dst, hs.data(), sizeof(BState) * np, cudaMemcpyHostToDevice, ctx.s));
+    CK(cudaMemcpyAsync(B.dncell, hn.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx.s));
+    CK(cudaMemsetAsync(B.dloops, 0, sizeof(int), ctx.s));
+    const BState* active = B.dst;
+    // ---- launch shapes ----
+    std::vector<long long> key = batch_key<T>(B, P, o, inner);
+    if (key != B.tune_key) {
+        int st = autotune<T>(ctx, B, P, B.ddesc, B.dtask);
+        if (st) return st;
+        B.tune_key = key;
+    }
+    assign_grids<T>(B, P);
+    // ---- initial residual and check ----
+    for (const BStep& s : P.pre) {
+        launch_step<T>(ctx.s, s, B.ddesc, B.dtask, active, B.dpart);
+        CKL();
+        const int* t0 = B.dtask + s.task_off;
+        kb_check<<<s.nseg, TPB, 0, ctx.s>>>(t0, t0 + s.nseg + 1, B.dpart, B.dst, B.dncell, np, o->tol, o->tol_kind,
+                                            o->maxit, 0, B.dcounter, B.dloops, o->maxit + 2, 0, 0);
+        CKL();
+    }
+    CK(cudaMemsetAsync(B.dloops, 0, sizeof(int), ctx.s));
+    // ---- the loop: one graph launch ----
+    key.push_back((long long)(uintptr_t)B.ddesc);
+    key.push_back((long long)(uintptr_t)B.dtask);
+    key.push_back((long long)(uintptr_t)B.dpart);
+    key.push_back((long long)(uintptr_t)B.dst);
+    key.push_back(o->maxit);
+    key.push_back(o->tol_kind);
+    long long tb;
+    std::memcpy(&tb, &o->tol, 8);
+    key.push_back(tb);
+    for (const BStep& s : P.body) key.push_back(s.grid);
+    if (key != B.graph_key) {
+        batch_release_graph(B);
+        CK(cudaGraphCreate(&B.graph, 0));
+        cudaGraphConditionalHandle hc;
+        CK(cudaGraphConditionalHandleCreate(&hc, B.graph, 1, cudaGraphCondAssignDefault));
+        // (the struct holds a union without a default constructor: zeroed storage)
+        alignas(cudaGraphNodeParams) unsigned char cpbuf[sizeof(cudaGraphNodeParams)];
+        std::memset(cpbuf, 0, sizeof(cpbuf));
+        cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cpbuf);
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hc;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, B.graph, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(ctx.s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        int nk = 0;
+        const BStep* last_outer = nullptr;
+        for (const BStep& s : P.body) {
+            launch_step<T>(ctx.s, s, B.ddesc, B.dtask, active, B.dpart);
+            nk++;
+            if (s.kind == B_OUTER) last_outer = &s;
+        }
+        const int* t0 = B.dtask + last_outer->task_off;
+        kb_check<<<last_outer->nseg, TPB, 0, ctx.s>>>(t0, t0 + last_outer->nseg + 1, B.dpart, B.dst, B.dncell, np,
+                                                      o->tol, o->tol_kind, o->maxit, 1, B.dcounter, B.dloops,
+                                                      o->maxit + 2, hc, 1);
+        nk++;
+        cudaGraph_t got = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(ctx.s, &got);
+        if (ce != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            batch_release_graph(B);
+            ctx.err.msg = std::string("batched: graph capture: ") + cudaGetErrorString(ce);
+            return MPS_ERR_CUDA;
+        }
+        CK(cudaGraphInstantiate(&B.exec, B.graph, 0));
+        B.graph_key = key;
+        B.body_kernels = nk;
+    }
+    CK(cudaGraphLaunch(B.exec, ctx.s));
+    // ---- results ----
+    int loops = 0;
+    CK(cudaMemcpyAsync(hs.data(), B.dst, sizeof(BState) * np, cudaMemcpyDeviceToHost, ctx.s));
+    CK(cudaMemcpyAsync(&loops, B.dloops, sizeof(int), cudaMemcpyDeviceToHost, ctx.s));
+    for (int p = 0; p < np; p++) {
+        Ctx& sc = *B.sub[p];
+        const Lev& L0 = sc.lev[0];
+        const long long n = (long long)L0.nx * L0.ny * L0.nz;
+        k_unpack<double><<<nblk(n), TPB, 0, ctx.s>>>(L0, csplit<double>(sc.x64, L0), probs[p].soln);
+        CKL();
+        if (o->fill_ghosts) {
+            const int mx = std::max(std::max(L0.ny * L0.nz, L0.nx * L0.nz), L0.nx * L0.ny);
+            const double* zf[6];
+            for (int f = 0; f < 6; f++) zf[f] = probs[p].bcval[f];
+            k_fill_ghosts<<<nblk(mx), TPB, 0, ctx.s>>>(L0, probs[p].soln, zf[0], zf[1], zf[2], zf[3], zf[4], zf[5]);
+            CKL();
+        }
+    }
+    CK(cudaEventRecord(ctx.e1, ctx.s));
+    CK(cudaStreamSynchronize(ctx.s));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx.e0, ctx.e1));
+    ctx.launches += (long long)loops * B.body_kernels;
+    int worst = MPS_OK;
+    for (int p = 0; p < np; p++) {
+        if (infos) {
+            mps_solve_info& inf = infos[p];
+            std::memset(&inf, 0, sizeof(inf));
+            inf.status = hs[p].active ? MPS_ERR_NOT_CONVERGED : hs[p].status;
+            inf.iters = hs[p].iters;
+            inf.vcycles = hs[p].iters * inner;
+            inf.levels = B.sub[p]->nlev;
+            inf.rel_res = hs[p].rel;
+            inf.rms_res = hs[p].rms;
+            inf.rel_res0 = hs[p].rel0;
+            inf.time_ms = ms;
+            inf.launches = (int)(ctx.launches - launches0);
+        }
+        if (hs[p].status == MPS_ERR_NAN) worst = MPS_ERR_NAN;
+    }
+    return worst;
+}
+
+}  // namespace mps

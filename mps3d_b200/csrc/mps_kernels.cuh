@@ -59,15 +59,21 @@ struct OtherOnlyU {  // colour c known zero, the other colour read from memory
 // periodic seams of odd size where equal colours touch)
 // ---------------------------------------------------------------------
 template <class T, class Op, class U>
-__global__ void __launch_bounds__(TPB) k_colour(Lev L, Op op, int c, U u, T* __restrict__ out,
-                                                const T* __restrict__ f)
+__device__ __forceinline__ void colour_body(const Lev& L, const Op& op, int c, const U& u, T* __restrict__ out,
+                                            const T* __restrict__ f, unsigned t)
 {
-    unsigned t = blockIdx.x * TPB + threadIdx.x;
     int i, j, k;
     if (!decode(L, t, c, i, j, k)) return;
     T diag, off;
     row_any<T>(op, L, u, i, j, k, diag, off);
     out[t] = gs_value(__ldg(&f[t]), diag, off);
+}
+
+template <class T, class Op, class U>
+__global__ void __launch_bounds__(TPB) k_colour(Lev L, Op op, int c, U u, T* __restrict__ out,
+                                                const T* __restrict__ f)
+{
+    colour_body<T, Op, U>(L, op, c, u, out, f, blockIdx.x * TPB + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------
@@ -451,10 +457,10 @@ __global__ void __launch_bounds__(TPB) k_restrict_res(Lev F, CSplit<T> r, Lev C,
 // One thread per coarse cell, natural order.
 // ---------------------------------------------------------------------
 template <class T, class Op>
-__global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
-                                                        Split<T> fc, int geom)
+__device__ __forceinline__ void resid_restrict_body(const Lev& F, const Op& op, const CSplit<T>& u,
+                                                    const CSplit<T>& f, const Lev& C, const Split<T>& fc, int geom,
+                                                    unsigned t)
 {
-    unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned ncx = C.nx, ncy = C.ny;
     if (t >= ncx * ncy * (unsigned)C.nz) return;
     unsigned K = t / (ncx * ncy);
@@ -489,6 +495,13 @@ __global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> 
     }
     const int ci = I, cj = J, ck = K;
     fc.half(scol(ci, cj, ck))[soff(C, ci, cj, ck)] = geom ? s / vol : s * (T(1) / vol);
+}
+
+template <class T, class Op>
+__global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
+                                                        Split<T> fc, int geom)
+{
+    resid_restrict_body<T, Op>(F, op, u, f, C, fc, geom, blockIdx.x * TPB + threadIdx.x);
 }
 
 // coarse ghost rule for the correction (update_boundary_ghostvalues applied
@@ -534,11 +547,11 @@ __device__ __forceinline__ T coarse_at(const Lev& C, const CSplit<T>& e, int I, 
 // per fine cell.
 // ---------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, int only_col)
+__device__ __forceinline__ void prolong_body(const Lev& F, const Split<T>& u, const Lev& C, const CSplit<T>& e,
+                                             const Xfer& X, int only_col, unsigned t)
 {
     unsigned i, j, k;
     if (only_col < 0) {  // all cells, natural order
-        unsigned t = blockIdx.x * TPB + threadIdx.x;
         const unsigned nx = F.nx, ny = F.ny;
         if (t >= nx * ny * (unsigned)F.nz) return;
         k = t / (nx * ny);
@@ -547,7 +560,7 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
         i = rem - j * nx;
     } else if (only_col == 2) {  // red cells on the odd periodic seam planes
         int ii, jj, kk;
-        if (!decode(F, blockIdx.x * TPB + threadIdx.x, 0, ii, jj, kk)) return;
+        if (!decode(F, t, 0, ii, jj, kk)) return;
         const bool seam = (F.per[0] && (F.nx & 1) && (ii == 0 || ii == F.nx - 1)) ||
                           (F.per[1] && (F.ny & 1) && (jj == 0 || jj == F.ny - 1)) ||
                           (F.per[2] && (F.nz & 1) && (kk == 0 || kk == F.nz - 1));
@@ -555,7 +568,7 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
         i = ii; j = jj; k = kk;
     } else {  // the cells of one colour, split order (coalesced on that half)
         int ii, jj, kk;
-        if (!decode(F, blockIdx.x * TPB + threadIdx.x, only_col, ii, jj, kk)) return;
+        if (!decode(F, t, only_col, ii, jj, kk)) return;
         i = ii; j = jj; k = kk;
     }
     T v;
@@ -595,16 +608,21 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
     *p = *p + v;
 }
 
+template <class T>
+__global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, int only_col)
+{
+    prolong_body<T>(F, u, C, e, X, only_col, blockIdx.x * TPB + threadIdx.x);
+}
+
 // ---------------------------------------------------------------------
 // exact coarsest solve: u = A^{-1} f with the inverse precomputed (column
 // major, FP64).  Replaces bottomsolve's full-dimension GMRES
 // (mgridsteps.f90:218-382), which is an exact solve as well.  One CTA.
 // ---------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(512) k_coarse_solve(Lev C, const double* __restrict__ AinvT, CSplit<T> f,
-                                                      Split<T> u)
+__device__ __forceinline__ void coarse_solve_body(const Lev& C, const double* __restrict__ AinvT,
+                                                  const CSplit<T>& f, const Split<T>& u, double* fs)
 {
-    extern __shared__ double fs[];
     const int n = C.nx * C.ny * C.nz;
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
         int i = r % C.nx, j = (r / C.nx) % C.ny, k = r / (C.nx * C.ny);
@@ -617,6 +635,14 @@ __global__ void __launch_bounds__(512) k_coarse_solve(Lev C, const double* __res
         int i = r % C.nx, j = (r / C.nx) % C.ny, k = r / (C.nx * C.ny);
         u.half(scol(i, j, k))[soff(C, i, j, k)] = (T)acc;
     }
+}
+
+template <class T>
+__global__ void __launch_bounds__(512) k_coarse_solve(Lev C, const double* __restrict__ AinvT, CSplit<T> f,
+                                                      Split<T> u)
+{
+    extern __shared__ double fs[];
+    coarse_solve_body<T>(C, AinvT, f, u, fs);
 }
 
 // dense assembly of the coarsest operator (row major, FP64, pre-zeroed)

@@ -11,7 +11,10 @@
 // FP32 V-cycles + FP64 update (defect correction); FGMRES(m) right
 // preconditioned by the V-cycle with FP64 Gram-Schmidt and Givens.
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdint>
+#include <memory>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -128,8 +131,11 @@ struct GraphEntry {
     std::vector<int> cls;
 };
 
+struct BatchState;
+
 struct Ctx {
     int dev = 0;
+    BatchState* batch = nullptr;  // batched solves (mps_linsolve_batched_dev)
     long long launches = 0;
     Prof prof;
     std::vector<GraphEntry> graphs;
@@ -827,8 +833,10 @@ static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
 }
 
 // ----------------------------------------------------------------------
+// prepare_only: stop after the set-up (hierarchy, operators, right-hand side,
+// initial guess, coarsest inverse), for the batched driver
 static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, const Inputs& in, const int bc[6],
-                      const mps_solver_opts* o, mps_solve_info* info, int ref_norm_only)
+                      const mps_solver_opts* o, mps_solve_info* info, int ref_norm_only, int prepare_only = 0)
 {
     mps_solve_info inf;
     std::memset(&inf, 0, sizeof(inf));
@@ -1056,6 +1064,11 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         else st = coarse_inverse(ctx, ctx.h32, ctx.h32.rop[nl - 1]);
     }
     if (st) return st;
+    if (prepare_only) {
+        inf.levels = nl;
+        if (info) *info = inf;
+        return 0;
+    }
 
     // ---- iterations ----
     const Lev& L = L0;
@@ -1362,6 +1375,8 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
 
 }  // namespace mps
 
+#include "mps_batch.cuh"
+
 // ======================================================================
 // C ABI
 // ======================================================================
@@ -1421,6 +1436,7 @@ int mps_destroy(mps_handle h)
     Ctx& ctx = h->ctx;
     cudaSetDevice(ctx.dev);
     cudaStreamSynchronize(ctx.s);
+    destroy_batch(ctx);
     destroy_graphs(ctx);
     ctx.ar.clear();
     ctx.kar.clear();
@@ -1469,6 +1485,40 @@ static int run_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, co
         cudaEventDestroy(ev);
     }
     if (st && info) info->status = st;
+    return st;
+}
+
+int mps_linsolve_batched_dev(mps_handle h, int nprob, const mps_problem* probs, const mps_solver_opts* opts,
+                             mps_solve_info* infos, void* stream)
+{
+    if (!h) return MPS_ERR_BAD_ARG;
+    Ctx& ctx = h->ctx;
+    ctx.err = Err();
+    if (nprob < 1 || nprob > MPS_BATCH_MAX || !probs) { ctx.err.msg = "batched: bad problem count"; return MPS_ERR_BAD_ARG; }
+    if (cudaSetDevice(ctx.dev) != cudaSuccess) return MPS_ERR_CUDA;
+    mps_solver_opts o;
+    if (opts) o = *opts;
+    else mps_default_opts(&o);
+    if (o.krylov != MPS_KRYLOV_NONE || o.transpose || o.flux != MPS_FLUX_UPWIND || o.nu1 < 1 ||
+        (o.nu1 + o.nu2) % 2 != 0 || (o.precision != MPS_PREC_MIXED && o.precision != MPS_PREC_FP64)) {
+        ctx.err.msg = "batched: stationary iteration only (krylov NONE, upwind, no transpose), nu1 >= 1, nu1+nu2 even";
+        return MPS_ERR_BAD_ARG;
+    }
+    cudaStream_t user = (cudaStream_t)stream;
+    cudaEvent_t ev = nullptr;
+    if (user && user != ctx.s) {
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return MPS_ERR_CUDA;
+        cudaEventRecord(ev, user);
+        cudaStreamWaitEvent(ctx.s, ev, 0);
+    }
+    int st = o.precision == MPS_PREC_MIXED ? batched_solve<float>(ctx, nprob, probs, &o, infos)
+                                           : batched_solve<double>(ctx, nprob, probs, &o, infos);
+    if (ev) {
+        cudaEventRecord(ev, ctx.s);
+        cudaStreamWaitEvent(user, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    if (st && st != MPS_ERR_NAN) cudaStreamSynchronize(ctx.s);
     return st;
 }
 
@@ -1619,8 +1669,6 @@ int mps_apply_A_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, c
     int bcfix[6];
     for (int f = 0; f < 6; f++) bcfix[f] = bc_code[f];
     mps_solve_info info;
-    double zeros_face_dummy = 0.0;
-    (void)zeros_face_dummy;
     // DIRC/FLUX faces need value arrays for find_bvec; they do not enter A
     std::vector<double*> fb;
     const double* bv[6];

@@ -147,6 +147,46 @@ def linsolve_dev(dp: DeviceProblem, soln, handle: Optional[capi.Handle] = None, 
     return soln, info.as_dict()
 
 
+def linsolve_batched_dev(dps, solns, handle: Optional[capi.Handle] = None, stream=None, **kw):
+    """Solve independent problems together through mps_linsolve_batched_dev.
+
+    dps: list of :class:`DeviceProblem` (diffusion class: no convection);
+    solns: matching ghosted float64 CUDA tensors (initial guesses, updated in
+    place).  Returns the list of per-problem info dicts.  Options as for
+    :func:`linsolve` (stationary iteration; precision "mixed" or "fp64")."""
+    import torch
+
+    h = handle or default_handle()
+    n = len(dps)
+    assert n == len(solns) and n >= 1
+    descs = (capi.ProblemDesc * n)()
+    keep = []
+    for i, (dp, x) in enumerate(zip(dps, solns)):
+        p = dp.prob
+        d = descs[i]
+        d.g = _grid(p)
+        d.timederiv = int(p.timederiv)
+        d.dt = float(p.dt)
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        d.vel = ptr(dp.vel)
+        d.dcoeff = ptr(dp.dcoeff)
+        d.reac = ptr(dp.reac)
+        d.source = ptr(dp.source)
+        d.bc_code[:] = list(p.bc)
+        for f in range(6):
+            d.bcval[f] = dp.bcvals[f].data_ptr()
+        d.mgridsterm = None
+        d.soln = x.data_ptr()
+        keep.append((dp, x))
+    o = make_opts(**kw)
+    infos = (capi.Info * n)()
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    st = h._lib.mps_linsolve_batched_dev(h.h, n, descs, C.byref(o), infos, C.c_void_p(s))
+    if st not in (0, capi.MPS_ERR_NOT_CONVERGED):
+        raise capi.SolverError(st, h.last_error())
+    return [infos[i].as_dict() for i in range(n)]
+
+
 def apply_A_dev(dp: DeviceProblem, soln, handle: Optional[capi.Handle] = None, transpose=False):
     """AX = A soln (interior (lz,ly,lx) float64 CUDA tensor) through mps_apply_A_dev."""
     import torch

@@ -100,3 +100,90 @@ def random_operator(nx, ny, nz, bc, seed=0, vel=True, reac=True, timederiv=False
     bcv = [rng.uniform(-1, 1, size=s) for s in shapes]
     return Problem(nx, ny, nz, llen, dcoeff=dc, source=src, vel=v, reac=r, bc=bc, bcvals=bcv,
                    timederiv=timederiv, dt=dt, flux=flux)
+
+
+def inject_potential(phi_fine: np.ndarray, n: int) -> np.ndarray:
+    """Cell 2I of a ghosted (2n-1)^3 potential becomes cell I of an n^3 one
+    (injection: 257^3 -> 129^3 keeps cells 0, 2, ..., 256)."""
+    nf = 2 * n - 1
+    assert phi_fine.shape == (nf + 2,) * 3
+    out = np.zeros((n + 2,) * 3)
+    out[1:-1, 1:-1, 1:-1] = phi_fine[1:-1:2, 1:-1:2, 1:-1:2]
+    return out
+
+
+def electron_sg_step(n: int = 129, phi: np.ndarray = None, v_front: float = 1000.0, length: float = 0.01,
+                     dt: float = 1e-11, seed_config: int = 3) -> Problem:
+    """Config 3: one implicit electron drift-diffusion step with
+    Scharfetter-Gummel faces on an n^3 grid over a 1 cm cube.
+
+    mobility mu = 0.03 (1 + 0.5 U[0,1]) m^2/Vs, D = mu Te with Te ~ U[1,4] eV,
+    drift v = -mu E with E = -grad(phi) (electrons; the reference stores the
+    signed mobility, ion_elec_chem.f90:234-235), n_old lognormal(ln 1e16, 1)
+    m^-3, time derivative 1/dt on the diagonal and n_old/dt in the source
+    (edeneq.f90:441).  phi is the ghosted potential of the plasma Poisson
+    problem (a (2n-1)^3 solve injected onto n^3, :func:`inject_potential`);
+    None gives the linear ramp 0 -> v_front V along z.  x/y periodic, z ZGRD
+    (zero diffusive flux, convective outflow).
+    """
+    g = (n + 2, n + 2, n + 2)
+    h = length / n
+    if phi is None:
+        z = (np.arange(n) + 0.5) * h
+        phi = np.zeros(g)
+        phi[1:-1, 1:-1, 1:-1] = (v_front * z / length)[:, None, None]
+    ph = np.array(phi, dtype=np.float64, copy=True)
+    # ghosts of phi: periodic in x/y, Dirichlet 0 / v_front at z=0 / z=L
+    ph[1:-1, 1:-1, 0] = ph[1:-1, 1:-1, -2]
+    ph[1:-1, 1:-1, -1] = ph[1:-1, 1:-1, 1]
+    ph[1:-1, 0, 1:-1] = ph[1:-1, -2, 1:-1]
+    ph[1:-1, -1, 1:-1] = ph[1:-1, 1, 1:-1]
+    ph[0, 1:-1, 1:-1] = -ph[1, 1:-1, 1:-1]
+    ph[-1, 1:-1, 1:-1] = 2.0 * v_front - ph[-2, 1:-1, 1:-1]
+    c = ph[1:-1, 1:-1, 1:-1]
+    gx = (ph[1:-1, 1:-1, 2:] - ph[1:-1, 1:-1, :-2]) / (2 * h)
+    gy = (ph[1:-1, 2:, 1:-1] - ph[1:-1, :-2, 1:-1]) / (2 * h)
+    gz = (ph[2:, 1:-1, 1:-1] - ph[:-2, 1:-1, 1:-1]) / (2 * h)
+    del c
+    mu = 0.03 * (1.0 + 0.5 * _rng(seed_config, 1).uniform(0.0, 1.0, size=(n, n, n)))
+    te = _rng(seed_config, 2).uniform(1.0, 4.0, size=(n, n, n))
+    nold = _rng(seed_config, 3).lognormal(mean=np.log(1e16), sigma=1.0, size=(n, n, n))
+
+    def ghosted(a):
+        out = np.zeros(g)
+        out[1:-1, 1:-1, 1:-1] = a
+        out[1:-1, 1:-1, 0] = a[:, :, -1]
+        out[1:-1, 1:-1, -1] = a[:, :, 0]
+        out[1:-1, 0, 1:-1] = a[:, -1, :]
+        out[1:-1, -1, 1:-1] = a[:, 0, :]
+        out[0, 1:-1, 1:-1] = a[0]
+        out[-1, 1:-1, 1:-1] = a[-1]
+        return out
+
+    # v = -mu E = mu grad(phi)
+    vel = np.stack([ghosted(mu * gx), ghosted(mu * gy), ghosted(mu * gz)])
+    dc = ghosted(mu * te)
+    src = ghosted(nold / dt)
+    return Problem(n, n, n, (length, length, length), dcoeff=dc, source=src, vel=vel,
+                   bc=["PERI", "PERI", "PERI", "PERI", "ZGRD", "ZGRD"], bcvals=[None] * 6,
+                   timederiv=True, dt=dt, flux=1)
+
+
+BATCH_SIZES = (33, 49, 65, 97, 129)
+
+
+def batch_poisson(count: int = 64, sizes=BATCH_SIZES, seed_config: int = 4):
+    """Config 4: ``count`` independent constant-coefficient Poisson problems on
+    the unit cube, cubic sizes drawn uniformly from ``sizes``, Dirichlet 0,
+    right-hand sides U[-1,1] (a seed per problem)."""
+    ns = _rng(seed_config, 0).choice(np.asarray(sizes), size=count)
+    out = []
+    for q, n in enumerate(ns):
+        n = int(n)
+        g = (n + 2, n + 2, n + 2)
+        dc = np.zeros(g)
+        dc[1:-1, 1:-1, 1:-1] = 1.0
+        src = np.zeros(g)
+        src[1:-1, 1:-1, 1:-1] = _rng(seed_config, 1 + q).uniform(-1.0, 1.0, size=(n, n, n))
+        out.append(Problem(n, n, n, (1.0, 1.0, 1.0), dcoeff=dc, source=src, bc=["DIRC"] * 6, bcvals=[0.0] * 6))
+    return out

@@ -166,3 +166,21 @@ def test_failures_return_status(handle):
     # the handle stays usable after errors
     x, info = solver.linsolve(r, handle=handle)
     assert info["status"] == 0
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_electron_sg_step_matches_oracle(handle, prec):
+    """Implicit SG electron step (potential: a 33^3 plasma Poisson solve
+    injected onto 17^3), FGMRES(30) with a V-cycle preconditioner."""
+    pp = W.plasma_poisson(33, slab_cells=4)
+    phi_i, _ = _oracle_solution(pp)
+    phi = np.zeros((35, 35, 35))
+    phi[1:-1, 1:-1, 1:-1] = phi_i
+    p = W.electron_sg_step(17, phi=W.inject_potential(phi, 17))
+    ref, b = _oracle_solution(p)
+    x, info = solver.linsolve(p, handle=handle, tol=1e-11, precision=prec, krylov="fgmres", restart=30, maxit=60)
+    assert info["status"] == 0, info
+    xi = x[1:-1, 1:-1, 1:-1]
+    rel_res = np.linalg.norm(b - O.rows_apply(p, O.build_rows(p), np.ascontiguousarray(xi))) / np.linalg.norm(b)
+    assert rel_res <= 1e-10, rel_res
+    assert np.linalg.norm(xi - ref) / np.linalg.norm(ref) <= 1e-9
