@@ -363,6 +363,51 @@ def bench_batch(args, ws, h, dev):
     return out
 
 
+def bench_adjoint(args, ws, h, dev):
+    """Electron-flux adjoint at 129^3: loss = electron flux through z = L
+    after 5 implicit SG steps; gradients w.r.t. the electrode voltage and the
+    FP32 mobility field (torch.autograd over the C ABI: transposed SG solves,
+    operator VJP, symmetric Poisson adjoint).  Timed: one forward + backward;
+    checked: central differences with h = 1e-4 relative."""
+    import torch
+
+    from mps3d_b200 import workloads as W
+    from mps3d_b200.adjoint import ElectronFluxAdjoint
+
+    case = W.electron_adjoint_case(129)
+    model = ElectronFluxAdjoint(case, device=f"cuda:{dev}", handle=h, tol=1e-12)
+    V = case["v_front"]
+    mu = torch.from_numpy(case["mu"]).to(f"cuda:{dev}")
+    for _ in range(2):
+        L0, gV, gmu = model.gradient(V, mu)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    steps = max(1, args.steps // 2)
+    for _ in range(steps):
+        L0, gV, gmu = model.gradient(V, mu)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = dist_max(e0.elapsed_time(e1), ws) / steps
+    # central differences on the FP64 model (mobility perturbed in FP64)
+    tight = ElectronFluxAdjoint(case, device=f"cuda:{dev}", handle=h, tol=1e-13)
+    _, gV_t, gmu_t = tight.gradient(V, mu)
+    mu64 = mu.double()
+    f = lambda v, m: float(tight.loss(torch.tensor(v, dtype=torch.float64, device=mu.device), m))  # noqa: E731
+    hv = 1e-4 * V
+    fd_V = (f(V + hv, mu64) - f(V - hv, mu64)) / (2 * hv)
+    d = torch.from_numpy(np.random.default_rng(5005).uniform(-1.0, 1.0, size=mu.shape)).to(mu.device) * mu64 * 1e-4
+    fd_mu = (f(V, mu64 + d) - f(V, mu64 - d)) / 2.0
+    an_mu = float((gmu_t.double() * d).sum())
+    return {"workload": "electron flux through z=L after 5 implicit SG steps, 129^3 (plasma Poisson potential with "
+                        "electrode voltage V; mobility mu FP32 field); gradients w.r.t. V and mu",
+            "unit": "gradients/s", "value": ws * 1e3 / ms, "ms_per_gradient": ms, "loss": L0,
+            "dL_dV": gV, "fd_dL_dV": fd_V, "rel_err_V": abs(fd_V - gV_t) / abs(gV_t),
+            "rel_err_mu_directional": abs(fd_mu - an_mu) / abs(an_mu),
+            "fd_step": "1e-4 relative (V; every mobility cell along a random direction)"}
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -501,6 +546,7 @@ def run_ours(args, ws, rank, local):
     if not args.skip_others and n == 257:
         others["sg_step_129"] = bench_sg_step(args, ws, h, x, dev)
         others["batch64"] = bench_batch(args, ws, h, dev)
+        others["adjoint_129"] = bench_adjoint(args, ws, h, dev)
 
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "colour_pass_traffic.json")

@@ -218,6 +218,21 @@ typedef struct mps_problem {
 int mps_linsolve_batched_dev(mps_handle h, int nprob, const mps_problem* probs,
                              const mps_solver_opts* opts, mps_solve_info* infos, void* stream);
 
+/* Adjoint of a solve, operator part (extension: the reference has no
+ * adjoint).  Gradients of s = lam^T A(vel, dcoeff, reac) u with respect to the
+ * operator's cell fields, for interior lam and u (Fortran order, lx*ly*lz):
+ * gvel (3 x interior), gdcoeff, greac (interior); any output may be NULL.
+ * With x = A^{-1} b and lam = A^{-T} dL/dx (mps_linsolve_dev with
+ * opts->transpose = 1), dL/dtheta = -(this result).  vel may be NULL; opts
+ * selects the flux (NULL = upwind); uniform grid (dx = llen/l).  Queued on
+ * `stream` (NULL = default stream), not waited for; allocates nothing.
+ * The dependence of b on the fields (DIRC faces of SG operators) is not
+ * included. */
+int mps_operator_vjp_dev(const mps_grid* g, const double* vel, const double* dcoeff,
+                         const int bc_code[6], const double* lam, const double* u,
+                         const mps_solver_opts* opts, double* gvel, double* gdcoeff,
+                         double* greac, void* stream);
+
 /* AX = A soln like mps_apply_A_dev, for callers that must not allocate device
  * memory.  No counterpart in the reference: its find_AX works on arrays the
  * caller already owns, so it never needed one.  Callers that cannot allocate

@@ -40,7 +40,7 @@ EXPORTS = [
     "mps_default_opts", "mps_version", "mps_create", "mps_destroy", "mps_stream", "mps_last_error",
     "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once", "mps_apply_A_dev", "mps_find_bvec_dev",
     "mps_fill_ghosts_dev", "mps_set_profile", "mps_get_profile", "mps_apply_A_noalloc",
-    "mps_linsolve_batched_dev",
+    "mps_linsolve_batched_dev", "mps_operator_vjp_dev",
 ]
 
 PROF_SMOOTH, PROF_RESTRICT, PROF_PROLONG, PROF_RESID, PROF_NCLASS = 0, 1, 2, 3, 8
@@ -122,11 +122,12 @@ def load(build_if_missing: bool = False):
     L.mps_set_profile.argtypes = [vp, C.c_int]
     L.mps_get_profile.argtypes = [vp, C.POINTER(Profile), C.c_int]
     L.mps_linsolve_batched_dev.argtypes = [vp, C.c_int, C.POINTER(ProblemDesc), C.POINTER(Opts), C.POINTER(Info), vp]
+    L.mps_operator_vjp_dev.argtypes = [C.POINTER(Grid), vp, vp, ip, vp, vp, C.POINTER(Opts), vp, vp, vp, vp]
     L.mps_apply_A_noalloc.argtypes = [C.POINTER(Grid), C.c_int, C.c_double, vp, vp, vp, ip, vp, vp, C.POINTER(Opts),
                                       vp]
     for name in ("mps_set_profile", "mps_get_profile", "mps_create", "mps_destroy", "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once",
                  "mps_apply_A_dev", "mps_find_bvec_dev", "mps_fill_ghosts_dev", "mps_apply_A_noalloc",
-                 "mps_linsolve_batched_dev"):
+                 "mps_linsolve_batched_dev", "mps_operator_vjp_dev"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -187,3 +187,23 @@ def batch_poisson(count: int = 64, sizes=BATCH_SIZES, seed_config: int = 4):
         src[1:-1, 1:-1, 1:-1] = _rng(seed_config, 1 + q).uniform(-1.0, 1.0, size=(n, n, n))
         out.append(Problem(n, n, n, (1.0, 1.0, 1.0), dcoeff=dc, source=src, bc=["DIRC"] * 6, bcvals=[0.0] * 6))
     return out
+
+
+def electron_adjoint_case(n: int = 129, v_front: float = 1000.0, length: float = 0.01, dt: float = 1e-11,
+                          steps: int = 5, slab_cells: int = None):
+    """Config 5: the fields of the electron-flux adjoint on an n^3 grid.
+
+    The plasma Poisson problem of config 2 at n^3 (dielectric slab of
+    ``slab_cells`` cells, default 10 n / 257 rounded, so the same 0.39 mm),
+    whose FRONT Dirichlet value is the electrode voltage, and the electron
+    step of config 3 (mobility, Te, n_old) repeated ``steps`` times.  Returns
+    a dict of numpy arrays; ``mu`` is float32 (the differentiated field).
+    """
+    if slab_cells is None:
+        slab_cells = max(1, int(round(10 * n / 257)))
+    pp = plasma_poisson(n, slab_cells=slab_cells, v_front=v_front, length=length)
+    mu = (0.03 * (1.0 + 0.5 * _rng(3, 1).uniform(0.0, 1.0, size=(n, n, n)))).astype(np.float32)
+    te = _rng(3, 2).uniform(1.0, 4.0, size=(n, n, n))
+    nold = _rng(3, 3).lognormal(mean=np.log(1e16), sigma=1.0, size=(n, n, n))
+    return {"n": n, "length": length, "dt": dt, "steps": steps, "v_front": v_front, "eps": pp.dcoeff,
+            "rho": pp.source, "mu": mu, "te": te, "n_old": nold}

@@ -1023,6 +1023,132 @@ void orc_sg_face(double cL, double cR, double DL, double DR, double dx, double* 
     }
 }
 
+/* derivatives of orc_sg_face with respect to (cL, cR, DL, DR), differentiated
+ * branch by branch from the closed forms above (extension: the reference has
+ * no adjoint).  dwL[q], dwR[q] for q = cL, cR, DL, DR. */
+void orc_sg_face_d(double cL, double cR, double DL, double DR, double dx, double* dwL, double* dwR)
+{
+    const double eps = 1.0e-10;
+    const double c = 0.5 * (cL + cR);
+    const double S = DL + DR + eps;
+    const double D = 2.0 * DL * DR / S;
+    const double dD_dL = 2.0 * DR * (DR + eps) / (S * S), dD_dR = 2.0 * DL * (DL + eps) / (S * S);
+    double wLc = 0.0, wLD = 0.0, wRc = 0.0, wRD = 0.0;
+    for (int q = 0; q < 4; q++) dwL[q] = dwR[q] = 0.0;
+    if (fabs(D) < eps) {
+        const double sgn = c <= 0.0 ? -1.0 : 1.0;
+        dwL[0] = 0.5 * (1.0 + sgn);
+        dwR[1] = 0.5 * (1.0 - sgn);
+        return;
+    }
+    const double Pe = c * dx / D;
+    if (fabs(Pe) < eps) {
+        wLD = 1.0 / dx;
+        wRD = -1.0 / dx;
+    } else if (fabs(Pe) < 1.0e-2) {
+        /* the closed forms below cancel as Pe -> 0: Taylor series of the same
+         * weights, wL = c/(1 - e^-Pe) = (D/dx)(1 + Pe/2 + Pe^2/12 - Pe^4/720 + ...),
+         * wR = c - wL, truncated after the Pe^6 terms */
+        const double P2 = Pe * Pe;
+        wLc = 0.5 + Pe / 6.0 - P2 * Pe / 180.0 + P2 * P2 * Pe / 5040.0;
+        wRc = 1.0 - wLc;
+        wLD = (1.0 - P2 / 12.0 + P2 * P2 / 240.0 - P2 * P2 * P2 / 6048.0) / dx;
+        wRD = -wLD;
+    } else if (Pe > 0.0) {
+        const double E = exp(-Pe), q1 = 1.0 - E;
+        wLc = 1.0 / q1 - Pe * E / (q1 * q1);
+        wLD = c * E * Pe / (D * q1 * q1);
+        wRc = -E / q1 + Pe * E / (q1 * q1);
+        wRD = -c * E * Pe / (D * q1 * q1);
+    } else {
+        const double P = exp(Pe), q1 = P - 1.0;
+        wLc = P / q1 - Pe * P / (q1 * q1);
+        wLD = c * P * Pe / (D * q1 * q1);
+        wRc = -1.0 / q1 + Pe * P / (q1 * q1);
+        wRD = -c * P * Pe / (D * q1 * q1);
+    }
+    dwL[0] = 0.5 * wLc; dwL[1] = 0.5 * wLc; dwL[2] = wLD * dD_dL; dwL[3] = wLD * dD_dR;
+    dwR[0] = 0.5 * wRc; dwR[1] = 0.5 * wRc; dwR[2] = wRD * dD_dL; dwR[3] = wRD * dD_dR;
+}
+
+/* gradients of s = lam^T A(vel, dcoeff, reac) u with respect to the cell
+ * fields (interior arrays lam, u; uniform grid), accumulated face by face:
+ * a face (L, R) with flux F = wL u_L + wR u_R adds F (lam_L - lam_R) / h to s,
+ * boundary and diagonal terms add lam_c u_c times their coefficient. */
+void orc_operator_vjp(const orc_grid* g, int flux, const double* vel, const double* dcoeff, const int* bc,
+                      const double* lam, const double* u, double* gvel, double* gd, double* greac)
+{
+    const int lx = g->lx, ly = g->ly, lz = g->lz;
+    const long ng = ngh(lx, ly, lz), n = nin(lx, ly, lz);
+    const int L[3] = {lx, ly, lz};
+    const double h[3] = {g->llenx / lx, g->lleny / ly, g->llenz / lz};
+    memset(gvel, 0, sizeof(double) * 3 * n);
+    memset(gd, 0, sizeof(double) * n);
+    for (long c = 0; c < n; c++) greac[c] = -lam[c] * u[c];
+    for (int ax = 0; ax < 3; ax++) {
+        const double* v = vel + ax * ng;
+        double* gv = gvel + ax * n;
+        const int per = bc[2 * ax] == ORC_PERI;
+        const double hx = h[ax];
+        for (int k = 1; k <= lz; k++)
+            for (int j = 1; j <= ly; j++)
+                for (int i = 1; i <= lx; i++) {
+                    int idx[3] = {i, j, k};
+                    const int pos = idx[ax];
+                    const long c = IX(i, j, k);
+                    const double vc = v[GX(i, j, k)], kc = dcoeff[GX(i, j, k)];
+                    if (pos < L[ax] || per) {
+                        int r3[3] = {i, j, k};
+                        r3[ax] = pos < L[ax] ? pos + 1 : 1;
+                        const long cr = IX(r3[0], r3[1], r3[2]);
+                        const double vr = v[GX(r3[0], r3[1], r3[2])], kr = dcoeff[GX(r3[0], r3[1], r3[2])];
+                        double dwL[4], dwR[4];
+                        if (flux == ORC_FLUX_SG) {
+                            orc_sg_face_d(vc, vr, kc, kr, hx, dwL, dwR);
+                        } else {
+                            const double vh = 0.5 * (vc + vr);
+                            const double a = 0.5 / hx;
+                            dwL[0] = dwL[1] = vh > 0.0 ? 0.5 : 0.0;
+                            dwR[0] = dwR[1] = vh > 0.0 ? 0.0 : 0.5;
+                            dwL[2] = dwL[3] = a;
+                            dwR[2] = dwR[3] = -a;
+                        }
+                        const double m = (lam[c] - lam[cr]) / hx;
+                        gv[c] += m * (dwL[0] * u[c] + dwR[0] * u[cr]);
+                        gv[cr] += m * (dwL[1] * u[c] + dwR[1] * u[cr]);
+                        gd[c] += m * (dwL[2] * u[c] + dwR[2] * u[cr]);
+                        gd[cr] += m * (dwL[3] * u[c] + dwR[3] * u[cr]);
+                    }
+                    if (!per && (pos == 1 || pos == L[ax])) {
+                        for (int side = 0; side < 2; side++) {
+                            if ((side == 0 && pos != 1) || (side == 1 && pos != L[ax])) continue;
+                            const int code = bc[2 * ax + side];
+                            const double lu = lam[c] * u[c];
+                            if (code == ORC_DIRC) {
+                                if (flux == ORC_FLUX_SG) {
+                                    double dwL[4], dwR[4];
+                                    orc_sg_face_d(vc, vc, kc, kc, 0.5 * hx, dwL, dwR);
+                                    if (side == 0) {
+                                        gv[c] -= lu * (dwR[0] + dwR[1]) / hx;
+                                        gd[c] -= lu * (dwR[2] + dwR[3]) / hx;
+                                    } else {
+                                        gv[c] += lu * (dwL[0] + dwL[1]) / hx;
+                                        gd[c] += lu * (dwL[2] + dwL[3]) / hx;
+                                    }
+                                } else {
+                                    gd[c] += lu * 2.0 / (hx * hx);
+                                    if (side == 0 && vc < 0.0) gv[c] -= lu / hx;
+                                    if (side == 1 && vc > 0.0) gv[c] += lu / hx;
+                                }
+                            } else if (code == ORC_ZGRD) {
+                                gv[c] += side == 0 ? -lu / hx : lu / hx;
+                            }
+                        }
+                    }
+                }
+    }
+}
+
 #define R7(q, c) rows[(long)(q) * n + (c)]
 
 /* upwind rows from the find_AX formulas (discretepde.f90:620-1116); SG rows

@@ -88,6 +88,11 @@ void orc_build_rhs(const orc_grid* g, int flux, const double* vel, const double*
 void orc_rows_apply(const orc_grid* g, const int* bc, const double* rows,
                     const double* u, double* Au);
 void orc_rows_transpose(const orc_grid* g, const int* bc, const double* rows, double* rowsT);
+/* gradients of lam^T A(vel, dcoeff, reac) u (interior lam, u; uniform grid)
+ * with respect to vel (3 x interior), dcoeff and reac (interior) */
+void orc_operator_vjp(const orc_grid* g, int flux, const double* vel, const double* dcoeff, const int* bc,
+                      const double* lam, const double* u, double* gvel, double* gd, double* greac);
+void orc_sg_face_d(double cL, double cR, double DL, double DR, double dx, double* dwL, double* dwR);
 void orc_sg_face(double cL, double cR, double DL, double DR, double dx,
                  double* wL, double* wR);
 /* correction-scheme V-cycle over rows operators (coarse rows rediscretised

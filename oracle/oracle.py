@@ -60,6 +60,8 @@ def lib():
         L.orc_rows_apply.argtypes = [gp, ip, dp, dp, dp]
         L.orc_rows_transpose.argtypes = [gp, ip, dp, dp]
         L.orc_sg_face.argtypes = [C.c_double] * 5 + [dp, dp]
+        L.orc_sg_face_d.argtypes = [C.c_double] * 5 + [dp, dp]
+        L.orc_operator_vjp.argtypes = [gp, C.c_int, dp, dp, ip, dp, dp, dp, dp, dp]
         L.orc_mg_create.argtypes = [gp, C.c_int, C.c_int, C.c_double, dp, dp, dp, ip, C.c_int]
         L.orc_mg_create.restype = C.c_void_p
         L.orc_mg_destroy.argtypes = [C.c_void_p]
@@ -195,6 +197,26 @@ def sg_face(cL, cR, DL, DR, dx):
     wL, wR = C.c_double(), C.c_double()
     lib().orc_sg_face(cL, cR, DL, DR, dx, C.byref(wL), C.byref(wR))
     return wL.value, wR.value
+
+
+def operator_vjp(prob, lam, u, flux=None):
+    """Gradients of lam^T A u with respect to vel (3, lz, ly, lx), dcoeff and
+    reac (lz, ly, lx) for interior lam, u (uniform grid)."""
+    g = _grid(prob)
+    fl = prob.flux if flux is None else flux
+    gv = np.zeros((3,) + prob.shape)
+    gd = np.zeros(prob.shape)
+    gr = np.zeros(prob.shape)
+    vel = prob.vel if prob.vel is not None else np.zeros((3,) + prob.ghost_shape)
+    lib().orc_operator_vjp(C.byref(g), fl, _p(np.ascontiguousarray(vel)), _p(prob.dcoeff), _bc(prob),
+                           _p(np.ascontiguousarray(lam)), _p(np.ascontiguousarray(u)), _p(gv), _p(gd), _p(gr))
+    return gv, gd, gr
+
+
+def sg_face_d(cL, cR, DL, DR, dx):
+    dwL, dwR = (C.c_double * 4)(), (C.c_double * 4)()
+    lib().orc_sg_face_d(cL, cR, DL, DR, dx, dwL, dwR)
+    return list(dwL), list(dwR)
 
 
 class RowsMG:
