@@ -172,11 +172,16 @@ def electron_sg_step(n: int = 129, phi: np.ndarray = None, v_front: float = 1000
 BATCH_SIZES = (33, 49, 65, 97, 129)
 
 
+def batch_sizes(count: int = 64, sizes=BATCH_SIZES, seed_config: int = 4):
+    """The cubic sizes of :func:`batch_poisson` (without building the fields)."""
+    return [int(n) for n in _rng(seed_config, 0).choice(np.asarray(sizes), size=count)]
+
+
 def batch_poisson(count: int = 64, sizes=BATCH_SIZES, seed_config: int = 4):
     """Config 4: ``count`` independent constant-coefficient Poisson problems on
     the unit cube, cubic sizes drawn uniformly from ``sizes``, Dirichlet 0,
     right-hand sides U[-1,1] (a seed per problem)."""
-    ns = _rng(seed_config, 0).choice(np.asarray(sizes), size=count)
+    ns = batch_sizes(count, sizes, seed_config)
     out = []
     for q, n in enumerate(ns):
         n = int(n)
