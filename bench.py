@@ -244,6 +244,37 @@ def timed_solves(dp, xg, h, steps, ws, init=None, **kw):
     return dist_max(e0.elapsed_time(e1), ws) / steps, info
 
 
+def bench_poisson65(args, ws, rank, h, dev):
+    """Plain FP64 Poisson, 65^3 cells on the unit cube, coefficient 1, Dirichlet
+    0, U[-1,1] right-hand side, to 1e-10 relative residual: GPU solves/s (mixed
+    and FP64) and, on rank 0 with one GPU, the oracle's restatement of the
+    reference's V-cycle loop solving the 64^3 power-of-two twin on the host
+    cores (the reference cannot coarsen 65)."""
+    import torch
+
+    from mps3d_b200 import solver, workloads as W
+
+    p = W.poisson_dirichlet(65)
+    dp = solver.DeviceProblem(p, device=f"cuda:{dev}")
+    x = torch.zeros(p.ghost_shape, dtype=torch.float64, device=f"cuda:{dev}")
+    out = {"workload": "Poisson 65^3, unit cube, coefficient 1, Dirichlet 0, U[-1,1] source, 1e-10 rel. residual",
+           "unit": "solves/s"}
+    for prec in ("mixed", "fp64"):
+        ms, info = timed_solves(dp, x, h, args.steps, ws, precision=prec, tol=1e-10, maxit=60)
+        out[prec] = {"value": ws * 1e3 / ms, "ms_per_solve": ms, "iters": info["iters"], "rel_res": info["rel_res"]}
+    if rank == 0 and ws == 1 and not args.skip_cpu:
+        from oracle import oracle as orc
+
+        q = W.poisson_dirichlet(64)
+        t0 = time.perf_counter()
+        _, rel, _ = orc.solve(q, maxit=40, tol=1e-10, tol_kind=1)
+        t = time.perf_counter() - t0
+        out["cpu_oracle_64"] = {"s_per_solve": t, "vcycles": int(len(rel)), "final_rel_res": float(rel[-1]),
+                                "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                                "kind": "port (restatement of perform_vcycle, CELL hierarchy, 64^3 twin)"}
+    return out
+
+
 def bench_sg_step(args, ws, h, phi_fine, dev):
     """Implicit SG electron step, 129^3: the potential is the 257^3 plasma
     Poisson solution injected onto 129^3; FGMRES(30) preconditioned by an FP32
@@ -518,6 +549,7 @@ def run_ours(args, ws, rank, local):
     # ---- secondary configurations (figures beside the headline line) ----
     others = {}
     if not args.skip_others and n == 257:
+        others["poisson_65"] = bench_poisson65(args, ws, rank, h, dev)
         others["sg_step_129"] = bench_sg_step(args, ws, h, x, dev)
         others["batch64"] = bench_batch(args, ws, rank, h, dev)
         others["adjoint_129"] = bench_adjoint(args, ws, h, dev)
