@@ -166,14 +166,29 @@ __device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int 
     k4 = kfield ? ldv<T, W>(kb + off) : zerov<T, W>();
 }
 
-// Row evaluation of W consecutive cells of one colour on a uniform level
-// (vector loads).  Row (j,k), group g: split offsets o0..o0+W-1 with
-// o0 = W g + P (j + ny k); i = 2(W g + e) + q, q = (j+k+c)&1.  The x
-// neighbours of the group are the other colour at o0+q-1 .. o0+q+W-1 (one
-// vector plus one scalar), the y/z neighbours one vector each.  Returns
-// diag and offdiag (sum_n a_n u_n) per element; elements with i >= nx are
-// padding.
-template <class T, int W, class U>
+// Row evaluation of W consecutive cells of one colour (vector loads).  Row
+// (j,k), group g: split offsets o0..o0+W-1 with o0 = W g + P (j + ny k);
+// i = 2(W g + e) + q, q = (j+k+c)&1.  The x neighbours of the group are the
+// other colour at o0+q-1 .. o0+q+W-1 (one vector plus one scalar), the y/z
+// neighbours one vector each.  Returns diag and offdiag (sum_n a_n u_n) per
+// element; elements with i >= nx are padding.  UNI: every face has the
+// regular coefficient (a uniform level); otherwise the faces touching the
+// last cell of an axis (a merged odd cell of the geometric hierarchy) take
+// their own coefficients, as in row_eval (fcoef_ax / dcoef_ax).
+template <int AX, bool UNI>
+__device__ __forceinline__ double face_c(const Lev& L, int p, int q)
+{
+    if (UNI) return L.cr[AX];
+    return fcoef_ax<AX>(L, p, q);
+}
+template <int AX, bool UNI>
+__device__ __forceinline__ double dir_c(const Lev& L, int p)
+{
+    if (UNI) return L.dr[AX];
+    return dcoef_ax<AX>(L, p);
+}
+
+template <class T, int W, class U, bool UNI = true>
 __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c, const U& u, int row, int j,
                                            int k, int h0, int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
 {
@@ -183,7 +198,11 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
     const T* us = u.ptr(cc);
     const T* ko = kfield ? sel(op.k, oc) : nullptr;
     const T* ks = kfield ? sel(op.k, cc) : nullptr;
-    const T cx = (T)L.cr[0], cy = (T)L.cr[1], cz = (T)L.cr[2];
+    // y and z face coefficients of this row (the wrapped neighbour of a
+    // periodic face is the last cell when p = 0)
+    const int ny1 = L.ny - 1, nz1 = L.nz - 1;
+    const T cym = (T)face_c<1, UNI>(L, j, j > 0 ? j - 1 : ny1), cyp = (T)face_c<1, UNI>(L, j, j < ny1 ? j + 1 : 0);
+    const T czm = (T)face_c<2, UNI>(L, k, k > 0 ? k - 1 : nz1), czp = (T)face_c<2, UNI>(L, k, k < nz1 ? k + 1 : 0);
 
     VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
     const VecW<T, W> kc4 = kfield ? ldv<T, W>(ks + o0) : zerov<T, W>();
@@ -204,11 +223,12 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
             }                                                                                                 \
         }                                                                                                     \
     }
-    MPS_YZ(1, -1, cy, dcount_y)
-    MPS_YZ(1, 1, cy, dcount_y)
-    MPS_YZ(2, -1, cz, dcount_z)
-    MPS_YZ(2, 1, cz, dcount_z)
+    MPS_YZ(1, -1, cym, dcount_y)
+    MPS_YZ(1, 1, cyp, dcount_y)
+    MPS_YZ(2, -1, czm, dcount_z)
+    MPS_YZ(2, 1, czp, dcount_z)
 #undef MPS_YZ
+    const T byz = (T)dcount_y * (T)dir_c<1, UNI>(L, j) + (T)dcount_z * (T)dir_c<2, UNI>(L, k);
 
     // x neighbours: A = other colour at o0..o0+W-1, S = o0+W (q=1) or o0-1 (q=0)
     const VecW<T, W> ax = uo ? ldv<T, W>(uo + o0) : zerov<T, W>();
@@ -220,6 +240,7 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
         sx = u.ld(uo, so);
         skx = kfield ? __ldg(ko + so) : T(0);
     }
+    const int nx1 = L.nx - 1;
 #pragma unroll
     for (int e = 0; e < W; e++) {
         const int i = 2 * (h0 + e) + q;
@@ -232,20 +253,20 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
             uxp = ax.v[e]; kxp = akx.v[e];
         }
         T mxm = T(1), mxp = T(1);
-        int dx = 0;
+        T bx = T(0);
         if (i == 0) {  // x- boundary / periodic wrap
             if (L.per[0]) {
-                const int a = L.nx - 1;
+                const int a = nx1;
                 const int wo = (a >> 1) + L.P * row;
                 const bool same = ((a + j + k) & 1) == cc;
                 uxm = u.ld(same ? us : uo, wo);
                 kxm = kfield ? __ldg((same ? ks : ko) + wo) : T(0);
             } else {
                 mxm = T(0);
-                dx += L.bc[0] == BC_DIRC;
+                if (L.bc[0] == BC_DIRC) bx += (T)dir_c<0, UNI>(L, i);
             }
         }
-        if (i == L.nx - 1) {  // x+ boundary / periodic wrap
+        if (i == nx1) {  // x+ boundary / periodic wrap
             if (L.per[0]) {
                 const int wo = L.P * row;
                 const bool same = ((j + k) & 1) == cc;
@@ -253,17 +274,18 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
                 kxp = kfield ? __ldg((same ? ks : ko) + wo) : T(0);
             } else {
                 mxp = T(0);
-                dx += L.bc[1] == BC_DIRC;
+                if (L.bc[1] == BC_DIRC) bx += (T)dir_c<0, UNI>(L, i);
             }
         }
+        const T cxm = (T)face_c<0, UNI>(L, i, i > 0 ? i - 1 : nx1), cxp = (T)face_c<0, UNI>(L, i, i < nx1 ? i + 1 : 0);
         const T kc = kfield ? kc4.v[e] : op.kc;
         const T d0 = op.dex[0] ? __ldg(sel(op.dex, cc) + o0 + e) : op.dexc;
         T w0, w1;
-        if (kfield) { w0 = mxm * (kc + kxm) * cx; w1 = mxp * (kc + kxp) * cx; }
-        else { w0 = mxm * cx; w1 = mxp * cx; }
+        if (kfield) { w0 = mxm * (kc + kxm) * cxm; w1 = mxp * (kc + kxp) * cxp; }
+        else { w0 = mxm * cxm; w1 = mxp * cxp; }
         const T ws = wsum.v[e] + (w0 + w1);
         const T ac = acc.v[e] + (w0 * uxm + w1 * uxp);
-        const T bnd = T(2) * ((T)dx * cx + (T)dcount_y * cy + (T)dcount_z * cz);
+        const T bnd = bx + byz;
         if (kfield) { diag.v[e] = d0 + T(0.5) * ws + kc * bnd; off.v[e] = T(-0.5) * ac; }
         else { diag.v[e] = d0 + kc * (ws + bnd); off.v[e] = -kc * ac; }
     }
@@ -289,17 +311,18 @@ __device__ __forceinline__ bool group_decode(const Lev& L, const FastDiv& divG, 
     return true;
 }
 
-// colour pass on a uniform level: W cells of colour c per thread.  Elements
-// past the end of the row (pads) are written as 0.  Same results as k_colour.
+// colour pass, W cells of colour c per thread (vector loads).  Elements past
+// the end of the row (pads) are written as 0.  Same results as k_colour.
 template <class T, int W, class U>
 __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
                                                     const T* __restrict__ f, FastDiv divG)
 {
     GroupIdx G;
     if (!group_decode<W>(L, divG, c, G)) return;
-    VecW<T, W> diag, off;
-    group_rows<T, W, U>(L, op, c, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
     const VecW<T, W> f4 = ldv<T, W>(f + G.o0);
+    VecW<T, W> diag, off;
+    if (L.uniform) group_rows<T, W, U, true>(L, op, c, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
+    else group_rows<T, W, U, false>(L, op, c, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
     VecW<T, W> res;
 #pragma unroll
     for (int e = 0; e < W; e++) {
@@ -316,8 +339,7 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, 
 template <class T, int W, class R>
 __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_residv(Lev L, KOp<T> op, int c, CSplit<T> u,
                                                                        const T* __restrict__ f, R* __restrict__ rout,
-                                                                       RedBuf rb, int accumulate, FastDiv divG,
-                                                                       int seam_only)
+                                                                       RedBuf rb, int accumulate, FastDiv divG)
 {
     __shared__ double sh[32];
     double rr = 0.0, ff = 0.0;
@@ -332,31 +354,31 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_residv(Lev L, K
         G.k = (int)L.divNy.div(row);
         G.j = (int)row - G.k * L.ny;
         G.h0 = W * (int)(t - row * (unsigned)(L.P / W));
-        G.q = (G.j + G.k + c) & 1;
         G.o0 = G.h0 + L.P * (int)row;
-        if (seam_only) {  // only groups touching an odd periodic seam
-            const bool sx = L.per[0] && (L.nx & 1) && (G.h0 == 0 || 2 * (G.h0 + W) + 1 >= L.nx);
-            const bool sy = L.per[1] && (L.ny & 1) && (G.j == 0 || G.j == L.ny - 1);
-            const bool sz = L.per[2] && (L.nz & 1) && (G.k == 0 || G.k == L.nz - 1);
-            if (!(sx || sy || sz)) continue;
-        }
-        VecW<T, W> diag, off;
-        group_rows<T, W, CSplit<T>>(L, op, c, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
-        const VecW<T, W> f4 = ldv<T, W>(f + G.o0);
-        const VecW<T, W> u4 = ldv<T, W>(u.half(c) + G.o0);
-        VecW<R, W> r4;
+        // c < 0: both colours of the group, one after the other (the second
+        // colour's neighbours were just read as the first colour's centres)
+        const int c0 = c < 0 ? 0 : c, c1 = c < 0 ? 1 : c;
+        for (int cc = c0; cc <= c1; cc++) {
+            G.q = (G.j + G.k + cc) & 1;
+            VecW<T, W> diag, off;
+            group_rows<T, W, CSplit<T>>(L, op, cc, u, G.row, G.j, G.k, G.h0, G.q, G.o0, diag, off);
+            const T* fh = c < 0 ? f + (cc ? L.half : 0) : f;
+            const VecW<T, W> f4 = ldv<T, W>(fh + G.o0);
+            const VecW<T, W> u4 = ldv<T, W>(u.half(cc) + G.o0);
+            VecW<R, W> r4;
 #pragma unroll
-        for (int e = 0; e < W; e++) {
-            const int i = 2 * (G.h0 + e) + G.q;
-            const T r = f4.v[e] - (diag.v[e] * u4.v[e] + off.v[e]);
-            const bool ok = i < L.nx;
-            r4.v[e] = ok ? (R)r : R(0);
-            if (ok) {
-                rr += (double)r * (double)r;
-                ff += (double)f4.v[e] * (double)f4.v[e];
+            for (int e = 0; e < W; e++) {
+                const int i = 2 * (G.h0 + e) + G.q;
+                const T r = f4.v[e] - (diag.v[e] * u4.v[e] + off.v[e]);
+                const bool ok = i < L.nx;
+                r4.v[e] = ok ? (R)r : R(0);
+                if (ok) {
+                    rr += (double)r * (double)r;
+                    ff += (double)f4.v[e] * (double)f4.v[e];
+                }
             }
+            if (rout) stv<R, W>(rout + (c < 0 && cc ? L.half : 0) + G.o0, r4);
         }
-        if (rout) stv<R, W>(rout + G.o0, r4);
     }
     const double a = block_sum(rr, sh);
     const double b = block_sum(ff, sh);
@@ -386,21 +408,20 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_residv(Lev L, K
     }
 }
 
-// restriction of a residual held in split layout (type T) to the coarse
-// right-hand side: mean (volume-weighted for the geometric hierarchy) over
-// the children; with red_only the black children count as 0 (the residual of
-// the colour updated last vanishes up to rounding)
-template <class T>
-__global__ void __launch_bounds__(TPB) k_restrict_res(Lev F, CSplit<T> r, Lev C, Split<T> fc, int geom, int red_only)
+// ---------------------------------------------------------------------
+// residual r = f - A u on the fine level fused with the restriction to the
+// coarse level: coarse value = mean of r over the children {2I,2I+1}^3 that
+// exist (restriction, mgridsteps.f90:11-53, applied to the residual at :531).
+// One thread per coarse cell, natural order.
+// ---------------------------------------------------------------------
+// the share `part` of `nparts` of the children of coarse cell (I,J,K):
+// sum of width-weighted residuals and of the weights
+template <class T, class Op>
+__device__ __forceinline__ void resid_restrict_part(const Lev& F, const Op& op, const CSplit<T>& u,
+                                                    const CSplit<T>& f, const Lev& C, int geom, int I, int J, int K,
+                                                    int part, int nparts, T& s, T& vol)
 {
-    unsigned t = blockIdx.x * TPB + threadIdx.x;
-    const unsigned ncx = C.nx, ncy = C.ny;
-    if (t >= ncx * ncy * (unsigned)C.nz) return;
-    unsigned K = t / (ncx * ncy);
-    unsigned rem = t - K * ncx * ncy;
-    unsigned J = rem / ncx;
-    unsigned I = rem - J * ncx;
-    const int cI[3] = {(int)I, (int)J, (int)K};
+    const int cI[3] = {I, J, K};
     int lo[3], cnt[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -408,54 +429,21 @@ __global__ void __launch_bounds__(TPB) k_restrict_res(Lev F, CSplit<T> r, Lev C,
         lo[a] = nf == nc ? cI[a] : 2 * cI[a];
         cnt[a] = nf == nc ? 1 : ((geom && cI[a] == nc - 1) ? nf - 2 * (nc - 1) : 2);
     }
-    // seam children keep their (non-zero) black residual
-    const bool seamx = F.per[0] && (F.nx & 1), seamy = F.per[1] && (F.ny & 1), seamz = F.per[2] && (F.nz & 1);
-    if (cnt[0] == 2 && cnt[1] == 2 && cnt[2] == 2 && (!geom || F.uniform)) {
-        // regular 2x2x2 block of equal cells
-        T s = T(0);
-#pragma unroll
-        for (int dk = 0; dk < 2; dk++)
-#pragma unroll
-            for (int dj = 0; dj < 2; dj++)
-#pragma unroll
-                for (int di = 0; di < 2; di++) {
-                    const int i = lo[0] + di, j = lo[1] + dj, k = lo[2] + dk;
-                    const bool black = ((di + dj + dk + lo[0] + lo[1] + lo[2]) & 1) != 0;
-                    const bool seam = (seamx && (i == 0 || i == F.nx - 1)) || (seamy && (j == 0 || j == F.ny - 1)) ||
-                                      (seamz && (k == 0 || k == F.nz - 1));
-                    if (!red_only || !black || seam) s += r.get(F, i, j, k);
-                }
-        fc.half(scol(I, J, K))[soff(C, I, J, K)] = s * T(0.125);
-        return;
+    s = T(0);
+    vol = T(0);
+    const int total = cnt[0] * cnt[1] * cnt[2];
+    for (int ch = part; ch < total; ch += nparts) {
+        const int di = ch % cnt[0], dj = (ch / cnt[0]) % cnt[1], dk = ch / (cnt[0] * cnt[1]);
+        const int i = lo[0] + di, j = lo[1] + dj, k = lo[2] + dk;
+        const T v = geom ? (T)(cwidth(F, 0, i) * cwidth(F, 1, j) * cwidth(F, 2, k)) : T(1);
+        T diag, off;
+        row_any<T>(op, F, u, i, j, k, diag, off);
+        const T r = f.get(F, i, j, k) - (diag * u.get(F, i, j, k) + off);
+        s += v * r;
+        vol += v;
     }
-    T s = T(0), vol = T(0);
-    for (int dk = 0; dk < cnt[2]; dk++) {
-        const int k = lo[2] + dk;
-        const T wz = geom ? (T)cwidth(F, 2, k) : T(1);
-        for (int dj = 0; dj < cnt[1]; dj++) {
-            const int j = lo[1] + dj;
-            const T wy = geom ? (T)cwidth(F, 1, j) : T(1);
-            for (int di = 0; di < cnt[0]; di++) {
-                const int i = lo[0] + di;
-                const T wx = geom ? (T)cwidth(F, 0, i) : T(1);
-                const T v = wx * wy * wz;
-                const int col = (i + j + k) & 1;
-                const bool seam = (seamx && (i == 0 || i == F.nx - 1)) || (seamy && (j == 0 || j == F.ny - 1)) ||
-                                  (seamz && (k == 0 || k == F.nz - 1));
-                if (!red_only || col == 0 || seam) s += v * r.get(F, i, j, k);
-                vol += v;
-            }
-        }
-    }
-    fc.half(scol(I, J, K))[soff(C, I, J, K)] = s / vol;
 }
 
-// ---------------------------------------------------------------------
-// residual r = f - A u on the fine level fused with the restriction to the
-// coarse level: coarse value = mean of r over the children {2I,2I+1}^3 that
-// exist (restriction, mgridsteps.f90:11-53, applied to the residual at :531).
-// One thread per coarse cell, natural order.
-// ---------------------------------------------------------------------
 template <class T, class Op>
 __device__ __forceinline__ void resid_restrict_body(const Lev& F, const Op& op, const CSplit<T>& u,
                                                     const CSplit<T>& f, const Lev& C, const Split<T>& fc, int geom,
@@ -463,38 +451,13 @@ __device__ __forceinline__ void resid_restrict_body(const Lev& F, const Op& op, 
 {
     const unsigned ncx = C.nx, ncy = C.ny;
     if (t >= ncx * ncy * (unsigned)C.nz) return;
-    unsigned K = t / (ncx * ncy);
-    unsigned rem = t - K * ncx * ncy;
-    unsigned J = rem / ncx;
-    unsigned I = rem - J * ncx;
-    const int cI[3] = {(int)I, (int)J, (int)K};
-    int lo[3], cnt[3];
-    for (int a = 0; a < 3; a++) {
-        const int nf = lev_n(F, a), nc = lev_n(C, a);
-        lo[a] = nf == nc ? cI[a] : 2 * cI[a];
-        cnt[a] = nf == nc ? 1 : ((geom && cI[a] == nc - 1) ? nf - 2 * (nc - 1) : 2);
-    }
-    T s = T(0), vol = T(0);
-    for (int dk = 0; dk < cnt[2]; dk++) {
-        const int k = lo[2] + dk;
-        const T wz = geom ? (T)cwidth(F, 2, k) : T(1);
-        for (int dj = 0; dj < cnt[1]; dj++) {
-            const int j = lo[1] + dj;
-            const T wy = geom ? (T)cwidth(F, 1, j) : T(1);
-            for (int di = 0; di < cnt[0]; di++) {
-                const int i = lo[0] + di;
-                const T wx = geom ? (T)cwidth(F, 0, i) : T(1);
-                T diag, off;
-                row_any<T>(op, F, u, i, j, k, diag, off);
-                T r = f.get(F, i, j, k) - (diag * u.get(F, i, j, k) + off);
-                const T v = wx * wy * wz;
-                s += v * r;
-                vol += v;
-            }
-        }
-    }
-    const int ci = I, cj = J, ck = K;
-    fc.half(scol(ci, cj, ck))[soff(C, ci, cj, ck)] = geom ? s / vol : s * (T(1) / vol);
+    const unsigned K = t / (ncx * ncy);
+    const unsigned rem = t - K * ncx * ncy;
+    const unsigned J = rem / ncx;
+    const unsigned I = rem - J * ncx;
+    T s, vol;
+    resid_restrict_part<T, Op>(F, op, u, f, C, geom, (int)I, (int)J, (int)K, 0, 1, s, vol);
+    fc.half(scol(I, J, K))[soff(C, I, J, K)] = geom ? s / vol : s * (T(1) / vol);
 }
 
 template <class T, class Op>
@@ -502,6 +465,117 @@ __global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> 
                                                         Split<T> fc, int geom)
 {
     resid_restrict_body<T, Op>(F, op, u, f, C, fc, geom, blockIdx.x * TPB + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------
+// fused residual + restriction in two launches.  Bulk: the coarse cells
+// whose 2x2x2 children are regular cells away from odd periodic seams (a
+// box).  After a black pass the black residual vanishes there, and the red
+// child of coarse cell I in fine row (j,k) sits at split offset I of that
+// row's red half, so one thread takes W consecutive coarse cells of one
+// coarse row: the red residuals of the four fine rows (2J+dj, 2K+dk) with the
+// vector row evaluation, summed and scaled by 1/8 (equal children).  No
+// residual is stored.  Shell: every other coarse cell, with the general body
+// (all children, residual evaluated on the fly).
+// ---------------------------------------------------------------------
+struct Box {
+    int lo[3], hi[3];
+};
+
+template <class T, int W>
+__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
+                                                                                 const T* __restrict__ fred, Lev C,
+                                                                                 Split<T> fc, FastDiv divG, Box bx)
+{
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned R = divG.div(t);  // coarse row J + Cny K
+    if (R >= C.rows) return;
+    const int K = (int)C.divNy.div(R);
+    const int J = (int)R - K * C.ny;
+    if (J < bx.lo[1] || J > bx.hi[1] || K < bx.lo[2] || K > bx.hi[2]) return;
+    const int h0 = W * (int)(t - R * (unsigned)(F.P / W));
+    if (h0 > bx.hi[0] || h0 + W - 1 < bx.lo[0]) return;
+    VecW<T, W> s = zerov<T, W>();
+#pragma unroll
+    for (int dk = 0; dk < 2; dk++)
+#pragma unroll
+        for (int dj = 0; dj < 2; dj++) {
+            const int j = 2 * J + dj, k = 2 * K + dk;
+            const int row = j + F.ny * k;
+            const int q = (j + k) & 1;
+            const int o0 = h0 + F.P * row;
+            VecW<T, W> diag, off;
+            if (F.uniform) group_rows<T, W, CSplit<T>, true>(F, op, 0, u, row, j, k, h0, q, o0, diag, off);
+            else group_rows<T, W, CSplit<T>, false>(F, op, 0, u, row, j, k, h0, q, o0, diag, off);
+            const VecW<T, W> f4 = ldv<T, W>(fred + o0);
+            const VecW<T, W> u4 = ldv<T, W>(u.c[0] + o0);
+#pragma unroll
+            for (int e = 0; e < W; e++) s.v[e] += f4.v[e] - (diag.v[e] * u4.v[e] + off.v[e]);
+        }
+    const long long cb = (long long)C.P * (J + (long long)C.ny * K);
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int I = h0 + e;
+        if (I >= bx.lo[0] && I <= bx.hi[0]) fc.half((I + J + K) & 1)[(I >> 1) + cb] = s.v[e] * T(0.125);
+    }
+}
+
+// the t-th cell of an n[0] x n[1] x n[2] grid outside box b: z slabs first,
+// then y slabs of the remaining planes, then the x ends of the remaining rows
+__device__ __forceinline__ void shell_cell(long long t, const int n[3], const Box& b, int& I, int& J, int& K)
+{
+    const long long nx = n[0], ny = n[1];
+    const long long zin = b.hi[2] - b.lo[2] + 1, yin = b.hi[1] - b.lo[1] + 1;
+    const long long yout = ny - yin, xout = nx - (b.hi[0] - b.lo[0] + 1);
+    const long long s1 = ((long long)n[2] - zin) * ny * nx;
+    if (t < s1) {
+        const long long p = t / (ny * nx), r = t - p * ny * nx;
+        K = (int)(p < b.lo[2] ? p : b.hi[2] + 1 + (p - b.lo[2]));
+        J = (int)(r / nx);
+        I = (int)(r - J * nx);
+        return;
+    }
+    t -= s1;
+    const long long s2 = zin * yout * nx;
+    if (t < s2) {
+        const long long p = t / (yout * nx), r = t - p * yout * nx;
+        K = b.lo[2] + (int)p;
+        const long long q = r / nx;
+        J = (int)(q < b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
+        I = (int)(r - q * nx);
+        return;
+    }
+    t -= s2;
+    const long long p = t / (yin * xout), r = t - p * yin * xout;
+    K = b.lo[2] + (int)p;
+    const long long q = r / xout, m = r - q * xout;
+    J = b.lo[1] + (int)q;
+    I = (int)(m < b.lo[0] ? m : b.hi[0] + 1 + (m - b.lo[0]));
+}
+
+// eight lanes per shell cell, each summing a share of the children
+template <class T, class Op>
+__global__ void __launch_bounds__(TPB) k_resid_restrict_shell(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
+                                                              Split<T> fc, int geom, Box bx, long long count)
+{
+    const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
+    const long long cell = t >> 3;
+    const int part = (int)(t & 7);
+    const bool ok = cell < count;
+    int I = 0, J = 0, K = 0;
+    T s = T(0), vol = T(0);
+    if (ok) {
+        const int n[3] = {C.nx, C.ny, C.nz};
+        shell_cell(cell, n, bx, I, J, K);
+        resid_restrict_part<T, Op>(F, op, u, f, C, geom, I, J, K, part, 8, s, vol);
+    }
+    // every lane of the warp takes part in the shuffles
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o, 8);
+        vol += __shfl_xor_sync(0xffffffffu, vol, o, 8);
+    }
+    if (ok && part == 0) fc.half(scol(I, J, K))[soff(C, I, J, K)] = geom ? s / vol : s * (T(1) / vol);
 }
 
 // coarse ghost rule for the correction (update_boundary_ghostvalues applied
@@ -612,6 +686,180 @@ template <class T>
 __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, int only_col)
 {
     prolong_body<T>(F, u, C, e, X, only_col, blockIdx.x * TPB + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------
+// prolongation + correction on the geometric hierarchy, W cells of one colour
+// per thread along a fine row.  Inside a box of fine indices the bracketing
+// coarse centres are regular (fine 2I: 1/4 e[I-1] + 3/4 e[I]; fine 2I+1:
+// 3/4 e[I] + 1/4 e[I+1]); elsewhere the per-axis tables give the brackets and
+// the coarse ghost rule applies (same numbers as k_prolong_correct).
+// mode 0: black cells of the rows inside the box in (y,z); mode 1: black
+// cells of the other rows; mode 2: red cells on odd periodic seam planes
+// (read by the next red pass), one cell per thread.
+// ---------------------------------------------------------------------
+// the r-th row (j,k) of an ny x nz set outside the rectangle [lo1,hi1] x [lo2,hi2]
+__device__ __forceinline__ void shell_row(long long r, int ny, const Box& b, int& j, int& k)
+{
+    const long long yin = b.hi[1] - b.lo[1] + 1, yout = ny - yin;
+    const long long s1 = ((long long)b.lo[2]) * ny;
+    if (r < s1) { k = (int)(r / ny); j = (int)(r - (long long)k * ny); return; }
+    r -= s1;
+    const long long zin = b.hi[2] - b.lo[2] + 1;
+    const long long s2 = zin * yout;
+    if (r < s2) {
+        k = b.lo[2] + (int)(r / yout);
+        const long long q = r - (long long)(k - b.lo[2]) * yout;
+        j = (int)(q < b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
+        return;
+    }
+    r -= s2;
+    k = b.hi[2] + 1 + (int)(r / ny);
+    j = (int)(r - (long long)(k - b.hi[2] - 1) * ny);
+}
+
+template <class T>
+__device__ __forceinline__ void lin_axis(const Xfer& X, int ax, int i, bool regular, int& a, int& b, T& t)
+{
+    if (regular) {
+        const int I = i >> 1;
+        if (i & 1) { a = I; b = I + 1; t = T(0.25); }
+        else { a = I - 1; b = I; t = T(0.75); }
+    } else {
+        const Lin L = X.tab[ax][i];
+        a = L.j0;
+        b = L.j1;
+        t = (T)L.t;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ T coarse_val(const Lev& C, const CSplit<T>& e, int x, int y, int z)
+{
+    if (x >= 0 && x < C.nx && y >= 0 && y < C.ny && z >= 0 && z < C.nz)
+        return __ldg(&e.half((x + y + z) & 1)[(x >> 1) + (long long)C.P * (y + (long long)C.ny * z)]);
+    return coarse_at(C, e, x, y, z);
+}
+
+template <class T>
+__device__ __forceinline__ T trilinear(const Lev& C, const CSplit<T>& e, int x0, int x1, T tx, int y0, int y1, T ty,
+                                       int z0, int z1, T tz)
+{
+    const T c000 = coarse_val(C, e, x0, y0, z0), c100 = coarse_val(C, e, x1, y0, z0);
+    const T c010 = coarse_val(C, e, x0, y1, z0), c110 = coarse_val(C, e, x1, y1, z0);
+    const T c001 = coarse_val(C, e, x0, y0, z1), c101 = coarse_val(C, e, x1, y0, z1);
+    const T c011 = coarse_val(C, e, x0, y1, z1), c111 = coarse_val(C, e, x1, y1, z1);
+    const T x00 = c000 + tx * (c100 - c000), x10 = c010 + tx * (c110 - c010);
+    const T x01 = c001 + tx * (c101 - c001), x11 = c011 + tx * (c111 - c011);
+    const T y0v = x00 + ty * (x10 - x00), y1v = x01 + ty * (x11 - x01);
+    return y0v + tz * (y1v - y0v);
+}
+
+template <class T, int W>
+__global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, Box bx, int mode,
+                                                   long long count)
+{
+    const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
+    if (t >= count) return;
+    const int G = F.P / W;
+    int j, k, h0, c, nel;
+    if (mode == 0) {
+        const long long r = t / G;
+        h0 = W * (int)(t - r * G);
+        const int yin = bx.hi[1] - bx.lo[1] + 1;
+        k = bx.lo[2] + (int)(r / yin);
+        j = bx.lo[1] + (int)(r - (long long)(k - bx.lo[2]) * yin);
+        c = 1;
+        nel = W;
+    } else if (mode == 1) {
+        const long long r = t / G;
+        h0 = W * (int)(t - r * G);
+        shell_row(r, F.ny, bx, j, k);
+        c = 1;
+        nel = W;
+    } else {
+        // red seam cells: full rows on y/z seam planes, then the two x ends
+        // of every other row (bx.lo/hi[1..2] delimit the rows off the planes)
+        const bool sx = F.per[0] && (F.nx & 1);
+        const int nh = (F.nx + 1) >> 1;
+        const long long rows_in = (long long)(bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
+        const long long rows_out = (long long)F.ny * F.nz - rows_in;
+        int i;
+        if (t < rows_out * nh) {
+            const long long r = t / nh;
+            shell_row(r, F.ny, bx, j, k);
+            i = 2 * (int)(t - r * nh) + ((j + k) & 1);
+        } else {
+            if (!sx) return;
+            const long long t2 = t - rows_out * nh;
+            const long long r = t2 >> 1;
+            const int yin = bx.hi[1] - bx.lo[1] + 1;
+            k = bx.lo[2] + (int)(r / yin);
+            j = bx.lo[1] + (int)(r - (long long)(k - bx.lo[2]) * yin);
+            i = (t2 & 1) ? F.nx - 1 : 0;
+            if (((i + j + k) & 1) != 0) return;  // not red
+        }
+        if (i >= F.nx) return;
+        int x0, x1, y0, y1, z0, z1;
+        T tx, ty, tz;
+        lin_axis<T>(X, 0, i, false, x0, x1, tx);
+        lin_axis<T>(X, 1, j, false, y0, y1, ty);
+        lin_axis<T>(X, 2, k, false, z0, z1, tz);
+        T* p = &u.c[0][(i >> 1) + (long long)F.P * (j + (long long)F.ny * k)];
+        *p = *p + trilinear<T>(C, e, x0, x1, tx, y0, y1, ty, z0, z1, tz);
+        return;
+    }
+    (void)nel;
+    const int q = (j + k + c) & 1;
+    const long long o0 = h0 + (long long)F.P * (j + (long long)F.ny * k);
+    const bool yreg = mode == 0, zreg = mode == 0;
+    int y0, y1, z0, z1;
+    T ty, tz;
+    lin_axis<T>(X, 1, j, yreg, y0, y1, ty);
+    lin_axis<T>(X, 2, k, zreg, z0, z1, tz);
+    T* base = u.half(c) + o0;
+    if (mode == 0 && 2 * h0 + q >= bx.lo[0] && 2 * (h0 + W - 1) + q <= bx.hi[0]) {
+        // all W cells regular: coarse x = X0 .. X0+W of four coarse rows,
+        // shared by the W cells (same lerp order as trilinear())
+        const T tx = q ? T(0.25) : T(0.75);
+        const int X0 = h0 - 1 + q;
+        VecW<T, W> xi[2][2];
+#pragma unroll
+        for (int zz = 0; zz < 2; zz++)
+#pragma unroll
+            for (int yy = 0; yy < 2; yy++) {
+                const int y = yy ? y1 : y0, z = zz ? z1 : z0;
+                const int rb = C.P * (y + C.ny * z);
+                const int par = (y + z) & 1;
+                T cv[W + 1];
+#pragma unroll
+                for (int m = 0; m <= W; m++) {
+                    const int x = X0 + m;
+                    cv[m] = __ldg(&e.half((x + par) & 1)[(x >> 1) + rb]);
+                }
+#pragma unroll
+                for (int el = 0; el < W; el++) xi[yy][zz].v[el] = cv[el] + tx * (cv[el + 1] - cv[el]);
+            }
+        VecW<T, W> u4 = ldv<T, W>(base);
+#pragma unroll
+        for (int el = 0; el < W; el++) {
+            const T a0 = xi[0][0].v[el] + ty * (xi[1][0].v[el] - xi[0][0].v[el]);
+            const T a1 = xi[0][1].v[el] + ty * (xi[1][1].v[el] - xi[0][1].v[el]);
+            u4.v[el] += a0 + tz * (a1 - a0);
+        }
+        stv<T, W>(base, u4);
+        return;
+    }
+#pragma unroll
+    for (int el = 0; el < W; el++) {
+        const int i = 2 * (h0 + el) + q;
+        if (i >= F.nx) continue;
+        const bool xreg = i >= bx.lo[0] && i <= bx.hi[0];
+        int x0, x1;
+        T tx;
+        lin_axis<T>(X, 0, i, xreg, x0, x1, tx);
+        base[el] = base[el] + trilinear<T>(C, e, x0, x1, tx, y0, y1, ty, z0, z1, tz);
+    }
 }
 
 // ---------------------------------------------------------------------

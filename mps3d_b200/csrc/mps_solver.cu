@@ -467,7 +467,42 @@ static bool odd_periodic(const Lev& L)
     return (L.per[0] && (L.nx & 1)) || (L.per[1] && (L.ny & 1)) || (L.per[2] && (L.nz & 1));
 }
 
-// ---- one colour pass ----
+// ---- transfer boxes ----
+// coarse cells whose 2x2x2 children are regular cells of uniform coefficients
+// away from odd periodic seams (false when an axis does not halve)
+static bool restrict_box(const Lev& F, const Lev& C, Box& b)
+{
+    const int nf[3] = {F.nx, F.ny, F.nz}, nc[3] = {C.nx, C.ny, C.nz};
+    for (int a = 0; a < 3; a++) {
+        if (nf[a] != 2 * nc[a] && nf[a] != 2 * nc[a] + 1) return false;
+        const bool seam = F.per[a] && (nf[a] & 1);
+        const bool irregular_end = nf[a] != 2 * nc[a] || !F.uniform;  // unequal children
+        b.lo[a] = seam ? 1 : 0;
+        b.hi[a] = nc[a] - 1 - ((irregular_end || seam) ? 1 : 0);
+        if (b.hi[a] < b.lo[a]) return false;
+    }
+    return true;
+}
+// fine cells whose bracketing coarse centres are regular cells (geometric hierarchy)
+static bool prolong_box(const Lev& F, const Lev& C, const Xfer& X, Box& b)
+{
+    if (!X.geom) return false;
+    const int nf[3] = {F.nx, F.ny, F.nz}, nc[3] = {C.nx, C.ny, C.nz};
+    for (int a = 0; a < 3; a++) {
+        if (nf[a] != 2 * nc[a] && nf[a] != 2 * nc[a] + 1) return false;
+        const int creg = nc[a] - ((nf[a] != 2 * nc[a] || !F.uniform) ? 1 : 0);
+        b.lo[a] = 1;
+        b.hi[a] = 2 * creg - 3;
+        if (b.hi[a] < b.lo[a]) return false;
+    }
+    return true;
+}
+static long long box_cells(const Box& b)
+{
+    return (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
+}
+
+// ---- one colour pass ----// ---- one colour pass ----
 template <class T, class Op>
 static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zero_state)
 {
@@ -479,8 +514,9 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     else out = H.U[l][H.bi[l] ^ 1] + L.half;
     if (l == 0) prof_begin(ctx, MPS_PROF_SMOOTH);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
-        if (L.uniform) {
-            // vector kernel: 4 cells per thread in FP32, 2 in FP64
+        if (L.uniform || L.nx >= 16) {
+            // vector kernel: 4 cells per thread in FP32, 2 in FP64 (a merged
+            // last cell is evaluated by the general rows inside the kernel)
             constexpr int W = sizeof(T) == 4 ? 4 : 2;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
@@ -549,56 +585,84 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     if (l == 0) prof_begin(ctx, MPS_PROF_RESTRICT);
     bool done = false;
     if constexpr (std::is_same<Op, KOp<T>>::value) {
-        if (L.uniform) {
-            // residual of the red colour (vector kernel) + restriction; after a
-            // black pass the black residual vanishes except across odd periodic seams
+        Box bx;
+        if (o->nu1 >= 1 && L.nx >= 16 && restrict_box(L, C, bx)) {
+            // red residual of the bulk's children restricted in registers, the
+            // shell with the general body
             constexpr int W = sizeof(T) == 4 ? 4 : 2;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
-            const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
-            RedBuf none;
-            none.partial = nullptr;
-            none.counter = nullptr;
-            none.out = nullptr;
-            // nu1 == 0: both colours in full; odd periodic seams: the black
-            // residual only on the seam planes (elsewhere it vanishes)
-            const bool both = o->nu1 == 0;
-            const bool seams = !both && odd_periodic(L);
-            const unsigned nbg = std::min<unsigned>(nbv, 148 * 8);
-            for (int c = 0; c < ((both || seams) ? 2 : 1); c++) {
-                k_residv<T, W, T><<<c == 1 && seams ? nbg : nbv, TPB, 0, ctx.s>>>(
-                    L, ops[l], c, ccur(H, L, l), H.F[l] + (c ? L.half : 0), H.R[l] + (c ? L.half : 0), none, 0, dg,
-                    (c == 1 && seams) ? 1 : 0);
+            const long long nt = (long long)C.rows * (L.P / W);
+            k_resid_restrict_v<T, W><<<nblk(nt), TPB, 0, ctx.s>>>(L, ops[l], ccur(H, L, l), H.F[l], C,
+                                                                  split<T>(H.F[l + 1], C), dg, bx);
+            CKL();
+            const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
+            if (shell > 0) {
+                k_resid_restrict_shell<T, Op><<<nblk(8 * shell), TPB, 0, ctx.s>>>(
+                    L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, bx,
+                    shell);
                 CKL();
             }
-            k_restrict_res<T><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
-                L, csplit<T>(H.R[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, both ? 0 : 1);
             done = true;
         }
     }
-    if (!done)
+    if (!done) {
         k_resid_restrict<T, Op><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
             L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom);
+        CKL();
+    }
     if (l == 0) prof_end(ctx);
-    CKL();
     if ((st = vcycle_rec(ctx, H, ops, l + 1, o, true))) return st;
     if (l == 0) prof_begin(ctx, MPS_PROF_PROLONG);
     // the first post-smoothing pass overwrites the red cells from the black
     // ones, so only black cells need the correction (unless an odd periodic
     // seam makes red cells read red neighbours)
-    if (o->nu2 >= 1) {
+    Box pb;
+    if (o->nu2 >= 1 && L.nx >= 16 && prolong_box(L, C, ctx.xf[l], pb)) {
+        constexpr int W = 4;
+        const long long G = L.P / W;
+        const long long rall = (long long)L.ny * L.nz;
+        const long long rin = (long long)(pb.hi[1] - pb.lo[1] + 1) * (pb.hi[2] - pb.lo[2] + 1);
+        k_prolong_v<T, W><<<nblk(rin * G), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l], pb, 0,
+                                                              rin * G);
+        CKL();
+        if (rall > rin) {
+            k_prolong_v<T, W><<<nblk((rall - rin) * G), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1),
+                                                                          ctx.xf[l], pb, 1, (rall - rin) * G);
+            CKL();
+        }
+        if (odd_periodic(L)) {  // red cells on the seams are read by the next red pass
+            Box sb;
+            const int sy = L.per[1] && (L.ny & 1), sz = L.per[2] && (L.nz & 1), sx = L.per[0] && (L.nx & 1);
+            sb.lo[0] = 0;
+            sb.hi[0] = L.nx - 1;
+            sb.lo[1] = sy;
+            sb.hi[1] = L.ny - 1 - sy;
+            sb.lo[2] = sz;
+            sb.hi[2] = L.nz - 1 - sz;
+            const long long rin2 = (long long)(sb.hi[1] - sb.lo[1] + 1) * (sb.hi[2] - sb.lo[2] + 1);
+            const long long cnt = (rall - rin2) * ((L.nx + 1) / 2) + (sx ? 2 * rin2 : 0);
+            if (cnt > 0) {
+                k_prolong_v<T, W><<<nblk(cnt), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
+                                                                 sb, 2, cnt);
+                CKL();
+            }
+        }
+    } else if (o->nu2 >= 1) {
         k_prolong_correct<T><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, cur(H, L, l), C,
                                                                                ccur(H, C, l + 1), ctx.xf[l], 1);
-        if (odd_periodic(L)) {  // red cells on the seams are read by the next red pass
-            CKL();
+        CKL();
+        if (odd_periodic(L)) {
             k_prolong_correct<T><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, cur(H, L, l), C,
                                                                                    ccur(H, C, l + 1), ctx.xf[l], 2);
+            CKL();
         }
-    } else
+    } else {
         k_prolong_correct<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
             L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l], -1);
+        CKL();
+    }
     if (l == 0) prof_end(ctx);
-    CKL();
     for (int s = 0; s < o->nu2; s++) {
         if ((st = colour_pass(ctx, H, ops[l], l, 0, 0))) return st;
         if ((st = colour_pass(ctx, H, ops[l], l, 1, 0))) return st;
@@ -625,11 +689,10 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
             const unsigned nbv = std::min<unsigned>(nblk((long long)(L.P / W) * L.rows), 148 * 8);
-            for (int c = 0; c < 2; c++) {
-                k_residv<T, W, R><<<nbv, TPB, 0, ctx.s>>>(L, op, c, u, f.half(c), rout.c[0] ? rout.half(c) : nullptr,
-                                                           ctx.rb, c, dg, 0);
-                CKL();
-            }
+            // both colours in one pass (f and rout as split bases, halves L.half apart)
+            k_residv<T, W, R><<<nbv, TPB, 0, ctx.s>>>(L, op, -1, u, f.half(0), rout.c[0] ? rout.half(0) : nullptr,
+                                                       ctx.rb, 0, dg);
+            CKL();
             prof_end(ctx);
             return 0;
         }
