@@ -522,44 +522,45 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_resid_restrict_
 
 // the t-th cell of an n[0] x n[1] x n[2] grid outside box b: z slabs first,
 // then y slabs of the remaining planes, then the x ends of the remaining rows
-__device__ __forceinline__ void shell_cell(long long t, const int n[3], const Box& b, int& I, int& J, int& K)
+__device__ __forceinline__ void shell_cell(unsigned t, const int n[3], const Box& b, int& I, int& J, int& K)
 {
-    const long long nx = n[0], ny = n[1];
-    const long long zin = b.hi[2] - b.lo[2] + 1, yin = b.hi[1] - b.lo[1] + 1;
-    const long long yout = ny - yin, xout = nx - (b.hi[0] - b.lo[0] + 1);
-    const long long s1 = ((long long)n[2] - zin) * ny * nx;
+    const unsigned nx = n[0], ny = n[1];
+    const unsigned zin = b.hi[2] - b.lo[2] + 1, yin = b.hi[1] - b.lo[1] + 1;
+    const unsigned yout = ny - yin, xout = nx - (b.hi[0] - b.lo[0] + 1);
+    const unsigned plane = ny * nx;
+    const unsigned s1 = ((unsigned)n[2] - zin) * plane;
     if (t < s1) {
-        const long long p = t / (ny * nx), r = t - p * ny * nx;
-        K = (int)(p < b.lo[2] ? p : b.hi[2] + 1 + (p - b.lo[2]));
+        const unsigned p = t / plane, r = t - p * plane;
+        K = (int)(p < (unsigned)b.lo[2] ? p : b.hi[2] + 1 + (p - b.lo[2]));
         J = (int)(r / nx);
-        I = (int)(r - J * nx);
+        I = (int)(r - (unsigned)J * nx);
         return;
     }
     t -= s1;
-    const long long s2 = zin * yout * nx;
+    const unsigned s2 = zin * yout * nx;
     if (t < s2) {
-        const long long p = t / (yout * nx), r = t - p * yout * nx;
+        const unsigned p = t / (yout * nx), r = t - p * yout * nx;
         K = b.lo[2] + (int)p;
-        const long long q = r / nx;
-        J = (int)(q < b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
+        const unsigned q = r / nx;
+        J = (int)(q < (unsigned)b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
         I = (int)(r - q * nx);
         return;
     }
     t -= s2;
-    const long long p = t / (yin * xout), r = t - p * yin * xout;
+    const unsigned p = t / (yin * xout), r = t - p * yin * xout;
     K = b.lo[2] + (int)p;
-    const long long q = r / xout, m = r - q * xout;
+    const unsigned q = r / xout, m = r - q * xout;
     J = b.lo[1] + (int)q;
-    I = (int)(m < b.lo[0] ? m : b.hi[0] + 1 + (m - b.lo[0]));
+    I = (int)(m < (unsigned)b.lo[0] ? m : b.hi[0] + 1 + (m - b.lo[0]));
 }
 
 // eight lanes per shell cell, each summing a share of the children
 template <class T, class Op>
 __global__ void __launch_bounds__(TPB) k_resid_restrict_shell(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
-                                                              Split<T> fc, int geom, Box bx, long long count)
+                                                              Split<T> fc, int geom, Box bx, unsigned count)
 {
-    const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
-    const long long cell = t >> 3;
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned cell = t >> 3;
     const int part = (int)(t & 7);
     const bool ok = cell < count;
     int I = 0, J = 0, K = 0;
@@ -694,28 +695,32 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
 // coarse centres are regular (fine 2I: 1/4 e[I-1] + 3/4 e[I]; fine 2I+1:
 // 3/4 e[I] + 1/4 e[I+1]); elsewhere the per-axis tables give the brackets and
 // the coarse ghost rule applies (same numbers as k_prolong_correct).
-// mode 0: black cells of the rows inside the box in (y,z); mode 1: black
-// cells of the other rows; mode 2: red cells on odd periodic seam planes
-// (read by the next red pass), one cell per thread.
+// mode 0: black cells of the groups whose cells all lie inside the box;
+// mode 3: the other groups of the rows inside the box in (y,z); mode 1:
+// black cells of the other rows; mode 2: red cells on odd periodic seam
+// planes (read by the next red pass), one cell per thread.
 // ---------------------------------------------------------------------
 // the r-th row (j,k) of an ny x nz set outside the rectangle [lo1,hi1] x [lo2,hi2]
-__device__ __forceinline__ void shell_row(long long r, int ny, const Box& b, int& j, int& k)
+__device__ __forceinline__ void shell_row(unsigned r, int ny, const Box& b, int& j, int& k)
 {
-    const long long yin = b.hi[1] - b.lo[1] + 1, yout = ny - yin;
-    const long long s1 = ((long long)b.lo[2]) * ny;
-    if (r < s1) { k = (int)(r / ny); j = (int)(r - (long long)k * ny); return; }
+    const unsigned uny = (unsigned)ny;
+    const unsigned yin = (unsigned)(b.hi[1] - b.lo[1] + 1), yout = uny - yin;
+    const unsigned s1 = (unsigned)b.lo[2] * uny;
+    if (r < s1) { k = (int)(r / uny); j = (int)(r - (unsigned)k * uny); return; }
     r -= s1;
-    const long long zin = b.hi[2] - b.lo[2] + 1;
-    const long long s2 = zin * yout;
+    const unsigned zin = (unsigned)(b.hi[2] - b.lo[2] + 1);
+    const unsigned s2 = zin * yout;
     if (r < s2) {
-        k = b.lo[2] + (int)(r / yout);
-        const long long q = r - (long long)(k - b.lo[2]) * yout;
-        j = (int)(q < b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
+        const unsigned kk = r / yout;
+        k = b.lo[2] + (int)kk;
+        const unsigned q = r - kk * yout;
+        j = (int)(q < (unsigned)b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
         return;
     }
     r -= s2;
-    k = b.hi[2] + 1 + (int)(r / ny);
-    j = (int)(r - (long long)(k - b.hi[2] - 1) * ny);
+    const unsigned kk = r / uny;
+    k = b.hi[2] + 1 + (int)kk;
+    j = (int)(r - kk * uny);
 }
 
 template <class T>
@@ -755,25 +760,44 @@ __device__ __forceinline__ T trilinear(const Lev& C, const CSplit<T>& e, int x0,
     return y0v + tz * (y1v - y0v);
 }
 
+// divisors of the thread decode (32-bit multiply-high division)
+struct ProlongDiv {
+    FastDiv g;    // by the groups per row, P / W
+    FastDiv yin;  // by the rows of the box along y
+    FastDiv nh;   // by the cells of one colour per row, (nx+1)/2
+    FastDiv gin;  // by the groups whose cells all lie in the box along x
+    FastDiv gout; // by the other groups of a row
+    int g_lo, g_hi;  // the groups in the box: [g_lo, g_hi]
+};
+
 template <class T, int W>
 __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, Box bx, int mode,
-                                                   long long count)
+                                                   unsigned count, ProlongDiv dv)
 {
-    const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
     if (t >= count) return;
-    const int G = F.P / W;
     int j, k, h0, c, nel;
-    if (mode == 0) {
-        const long long r = t / G;
-        h0 = W * (int)(t - r * G);
-        const int yin = bx.hi[1] - bx.lo[1] + 1;
-        k = bx.lo[2] + (int)(r / yin);
-        j = bx.lo[1] + (int)(r - (long long)(k - bx.lo[2]) * yin);
+    if (mode == 0 || mode == 3) {
+        // rows inside the box; mode 0: the groups inside along x (every cell
+        // regular, no divergent path in the warp), mode 3: the row ends
+        unsigned r, g;
+        if (mode == 0) {
+            r = dv.gin.div(t);
+            g = dv.g_lo + (t - r * dv.gin.d);
+        } else {
+            r = dv.gout.div(t);
+            const unsigned e = t - r * dv.gout.d;
+            g = e < (unsigned)dv.g_lo ? e : dv.g_hi + 1 + (e - dv.g_lo);
+        }
+        h0 = W * (int)g;
+        const unsigned kk = dv.yin.div(r);
+        k = bx.lo[2] + (int)kk;
+        j = bx.lo[1] + (int)(r - kk * dv.yin.d);
         c = 1;
         nel = W;
     } else if (mode == 1) {
-        const long long r = t / G;
-        h0 = W * (int)(t - r * G);
+        const unsigned r = dv.g.div(t);
+        h0 = W * (int)(t - r * dv.g.d);
         shell_row(r, F.ny, bx, j, k);
         c = 1;
         nel = W;
@@ -781,21 +805,20 @@ __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSp
         // red seam cells: full rows on y/z seam planes, then the two x ends
         // of every other row (bx.lo/hi[1..2] delimit the rows off the planes)
         const bool sx = F.per[0] && (F.nx & 1);
-        const int nh = (F.nx + 1) >> 1;
-        const long long rows_in = (long long)(bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
-        const long long rows_out = (long long)F.ny * F.nz - rows_in;
+        const unsigned rows_in = (unsigned)(bx.hi[1] - bx.lo[1] + 1) * (unsigned)(bx.hi[2] - bx.lo[2] + 1);
+        const unsigned rows_out = (unsigned)F.ny * (unsigned)F.nz - rows_in;
         int i;
-        if (t < rows_out * nh) {
-            const long long r = t / nh;
+        if (t < rows_out * dv.nh.d) {
+            const unsigned r = dv.nh.div(t);
             shell_row(r, F.ny, bx, j, k);
-            i = 2 * (int)(t - r * nh) + ((j + k) & 1);
+            i = 2 * (int)(t - r * dv.nh.d) + ((j + k) & 1);
         } else {
             if (!sx) return;
-            const long long t2 = t - rows_out * nh;
-            const long long r = t2 >> 1;
-            const int yin = bx.hi[1] - bx.lo[1] + 1;
-            k = bx.lo[2] + (int)(r / yin);
-            j = bx.lo[1] + (int)(r - (long long)(k - bx.lo[2]) * yin);
+            const unsigned t2 = t - rows_out * dv.nh.d;
+            const unsigned r = t2 >> 1;
+            const unsigned kk = dv.yin.div(r);
+            k = bx.lo[2] + (int)kk;
+            j = bx.lo[1] + (int)(r - kk * dv.yin.d);
             i = (t2 & 1) ? F.nx - 1 : 0;
             if (((i + j + k) & 1) != 0) return;  // not red
         }
@@ -812,13 +835,13 @@ __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSp
     (void)nel;
     const int q = (j + k + c) & 1;
     const long long o0 = h0 + (long long)F.P * (j + (long long)F.ny * k);
-    const bool yreg = mode == 0, zreg = mode == 0;
+    const bool yreg = mode != 1, zreg = mode != 1;
     int y0, y1, z0, z1;
     T ty, tz;
     lin_axis<T>(X, 1, j, yreg, y0, y1, ty);
     lin_axis<T>(X, 2, k, zreg, z0, z1, tz);
     T* base = u.half(c) + o0;
-    if (mode == 0 && 2 * h0 + q >= bx.lo[0] && 2 * (h0 + W - 1) + q <= bx.hi[0]) {
+    if (mode == 0) {
         // all W cells regular: coarse x = X0 .. X0+W of four coarse rows,
         // shared by the W cells (same lerp order as trilinear())
         const T tx = q ? T(0.25) : T(0.75);

@@ -600,7 +600,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             if (shell > 0) {
                 k_resid_restrict_shell<T, Op><<<nblk(8 * shell), TPB, 0, ctx.s>>>(
                     L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, bx,
-                    shell);
+                    (unsigned)shell);
                 CKL();
             }
             done = true;
@@ -623,12 +623,33 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         const long long G = L.P / W;
         const long long rall = (long long)L.ny * L.nz;
         const long long rin = (long long)(pb.hi[1] - pb.lo[1] + 1) * (pb.hi[2] - pb.lo[2] + 1);
-        k_prolong_v<T, W><<<nblk(rin * G), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l], pb, 0,
-                                                              rin * G);
-        CKL();
+        ProlongDiv dv;
+        dv.g.init((unsigned)G);
+        dv.yin.init((unsigned)(pb.hi[1] - pb.lo[1] + 1));
+        dv.nh.init((unsigned)((L.nx + 1) / 2));
+        // groups with every cell in the box for both row parities: 2Wg >= lo,
+        // 2W(g+1) - 1 <= hi
+        dv.g_lo = (pb.lo[0] + 2 * W - 1) / (2 * W);
+        dv.g_hi = (pb.hi[0] + 1) / (2 * W) - 1;
+        const long long gin = dv.g_hi >= dv.g_lo ? dv.g_hi - dv.g_lo + 1 : 0;
+        if (gin == 0) { dv.g_lo = 0; dv.g_hi = -1; }
+        dv.gin.init((unsigned)std::max<long long>(gin, 1));
+        dv.gout.init((unsigned)std::max<long long>(G - gin, 1));
+        if (gin > 0) {
+            k_prolong_v<T, W><<<nblk(rin * gin), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
+                                                                   pb, 0, (unsigned)(rin * gin), dv);
+            CKL();
+        }
+        if (G > gin) {
+            k_prolong_v<T, W><<<nblk(rin * (G - gin)), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1),
+                                                                         ctx.xf[l], pb, 3,
+                                                                         (unsigned)(rin * (G - gin)), dv);
+            CKL();
+        }
         if (rall > rin) {
             k_prolong_v<T, W><<<nblk((rall - rin) * G), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1),
-                                                                          ctx.xf[l], pb, 1, (rall - rin) * G);
+                                                                          ctx.xf[l], pb, 1, (unsigned)((rall - rin) * G),
+                                                                          dv);
             CKL();
         }
         if (odd_periodic(L)) {  // red cells on the seams are read by the next red pass
@@ -643,8 +664,10 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             const long long rin2 = (long long)(sb.hi[1] - sb.lo[1] + 1) * (sb.hi[2] - sb.lo[2] + 1);
             const long long cnt = (rall - rin2) * ((L.nx + 1) / 2) + (sx ? 2 * rin2 : 0);
             if (cnt > 0) {
+                ProlongDiv sv = dv;
+                sv.yin.init((unsigned)(sb.hi[1] - sb.lo[1] + 1));
                 k_prolong_v<T, W><<<nblk(cnt), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
-                                                                 sb, 2, cnt);
+                                                                 sb, 2, (unsigned)cnt, sv);
                 CKL();
             }
         }
