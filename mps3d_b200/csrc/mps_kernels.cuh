@@ -88,11 +88,25 @@ template <class T, int W>
 struct VecW {
     T v[W];
 };
+// 256-bit global accesses (sm_100): one instruction for 8 floats or 4
+// doubles; the address must be 32-byte aligned (groups start at multiples of
+// W elements of rows whose pitch P is a multiple of 8)
 template <class T, int W>
 __device__ __forceinline__ VecW<T, W> ldv(const T* p)
 {
     VecW<T, W> r;
-    if constexpr (sizeof(T) * W == 16) {
+    if constexpr (sizeof(T) * W == 32) {
+        if constexpr (sizeof(T) == 4) {
+            asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]),
+                  "=f"(r.v[6]), "=f"(r.v[7])
+                : "l"(p));
+        } else {
+            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+                : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3])
+                : "l"(p));
+        }
+    } else if constexpr (sizeof(T) * W == 16) {
         if constexpr (sizeof(T) == 4) {
             const float4 a = __ldg(reinterpret_cast<const float4*>(p));
             r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
@@ -113,7 +127,17 @@ __device__ __forceinline__ VecW<T, W> ldv(const T* p)
 template <class T, int W>
 __device__ __forceinline__ void stv(T* p, const VecW<T, W>& r)
 {
-    if constexpr (sizeof(T) * W == 16) {
+    if constexpr (sizeof(T) * W == 32) {
+        if constexpr (sizeof(T) == 4) {
+            asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(r.v[0]), "f"(r.v[1]),
+                         "f"(r.v[2]), "f"(r.v[3]), "f"(r.v[4]), "f"(r.v[5]), "f"(r.v[6]), "f"(r.v[7])
+                         : "memory");
+        } else {
+            asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(r.v[0]), "d"(r.v[1]), "d"(r.v[2]),
+                         "d"(r.v[3])
+                         : "memory");
+        }
+    } else if constexpr (sizeof(T) * W == 16) {
         if constexpr (sizeof(T) == 4) *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
         else *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
     } else if constexpr (sizeof(T) * W == 8) {
@@ -313,8 +337,30 @@ __device__ __forceinline__ bool group_decode(const Lev& L, const FastDiv& divG, 
 
 // colour pass, W cells of colour c per thread (vector loads).  Elements past
 // the end of the row (pads) are written as 0.  Same results as k_colour.
+// cells per thread and minimum resident blocks of the vector stencil kernels
+// (colour pass, residual, fused residual + restriction); measured on the
+// 257^3 plasma Poisson solve: 8 FP32 / 4 FP64 cells per thread (one 256-bit
+// access per field and row) with 3 blocks of 256 threads per SM
+#ifndef MPS_COLOUR_W32
+#define MPS_COLOUR_W32 8
+#endif
+#ifndef MPS_COLOUR_W64
+#define MPS_COLOUR_W64 4
+#endif
+#ifndef MPS_COLOUR_MINB32
+#define MPS_COLOUR_MINB32 3
+#endif
+#ifndef MPS_COLOUR_MINB64
+#define MPS_COLOUR_MINB64 3
+#endif
+template <class T>
+struct ColourShape {
+    static constexpr int W = sizeof(T) == 4 ? MPS_COLOUR_W32 : MPS_COLOUR_W64;
+    static constexpr int MINB = sizeof(T) == 4 ? MPS_COLOUR_MINB32 : MPS_COLOUR_MINB64;
+};
+
 template <class T, int W, class U>
-__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
+__global__ void __launch_bounds__(TPB, ColourShape<T>::MINB) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
                                                     const T* __restrict__ f, FastDiv divG)
 {
     GroupIdx G;
@@ -337,7 +383,7 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_colourv(Lev L, 
 // r^2 and f^2 reduced deterministically (accumulate = add to rb.out, for the
 // second colour)
 template <class T, int W, class R>
-__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_residv(Lev L, KOp<T> op, int c, CSplit<T> u,
+__global__ void __launch_bounds__(TPB, ColourShape<T>::MINB) k_residv(Lev L, KOp<T> op, int c, CSplit<T> u,
                                                                        const T* __restrict__ f, R* __restrict__ rout,
                                                                        RedBuf rb, int accumulate, FastDiv divG)
 {
@@ -482,8 +528,16 @@ struct Box {
     int lo[3], hi[3];
 };
 
+// the fused residual + restriction keeps 4 cells per thread (its thread
+// holds the sums of four fine rows; 8 FP32 cells spill)
+template <class T>
+struct RestrictShape {
+    static constexpr int W = 4;
+    static constexpr int MINB = sizeof(T) == 4 ? 4 : 3;
+};
+
 template <class T, int W>
-__global__ void __launch_bounds__(TPB, sizeof(T) == 4 ? 4 : 3) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
+__global__ void __launch_bounds__(TPB, RestrictShape<T>::MINB) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
                                                                                  const T* __restrict__ fred, Lev C,
                                                                                  Split<T> fc, FastDiv divG, Box bx)
 {

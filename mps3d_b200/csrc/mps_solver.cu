@@ -515,9 +515,9 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     if (l == 0) prof_begin(ctx, MPS_PROF_SMOOTH);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (L.uniform || L.nx >= 16) {
-            // vector kernel: 4 cells per thread in FP32, 2 in FP64 (a merged
-            // last cell is evaluated by the general rows inside the kernel)
-            constexpr int W = sizeof(T) == 4 ? 4 : 2;
+            // vector kernel, W cells per thread (faces at a merged last cell
+            // take their own coefficients inside the row evaluation)
+            constexpr int W = ColourShape<T>::W;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
             const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
@@ -589,7 +589,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         if (o->nu1 >= 1 && L.nx >= 16 && restrict_box(L, C, bx)) {
             // red residual of the bulk's children restricted in registers, the
             // shell with the general body
-            constexpr int W = sizeof(T) == 4 ? 4 : 2;
+            constexpr int W = RestrictShape<T>::W;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
             const long long nt = (long long)C.rows * (L.P / W);
@@ -708,7 +708,7 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
     prof_begin(ctx, MPS_PROF_RESID);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (L.uniform) {  // vector kernel, one launch per colour, norms accumulated
-            constexpr int W = sizeof(T) == 4 ? 4 : 2;
+            constexpr int W = ColourShape<T>::W;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
             const unsigned nbv = std::min<unsigned>(nblk((long long)(L.P / W) * L.rows), 148 * 8);
