@@ -176,8 +176,10 @@ int mps_find_bvec_dev(mps_handle h, const mps_grid* g, const double* vel, const 
                       const double* mgridsterm, double* b, const mps_solver_opts* opts,
                       void* stream);
 
-/* Profiling of the finest-level kernels (off by default).  mps_get_profile
- * returns the accumulated figures and resets them when reset != 0. */
+/* Profiling of the smoothing and transfer kernels of one level (off by
+ * default): on = 1 times the finest level, on = 1 + l level l; the residual
+ * class is always the finest level's.  mps_get_profile returns the
+ * accumulated figures and resets them when reset != 0. */
 int mps_set_profile(mps_handle h, int on);
 int mps_get_profile(mps_handle h, mps_profile* p, int reset);
 

@@ -178,8 +178,9 @@ class Handle:
     def stream(self) -> int:
         return self._lib.mps_stream(self.h) or 0
 
-    def set_profile(self, on: bool):
-        self._lib.mps_set_profile(self.h, int(bool(on)))
+    def set_profile(self, on):
+        """False: off; True or 1: time the finest level; 1 + l: time level l."""
+        self._lib.mps_set_profile(self.h, int(on))
 
     def get_profile(self, reset=True) -> Profile:
         p = Profile()

@@ -7,6 +7,7 @@ namespace mps {
 // ---------------------------------------------------------------------
 __global__ void k_gj_prepare(int n, const double* A, double* M)
 {
+    pdl_wait();
     const long long n2 = 2LL * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n2;
          t += (long long)gridDim.x * blockDim.x) {
@@ -17,6 +18,7 @@ __global__ void k_gj_prepare(int n, const double* A, double* M)
 
 __global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* Mg, double* AinvT, int* status, int smem)
 {
+    pdl_wait();
     // 32 x 32 threads: lanes stride columns, warps stride rows
     extern __shared__ double Ms[];
     __shared__ double fac[1024];
@@ -89,6 +91,7 @@ __global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* Mg, double
 // ---------------------------------------------------------------------
 __global__ void k_maxabs(Lev L, const double* __restrict__ g, int rel, unsigned long long* out)
 {
+    pdl_wait();
     const unsigned nx = L.nx, ny = L.ny;
     const unsigned total = nx * ny * (unsigned)L.nz;
     const double ref = rel ? g[(long long)1 + (nx + 2) * (1 + (long long)(ny + 2) * 1)] : 0.0;
@@ -114,6 +117,7 @@ __global__ void k_maxabs(Lev L, const double* __restrict__ g, int rel, unsigned 
 __global__ void k_fill_ghosts(Lev L, double* __restrict__ g, const double* bl, const double* br, const double* bb,
                               const double* bt, const double* bk, const double* bf)
 {
+    pdl_wait();
     const int nx = L.nx, ny = L.ny, nz = L.nz;
     const long long sx = 1, sy = nx + 2, sz = (long long)(nx + 2) * (ny + 2);
     auto G = [&](int i, int j, int k) -> double& { return g[i * sx + j * sy + k * sz]; };
@@ -156,6 +160,7 @@ __global__ void k_find_bvec(Lev L, const double* __restrict__ vel, const double*
                             const double* bb, const double* bt, const double* bk, const double* bf,
                             const double* __restrict__ sterm, int flux, Split<double> b)
 {
+    pdl_wait();
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned nx = L.nx, ny = L.ny, nz = L.nz;
     if (t >= nx * ny * nz) return;
@@ -201,6 +206,7 @@ __global__ void k_find_bvec(Lev L, const double* __restrict__ vel, const double*
 
 __global__ void k_restrict_field(Lev F, CSplit<double> in, Lev C, Split<double> out, int geom)
 {
+    pdl_wait();
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned ncx = C.nx, ncy = C.ny;
     if (t >= ncx * ncy * (unsigned)C.nz) return;
@@ -237,6 +243,7 @@ __global__ void k_restrict_field(Lev F, CSplit<double> in, Lev C, Split<double> 
 __global__ void k_multidot(long long n, int m, const double* const* __restrict__ V, const double* __restrict__ w,
                            double* __restrict__ partial)
 {
+    pdl_wait();
     __shared__ double sh[32];
     for (int q = 0; q < m; q++) {
         const double* v = V[q];
@@ -252,6 +259,7 @@ __global__ void k_multidot(long long n, int m, const double* const* __restrict__
 __global__ void k_multidot_finish(int m, int nblocks, const double* __restrict__ partial, double* __restrict__ h,
                                   int accumulate)
 {
+    pdl_wait();
     __shared__ double sh[32];
     const int q = blockIdx.x;
     if (q >= m) return;
@@ -264,6 +272,7 @@ __global__ void k_multidot_finish(int m, int nblocks, const double* __restrict__
 __global__ void k_multiaxpy(long long n, int m, const double* const* __restrict__ V, const double* __restrict__ h,
                             double* __restrict__ w)
 {
+    pdl_wait();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         double s = w[t];
         for (int q = 0; q < m; q++) s -= h[q] * V[q][t];
@@ -274,6 +283,7 @@ __global__ void k_multiaxpy(long long n, int m, const double* const* __restrict_
 __global__ void k_scale_to(long long n, const double* __restrict__ w, const double* __restrict__ hn, int idx,
                            double* __restrict__ v, float* __restrict__ v32)
 {
+    pdl_wait();
     const double inv = 1.0 / hn[idx];
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         double x = w[t] * inv;

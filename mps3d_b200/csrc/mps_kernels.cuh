@@ -9,6 +9,13 @@ namespace mps {
 
 constexpr int TPB = 256;
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialization attribute may be scheduled while its predecessor is
+// still running; this wait (first statement of every kernel) blocks until
+// the predecessor grid has completed and its writes are visible.  For an
+// ordinary launch it returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 struct RedBuf {
     double* partial;      // [2 * maxblocks]
     unsigned* counter;    // zero-initialised
@@ -73,6 +80,7 @@ template <class T, class Op, class U>
 __global__ void __launch_bounds__(TPB) k_colour(Lev L, Op op, int c, U u, T* __restrict__ out,
                                                 const T* __restrict__ f)
 {
+    pdl_wait();
     colour_body<T, Op, U>(L, op, c, u, out, f, blockIdx.x * TPB + threadIdx.x);
 }
 
@@ -363,6 +371,7 @@ template <class T, int W, class U>
 __global__ void __launch_bounds__(TPB, ColourShape<T>::MINB) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
                                                     const T* __restrict__ f, FastDiv divG)
 {
+    pdl_wait();
     GroupIdx G;
     if (!group_decode<W>(L, divG, c, G)) return;
     const VecW<T, W> f4 = ldv<T, W>(f + G.o0);
@@ -387,6 +396,7 @@ __global__ void __launch_bounds__(TPB, ColourShape<T>::MINB) k_residv(Lev L, KOp
                                                                        const T* __restrict__ f, R* __restrict__ rout,
                                                                        RedBuf rb, int accumulate, FastDiv divG)
 {
+    pdl_wait();
     __shared__ double sh[32];
     double rr = 0.0, ff = 0.0;
     const unsigned ngroups = (unsigned)(L.P / W) * L.rows;
@@ -510,6 +520,7 @@ template <class T, class Op>
 __global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
                                                         Split<T> fc, int geom)
 {
+    pdl_wait();
     resid_restrict_body<T, Op>(F, op, u, f, C, fc, geom, blockIdx.x * TPB + threadIdx.x);
 }
 
@@ -541,6 +552,7 @@ __global__ void __launch_bounds__(TPB, RestrictShape<T>::MINB) k_resid_restrict_
                                                                                  const T* __restrict__ fred, Lev C,
                                                                                  Split<T> fc, FastDiv divG, Box bx)
 {
+    pdl_wait();
     const unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned R = divG.div(t);  // coarse row J + Cny K
     if (R >= C.rows) return;
@@ -613,6 +625,7 @@ template <class T, class Op>
 __global__ void __launch_bounds__(TPB) k_resid_restrict_shell(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
                                                               Split<T> fc, int geom, Box bx, unsigned count)
 {
+    pdl_wait();
     const unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned cell = t >> 3;
     const int part = (int)(t & 7);
@@ -740,6 +753,7 @@ __device__ __forceinline__ void prolong_body(const Lev& F, const Split<T>& u, co
 template <class T>
 __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, int only_col)
 {
+    pdl_wait();
     prolong_body<T>(F, u, C, e, X, only_col, blockIdx.x * TPB + threadIdx.x);
 }
 
@@ -828,6 +842,7 @@ template <class T, int W>
 __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, Box bx, int mode,
                                                    unsigned count, ProlongDiv dv)
 {
+    pdl_wait();
     const unsigned t = blockIdx.x * TPB + threadIdx.x;
     if (t >= count) return;
     int j, k, h0, c, nel;
@@ -966,8 +981,137 @@ template <class T>
 __global__ void __launch_bounds__(512) k_coarse_solve(Lev C, const double* __restrict__ AinvT, CSplit<T> f,
                                                       Split<T> u)
 {
+    pdl_wait();
     extern __shared__ double fs[];
     coarse_solve_body<T>(C, AinvT, f, u, fs);
+}
+
+// ---------------------------------------------------------------------
+// the lower part of a V-cycle in one CTA: every level from `first` down to
+// the coarsest has at most SMALL_CELLS cells, where a launch per colour pass
+// costs more than the pass.  The same device bodies as the single-level
+// kernels, over thread-strided indices with a block barrier between phases:
+// pre-smoothing and residual restriction down, the dense coarsest solve,
+// prolongation (all cells) and post-smoothing up.  The buffer parities start
+// from the host's and advance exactly as the host's do.
+// ---------------------------------------------------------------------
+constexpr int SMALL_CELLS = 512;
+constexpr int SMALL_MAXL = 8;
+constexpr int SMALL_TPB = 1024;
+
+template <class T>
+struct SmallLevel {
+    Lev L;
+    KOp<T> op;
+    Xfer X;  // to the next coarser level
+    T* U[2];
+    T* F;
+};
+template <class T>
+struct SmallCycle {
+    int n;  // levels, the last is the coarsest
+    int nu1, nu2;
+    const double* AinvT;
+    SmallLevel<T> lev[SMALL_MAXL];
+};
+
+template <class T>
+__global__ void __launch_bounds__(SMALL_TPB) k_vcycle_small(const SmallCycle<T>* __restrict__ sc, int zero_first,
+                                                            unsigned ri_bits, unsigned bi_bits)
+{
+    pdl_wait();
+    __shared__ double fs[1024];
+    const SmallCycle<T>& S = *sc;
+    const int n = S.n;
+    unsigned ri = ri_bits, bi = bi_bits;  // bit l: parity of level l
+    auto cur = [&](int l) {
+        CSplit<T> u;
+        u.c[0] = S.lev[l].U[(ri >> l) & 1];
+        u.c[1] = S.lev[l].U[(bi >> l) & 1] + S.lev[l].L.half;
+        return u;
+    };
+    auto colour = [&](int l, int c, int zs) {
+        const SmallLevel<T>& Lv = S.lev[l];
+        const Lev& L = Lv.L;
+        const unsigned par = c == 0 ? (ri >> l) & 1 : (bi >> l) & 1;
+        T* out = Lv.U[par ^ 1] + (c ? L.half : 0);
+        const T* fh = Lv.F + (c ? L.half : 0);
+        const unsigned nt = (unsigned)L.P * L.rows;
+        if (zs == 2) {
+            for (unsigned t = threadIdx.x; t < nt; t += blockDim.x)
+                colour_body<T, KOp<T>, ZeroU<T>>(L, Lv.op, c, ZeroU<T>(), out, fh, t);
+        } else if (zs == 1) {
+            OtherOnlyU<T> u;
+            u.c = c;
+            const CSplit<T> cu = cur(l);
+            u.other = c == 0 ? cu.c[1] : cu.c[0];
+            for (unsigned t = threadIdx.x; t < nt; t += blockDim.x)
+                colour_body<T, KOp<T>, OtherOnlyU<T>>(L, Lv.op, c, u, out, fh, t);
+        } else {
+            const CSplit<T> u = cur(l);
+            for (unsigned t = threadIdx.x; t < nt; t += blockDim.x)
+                colour_body<T, KOp<T>, CSplit<T>>(L, Lv.op, c, u, out, fh, t);
+        }
+        if (c == 0) ri ^= 1u << l;
+        else bi ^= 1u << l;
+        __syncthreads();
+    };
+    for (int l = 0; l + 1 < n; l++) {
+        const bool z = l > 0 || zero_first;
+        for (int s2 = 0; s2 < S.nu1; s2++) {
+            colour(l, 0, z && s2 == 0 ? 2 : 0);
+            colour(l, 1, z && s2 == 0 ? 1 : 0);
+        }
+        const SmallLevel<T>& Lv = S.lev[l];
+        const SmallLevel<T>& Cv = S.lev[l + 1];
+        if (S.nu1 == 0 && z) {  // the zero initial guess of this level
+            const CSplit<T> u = cur(l);
+            for (long long t = threadIdx.x; t < Lv.L.half; t += blockDim.x) {
+                const_cast<T*>(u.c[0])[t] = T(0);
+                const_cast<T*>(u.c[1])[t] = T(0);
+            }
+            __syncthreads();
+        }
+        CSplit<T> f;
+        f.c[0] = Lv.F;
+        f.c[1] = Lv.F + Lv.L.half;
+        Split<T> fc;
+        fc.c[0] = Cv.F;
+        fc.c[1] = Cv.F + Cv.L.half;
+        const unsigned nc = (unsigned)Cv.L.nx * Cv.L.ny * Cv.L.nz;
+        const CSplit<T> u = cur(l);
+        for (unsigned t = threadIdx.x; t < nc; t += blockDim.x)
+            resid_restrict_body<T, KOp<T>>(Lv.L, Lv.op, u, f, Cv.L, fc, Lv.X.geom, t);
+        __syncthreads();
+    }
+    {
+        const SmallLevel<T>& Cv = S.lev[n - 1];
+        CSplit<T> f;
+        f.c[0] = Cv.F;
+        f.c[1] = Cv.F + Cv.L.half;
+        const CSplit<T> cu = cur(n - 1);
+        Split<T> u;
+        u.c[0] = const_cast<T*>(cu.c[0]);
+        u.c[1] = const_cast<T*>(cu.c[1]);
+        coarse_solve_body<T>(Cv.L, S.AinvT, f, u, fs);
+        __syncthreads();
+    }
+    for (int l = n - 2; l >= 0; l--) {
+        const SmallLevel<T>& Lv = S.lev[l];
+        const SmallLevel<T>& Cv = S.lev[l + 1];
+        const CSplit<T> cu = cur(l);
+        Split<T> u;
+        u.c[0] = const_cast<T*>(cu.c[0]);
+        u.c[1] = const_cast<T*>(cu.c[1]);
+        const CSplit<T> e = cur(l + 1);
+        const unsigned nf = (unsigned)Lv.L.nx * Lv.L.ny * Lv.L.nz;
+        for (unsigned t = threadIdx.x; t < nf; t += blockDim.x) prolong_body<T>(Lv.L, u, Cv.L, e, Lv.X, -1, t);
+        __syncthreads();
+        for (int s2 = 0; s2 < S.nu2; s2++) {
+            colour(l, 0, 0);
+            colour(l, 1, 0);
+        }
+    }
 }
 
 // dense assembly of the coarsest operator (row major, FP64, pre-zeroed)
@@ -1009,6 +1153,7 @@ __device__ __forceinline__ void dense_row(const ROp<T>& op, const Lev& L, int i,
 template <class T, class Op>
 __global__ void k_dense_assemble(Lev L, Op op, double* A)
 {
+    pdl_wait();
     const int n = L.nx * L.ny * L.nz;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         int i = r % L.nx, j = (r / L.nx) % L.ny, k = r / (L.nx * L.ny);
@@ -1059,6 +1204,7 @@ template <class T, class Op, class R>
 __global__ void __launch_bounds__(TPB) k_resid_norm(Lev L, Op op, CSplit<T> u, CSplit<T> f, Split<R> rout,
                                                     RedBuf rb)
 {
+    pdl_wait();
     __shared__ double sh[32];
     double rr = 0.0, ff = 0.0;
     const unsigned total = (unsigned)L.P * L.rows;
@@ -1084,6 +1230,7 @@ __global__ void __launch_bounds__(TPB) k_resid_norm(Lev L, Op op, CSplit<T> u, C
 template <class T, class Op, class Tu>
 __global__ void __launch_bounds__(TPB) k_apply(Lev L, Op op, CSplit<Tu> u, Split<double> out)
 {
+    pdl_wait();
     const unsigned total = (unsigned)L.P * L.rows;
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     if (t >= total) return;
@@ -1103,6 +1250,7 @@ __global__ void __launch_bounds__(TPB) k_apply(Lev L, Op op, CSplit<Tu> u, Split
 template <class T>
 __global__ void k_pack(Lev L, const double* __restrict__ g, Split<T> out, double scale, double shift)
 {
+    pdl_wait();
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned nx = L.nx, ny = L.ny;
     if (t >= nx * ny * (unsigned)L.nz) return;
@@ -1118,6 +1266,7 @@ __global__ void k_pack(Lev L, const double* __restrict__ g, Split<T> out, double
 template <class T>
 __global__ void k_unpack(Lev L, CSplit<T> in, double* __restrict__ g)
 {
+    pdl_wait();
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned nx = L.nx, ny = L.ny;
     if (t >= nx * ny * (unsigned)L.nz) return;
@@ -1133,6 +1282,7 @@ __global__ void k_unpack(Lev L, CSplit<T> in, double* __restrict__ g)
 template <class T>
 __global__ void k_unpack_nat(Lev L, CSplit<T> in, double* __restrict__ g)
 {
+    pdl_wait();
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned nx = L.nx, ny = L.ny;
     if (t >= nx * ny * (unsigned)L.nz) return;
@@ -1183,6 +1333,7 @@ template <class T>
 __global__ void k_build_rows(Lev L, CSplit<double> vx, CSplit<double> vy, CSplit<double> vz, CSplit<double> kf,
                              CSplit<double> reac, int has_reac, double dtinv, int flux, ROp<T> out_rows)
 {
+    pdl_wait();
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned nx = L.nx, ny = L.ny;
     if (t >= nx * ny * (unsigned)L.nz) return;
@@ -1255,6 +1406,7 @@ __global__ void k_build_rows(Lev L, CSplit<double> vx, CSplit<double> vy, CSplit
 template <class T>
 __global__ void k_transpose_rows(Lev L, ROp<T> in, ROp<T> out)
 {
+    pdl_wait();
     unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned nx = L.nx, ny = L.ny;
     if (t >= nx * ny * (unsigned)L.nz) return;
@@ -1282,6 +1434,7 @@ template <class T>
 __global__ void k_cast_field(long long n, const double* __restrict__ in, T* __restrict__ out, double scale,
                              double shift)
 {
+    pdl_wait();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
         out[t] = (T)((in ? in[t] : 0.0) * scale + shift);
 }
@@ -1289,6 +1442,7 @@ __global__ void k_cast_field(long long n, const double* __restrict__ in, T* __re
 template <class A, class B>
 __global__ void k_axpy(long long n, double a, const A* __restrict__ x, B* __restrict__ y)
 {
+    pdl_wait();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
         y[t] = (B)((double)y[t] + a * (double)x[t]);
 }

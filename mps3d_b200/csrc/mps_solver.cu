@@ -31,6 +31,29 @@ constexpr int MAX_DENSE = 1024;
 
 static inline unsigned nblk(long long n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
 
+// launch with the programmatic stream-serialization attribute: the kernel may
+// be scheduled before its predecessor on the stream finishes, and waits for it
+// in its first statement (pdl_wait); inside a captured graph this becomes a
+// programmatic edge, which shortens the gap between dependent launches
+template <class... KArgs, class... Args>
+static cudaError_t pdl_launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args)
+{
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
+
 struct Err {
     int code = 0;
     std::string msg;
@@ -99,6 +122,7 @@ struct Signature {
 
 struct Prof {
     bool on = false;
+    int level = 0;  // the level whose smoothing/transfer launches are timed
     std::vector<cudaEvent_t> ev;
     std::vector<int> cls;
     int used = 0;
@@ -136,6 +160,10 @@ struct BatchState;
 struct Ctx {
     int dev = 0;
     BatchState* batch = nullptr;  // batched solves (mps_linsolve_batched_dev)
+    // the levels at and below small_first run in one CTA (k_vcycle_small);
+    // small_bytes = word size of the hierarchy the descriptor describes
+    void* small_desc = nullptr;
+    int small_first = -1, small_bytes = 0;
     long long launches = 0;
     Prof prof;
     std::vector<GraphEntry> graphs;
@@ -512,7 +540,7 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     const T* fh = H.F[l] + (c ? L.half : 0);
     if (c == 0) out = H.U[l][H.ri[l] ^ 1];
     else out = H.U[l][H.bi[l] ^ 1] + L.half;
-    if (l == 0) prof_begin(ctx, MPS_PROF_SMOOTH);
+    if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_SMOOTH);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (L.uniform || L.nx >= 16) {
             // vector kernel, W cells per thread (faces at a merged last cell
@@ -522,16 +550,16 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
             dg.init((unsigned)(L.P / W));
             const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
             if (zero_state == 2) {
-                k_colourv<T, W, ZeroU<T>><<<nbv, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh, dg);
+                pdl_launch(k_colourv<T, W, ZeroU<T>>, nbv, TPB, 0, ctx.s, L, op, c, ZeroU<T>(), out, fh, dg);
             } else if (zero_state == 1) {
                 OtherOnlyU<T> u;
                 u.c = c;
                 u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
-                k_colourv<T, W, OtherOnlyU<T>><<<nbv, TPB, 0, ctx.s>>>(L, op, c, u, out, fh, dg);
+                pdl_launch(k_colourv<T, W, OtherOnlyU<T>>, nbv, TPB, 0, ctx.s, L, op, c, u, out, fh, dg);
             } else {
-                k_colourv<T, W, CSplit<T>><<<nbv, TPB, 0, ctx.s>>>(L, op, c, ccur(H, L, l), out, fh, dg);
+                pdl_launch(k_colourv<T, W, CSplit<T>>, nbv, TPB, 0, ctx.s, L, op, c, ccur(H, L, l), out, fh, dg);
             }
-            if (l == 0) prof_end(ctx);
+            if (l == ctx.prof.level) prof_end(ctx);
             CKL();
             if (c == 0) H.ri[l] ^= 1;
             else H.bi[l] ^= 1;
@@ -539,16 +567,16 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
         }
     }
     if (zero_state == 2) {  // whole state zero
-        k_colour<T, Op, ZeroU<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, ZeroU<T>(), out, fh);
+        pdl_launch(k_colour<T, Op, ZeroU<T>>, nb, TPB, 0, ctx.s, L, op, c, ZeroU<T>(), out, fh);
     } else if (zero_state == 1) {  // colour c zero, other colour valid
         OtherOnlyU<T> u;
         u.c = c;
         u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
-        k_colour<T, Op, OtherOnlyU<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, u, out, fh);
+        pdl_launch(k_colour<T, Op, OtherOnlyU<T>>, nb, TPB, 0, ctx.s, L, op, c, u, out, fh);
     } else {
-        k_colour<T, Op, CSplit<T>><<<nb, TPB, 0, ctx.s>>>(L, op, c, ccur(H, L, l), out, fh);
+        pdl_launch(k_colour<T, Op, CSplit<T>>, nb, TPB, 0, ctx.s, L, op, c, ccur(H, L, l), out, fh);
     }
-    if (l == 0) prof_end(ctx);
+    if (l == ctx.prof.level) prof_end(ctx);
     CKL();
     if (c == 0) H.ri[l] ^= 1;
     else H.bi[l] ^= 1;
@@ -560,7 +588,7 @@ static int coarse_solve(Ctx& ctx, Hier<T>& H, int l)
 {
     const Lev& L = ctx.lev[l];
     const int n = L.nx * L.ny * L.nz;
-    k_coarse_solve<T><<<1, 512, n * sizeof(double), ctx.s>>>(L, H.AinvT, csplit<T>(H.F[l], L), cur(H, L, l));
+    pdl_launch(k_coarse_solve<T>, 1, 512, n * sizeof(double), ctx.s, L, H.AinvT, csplit<T>(H.F[l], L), cur(H, L, l));
     CKL();
     return 0;
 }
@@ -568,6 +596,25 @@ static int coarse_solve(Ctx& ctx, Hier<T>& H, int l)
 template <class T, class Op>
 static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solver_opts* o, bool zero_guess)
 {
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (l == ctx.small_first && ctx.small_bytes == (int)sizeof(T)) {
+            unsigned rb = 0, bb = 0;
+            for (int q = l; q < ctx.nlev; q++) {
+                rb |= (unsigned)H.ri[q] << (q - l);
+                bb |= (unsigned)H.bi[q] << (q - l);
+            }
+            pdl_launch(k_vcycle_small<T>, 1, SMALL_TPB, 0, ctx.s, (const SmallCycle<T>*)ctx.small_desc, zero_guess ? 1 : 0,
+                                                           rb, bb);
+            CKL();
+            // each level ran nu1 + nu2 passes of each colour
+            const int flip = (o->nu1 + o->nu2) & 1;
+            for (int q = l; q + 1 < ctx.nlev; q++) {
+                H.ri[q] ^= flip;
+                H.bi[q] ^= flip;
+            }
+            return 0;
+        }
+    }
     if (l == ctx.nlev - 1) return coarse_solve(ctx, H, l);
     const Lev& L = ctx.lev[l];
     const Lev& C = ctx.lev[l + 1];
@@ -582,7 +629,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         CK(cudaMemsetAsync(H.U[l][H.ri[l]], 0, sizeof(T) * L.half, ctx.s));
         CK(cudaMemsetAsync(H.U[l][H.bi[l]] + L.half, 0, sizeof(T) * L.half, ctx.s));
     }
-    if (l == 0) prof_begin(ctx, MPS_PROF_RESTRICT);
+    if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_RESTRICT);
     bool done = false;
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         Box bx;
@@ -593,12 +640,12 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
             const long long nt = (long long)C.rows * (L.P / W);
-            k_resid_restrict_v<T, W><<<nblk(nt), TPB, 0, ctx.s>>>(L, ops[l], ccur(H, L, l), H.F[l], C,
+            pdl_launch(k_resid_restrict_v<T, W>, nblk(nt), TPB, 0, ctx.s, L, ops[l], ccur(H, L, l), H.F[l], C,
                                                                   split<T>(H.F[l + 1], C), dg, bx);
             CKL();
             const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
             if (shell > 0) {
-                k_resid_restrict_shell<T, Op><<<nblk(8 * shell), TPB, 0, ctx.s>>>(
+                pdl_launch(k_resid_restrict_shell<T, Op>, nblk(8 * shell), TPB, 0, ctx.s, 
                     L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, bx,
                     (unsigned)shell);
                 CKL();
@@ -607,13 +654,13 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         }
     }
     if (!done) {
-        k_resid_restrict<T, Op><<<nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s>>>(
+        pdl_launch(k_resid_restrict<T, Op>, nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s, 
             L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom);
         CKL();
     }
-    if (l == 0) prof_end(ctx);
+    if (l == ctx.prof.level) prof_end(ctx);
     if ((st = vcycle_rec(ctx, H, ops, l + 1, o, true))) return st;
-    if (l == 0) prof_begin(ctx, MPS_PROF_PROLONG);
+    if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_PROLONG);
     // the first post-smoothing pass overwrites the red cells from the black
     // ones, so only black cells need the correction (unless an odd periodic
     // seam makes red cells read red neighbours)
@@ -636,18 +683,18 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         dv.gin.init((unsigned)std::max<long long>(gin, 1));
         dv.gout.init((unsigned)std::max<long long>(G - gin, 1));
         if (gin > 0) {
-            k_prolong_v<T, W><<<nblk(rin * gin), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
+            pdl_launch(k_prolong_v<T, W>, nblk(rin * gin), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
                                                                    pb, 0, (unsigned)(rin * gin), dv);
             CKL();
         }
         if (G > gin) {
-            k_prolong_v<T, W><<<nblk(rin * (G - gin)), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1),
+            pdl_launch(k_prolong_v<T, W>, nblk(rin * (G - gin)), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1),
                                                                          ctx.xf[l], pb, 3,
                                                                          (unsigned)(rin * (G - gin)), dv);
             CKL();
         }
         if (rall > rin) {
-            k_prolong_v<T, W><<<nblk((rall - rin) * G), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1),
+            pdl_launch(k_prolong_v<T, W>, nblk((rall - rin) * G), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1),
                                                                           ctx.xf[l], pb, 1, (unsigned)((rall - rin) * G),
                                                                           dv);
             CKL();
@@ -666,26 +713,26 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             if (cnt > 0) {
                 ProlongDiv sv = dv;
                 sv.yin.init((unsigned)(sb.hi[1] - sb.lo[1] + 1));
-                k_prolong_v<T, W><<<nblk(cnt), TPB, 0, ctx.s>>>(L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
+                pdl_launch(k_prolong_v<T, W>, nblk(cnt), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
                                                                  sb, 2, (unsigned)cnt, sv);
                 CKL();
             }
         }
     } else if (o->nu2 >= 1) {
-        k_prolong_correct<T><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, cur(H, L, l), C,
+        pdl_launch(k_prolong_correct<T>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, L, cur(H, L, l), C,
                                                                                ccur(H, C, l + 1), ctx.xf[l], 1);
         CKL();
         if (odd_periodic(L)) {
-            k_prolong_correct<T><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, cur(H, L, l), C,
+            pdl_launch(k_prolong_correct<T>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, L, cur(H, L, l), C,
                                                                                    ccur(H, C, l + 1), ctx.xf[l], 2);
             CKL();
         }
     } else {
-        k_prolong_correct<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
+        pdl_launch(k_prolong_correct<T>, nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s, 
             L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l], -1);
         CKL();
     }
-    if (l == 0) prof_end(ctx);
+    if (l == ctx.prof.level) prof_end(ctx);
     for (int s = 0; s < o->nu2; s++) {
         if ((st = colour_pass(ctx, H, ops[l], l, 0, 0))) return st;
         if ((st = colour_pass(ctx, H, ops[l], l, 1, 0))) return st;
@@ -713,14 +760,14 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             dg.init((unsigned)(L.P / W));
             const unsigned nbv = std::min<unsigned>(nblk((long long)(L.P / W) * L.rows), 148 * 8);
             // both colours in one pass (f and rout as split bases, halves L.half apart)
-            k_residv<T, W, R><<<nbv, TPB, 0, ctx.s>>>(L, op, -1, u, f.half(0), rout.c[0] ? rout.half(0) : nullptr,
+            pdl_launch(k_residv<T, W, R>, nbv, TPB, 0, ctx.s, L, op, -1, u, f.half(0), rout.c[0] ? rout.half(0) : nullptr,
                                                        ctx.rb, 0, dg);
             CKL();
             prof_end(ctx);
             return 0;
         }
     }
-    k_resid_norm<T, Op, R><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(L, op, u, f, rout, ctx.rb);
+    pdl_launch(k_resid_norm<T, Op, R>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, L, op, u, f, rout, ctx.rb);
     prof_end(ctx);
     CKL();
     return 0;
@@ -884,12 +931,12 @@ static int build_rows_level(Ctx& ctx, int l, T* rows, double dtinv, int flux, in
     const double* z = ctx.pk[l];  // any valid pointer for unused fields
     auto cs = [&](const double* p) { return csplit<double>(p ? p : z, L); };
     T* dst = transpose ? tmp : rows;
-    k_build_rows<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(
+    pdl_launch(k_build_rows<T>, nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s, 
         L, cs(ctx.pv[0][l]), cs(ctx.pv[1][l]), cs(ctx.pv[2][l]), cs(ctx.pk[l]), cs(ctx.preac[l]),
         ctx.preac[l] != nullptr, dtinv, flux, make_rop<T>(dst, L));
     CKL();
     if (transpose) {
-        k_transpose_rows<T><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s>>>(L, make_rop<T>(tmp, L),
+        pdl_launch(k_transpose_rows<T>, nblk((long long)L.nx * L.ny * L.nz), TPB, 0, ctx.s, L, make_rop<T>(tmp, L),
                                                                                    make_rop<T>(rows, L));
         CKL();
     }
@@ -903,16 +950,16 @@ static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
     const Lev& L = ctx.lev[l];
     const int n = L.nx * L.ny * L.nz;
     CK(cudaMemsetAsync(ctx.dense, 0, sizeof(double) * n * n, ctx.s));
-    k_dense_assemble<T, Op><<<nblk(n), TPB, 0, ctx.s>>>(L, op, ctx.dense);
+    pdl_launch(k_dense_assemble<T, Op>, nblk(n), TPB, 0, ctx.s, L, op, ctx.dense);
     CKL();
-    k_gj_prepare<<<nblk(2LL * n * n), TPB, 0, ctx.s>>>(n, ctx.dense, ctx.gjM);
+    pdl_launch(k_gj_prepare, nblk(2LL * n * n), TPB, 0, ctx.s, n, ctx.dense, ctx.gjM);
     CKL();
     const size_t smem = sizeof(double) * 2 * (size_t)n * n;
     if (smem <= 200 * 1024) {
         CK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        k_gauss_jordan<<<1, 1024, smem, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus, 1);
+        pdl_launch(k_gauss_jordan, 1, 1024, smem, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 1);
     } else {
-        k_gauss_jordan<<<1, 1024, 0, ctx.s>>>(n, ctx.gjM, H.AinvT, ctx.dstatus, 0);
+        pdl_launch(k_gauss_jordan, 1, 1024, 0, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 0);
     }
     CKL();
     return 0;
@@ -999,15 +1046,15 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     const long long ng = (long long)(L0.nx + 2) * (L0.ny + 2) * (L0.nz + 2);
     const unsigned mb = std::min<unsigned>(nblk(ncell), 1184);
     if (in.vel)
-        for (int a = 0; a < 3; a++) { k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.vel + a * ng, 0, dm + 0); CKL(); }
-    if (in.reac) { k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.reac, 0, dm + 1); CKL(); }
-    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.dcoeff, 1, dm + 2);
+        for (int a = 0; a < 3; a++) { pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.vel + a * ng, 0, dm + 0); CKL(); }
+    if (in.reac) { pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.reac, 0, dm + 1); CKL(); }
+    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.dcoeff, 1, dm + 2);
     CKL();
-    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.source, 0, dm + 3);
+    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.source, 0, dm + 3);
     CKL();
-    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.soln, 0, dm + 4);
+    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.soln, 0, dm + 4);
     CKL();
-    k_maxabs<<<mb, TPB, 0, ctx.s>>>(L0, in.dcoeff, 0, dm + 5);
+    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.dcoeff, 0, dm + 5);
     CKL();
     unsigned long long hm[8];
     CK(cudaMemcpyAsync(hm, dm, sizeof(hm), cudaMemcpyDeviceToHost, ctx.s));
@@ -1048,15 +1095,15 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     if (o->krylov == MPS_KRYLOV_FGMRES && (st = setup_krylov(ctx, 2 * ctx.lev[0].half, o->restart))) return st;
 
     // ---- coefficient pyramid (FP64) ----
-    k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.dcoeff, split<double>(ctx.pk[0], L0), 1.0, 0.0);
+    pdl_launch(k_pack<double>, nblk(ncell), TPB, 0, ctx.s, L0, in.dcoeff, split<double>(ctx.pk[0], L0), 1.0, 0.0);
     CKL();
     if (sig.has_reac) {
-        k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.reac, split<double>(ctx.preac[0], L0), 1.0, 0.0);
+        pdl_launch(k_pack<double>, nblk(ncell), TPB, 0, ctx.s, L0, in.reac, split<double>(ctx.preac[0], L0), 1.0, 0.0);
         CKL();
     }
     if (sig.opclass == 1)
         for (int a = 0; a < 3; a++) {
-            k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.vel ? in.vel + a * ng : nullptr,
+            pdl_launch(k_pack<double>, nblk(ncell), TPB, 0, ctx.s, L0, in.vel ? in.vel + a * ng : nullptr,
                                                            split<double>(ctx.pv[a][0], L0), 1.0, 0.0);
             CKL();
         }
@@ -1065,17 +1112,17 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         const Lev& C = ctx.lev[l + 1];
         const unsigned nb = nblk((long long)C.nx * C.ny * C.nz);
         const int geom = ctx.xf[l].geom;
-        k_restrict_field<<<nb, TPB, 0, ctx.s>>>(F, csplit<double>(ctx.pk[l], F), C, split<double>(ctx.pk[l + 1], C),
+        pdl_launch(k_restrict_field, nb, TPB, 0, ctx.s, F, csplit<double>(ctx.pk[l], F), C, split<double>(ctx.pk[l + 1], C),
                                                 geom);
         CKL();
         if (sig.has_reac) {
-            k_restrict_field<<<nb, TPB, 0, ctx.s>>>(F, csplit<double>(ctx.preac[l], F), C,
+            pdl_launch(k_restrict_field, nb, TPB, 0, ctx.s, F, csplit<double>(ctx.preac[l], F), C,
                                                     split<double>(ctx.preac[l + 1], C), geom);
             CKL();
         }
         if (sig.opclass == 1)
             for (int a = 0; a < 3; a++) {
-                k_restrict_field<<<nb, TPB, 0, ctx.s>>>(F, csplit<double>(ctx.pv[a][l], F), C,
+                pdl_launch(k_restrict_field, nb, TPB, 0, ctx.s, F, csplit<double>(ctx.pv[a][l], F), C,
                                                         split<double>(ctx.pv[a][l + 1], C), geom);
                 CKL();
             }
@@ -1085,16 +1132,16 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         for (int l = 0; l < nl; l++) {
             const long long n2 = 2 * ctx.lev[l].half;
             if (sig.has_reac) {
-                k_cast_field<double><<<std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s>>>(n2, ctx.preac[l], ctx.dex64[l], -1.0, dtinv);
+                pdl_launch(k_cast_field<double>, std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s, n2, ctx.preac[l], ctx.dex64[l], -1.0, dtinv);
                 CKL();
             }
             if (need32) {
                 if (!sig.kuni) {
-                    k_cast_field<float><<<std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s>>>(n2, ctx.pk[l], ctx.k32[l], 1.0, 0.0);
+                    pdl_launch(k_cast_field<float>, std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s, n2, ctx.pk[l], ctx.k32[l], 1.0, 0.0);
                     CKL();
                 }
                 if (sig.has_reac) {
-                    k_cast_field<float><<<std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s>>>(n2, ctx.preac[l], ctx.dex32[l], -1.0, dtinv);
+                    pdl_launch(k_cast_field<float>, std::min<unsigned>(nblk(n2), 2368), TPB, 0, ctx.s, n2, ctx.preac[l], ctx.dex32[l], -1.0, dtinv);
                     CKL();
                 }
             }
@@ -1134,10 +1181,10 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     {
         const double* bv[6];
         for (int f = 0; f < 6; f++) bv[f] = in.bcval[f];
-        k_find_bvec<<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.vel, in.dcoeff, in.source, bv[0], bv[1], bv[2], bv[3],
+        pdl_launch(k_find_bvec, nblk(ncell), TPB, 0, ctx.s, L0, in.vel, in.dcoeff, in.source, bv[0], bv[1], bv[2], bv[3],
                                                     bv[4], bv[5], in.sterm, o->flux, split<double>(ctx.b64, L0));
         CKL();
-        k_pack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, in.soln, split<double>(ctx.x64, L0), 1.0, 0.0);
+        pdl_launch(k_pack<double>, nblk(ncell), TPB, 0, ctx.s, L0, in.soln, split<double>(ctx.x64, L0), 1.0, 0.0);
         CKL();
     }
     // ---- coarsest inverse ----
@@ -1150,6 +1197,46 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         else st = coarse_inverse(ctx, ctx.h32, ctx.h32.rop[nl - 1]);
     }
     if (st) return st;
+    // ---- the small levels in one CTA ----
+    ctx.small_first = -1;
+    ctx.small_bytes = 0;
+    if (sig.opclass == 0 && !prepare_only) {
+        int l0 = nl;
+        while (l0 > 0 && (long long)ctx.lev[l0 - 1].nx * ctx.lev[l0 - 1].ny * ctx.lev[l0 - 1].nz <= SMALL_CELLS) l0--;
+        if (nl - l0 >= 2 && nl - l0 <= SMALL_MAXL) {
+            if (!ctx.small_desc) CK(cudaMalloc(&ctx.small_desc, sizeof(SmallCycle<double>)));
+            auto fill = [&](auto& H, auto* sc) {
+                sc->n = nl - l0;
+                sc->nu1 = o->nu1;
+                sc->nu2 = o->nu2;
+                sc->AinvT = H.AinvT;
+                for (int q = l0; q < nl; q++) {
+                    auto& v = sc->lev[q - l0];
+                    v.L = ctx.lev[q];
+                    v.op = H.kop[q];
+                    v.X = ctx.xf[q];
+                    v.U[0] = H.U[q][0];
+                    v.U[1] = H.U[q][1];
+                    v.F = H.F[q];
+                }
+            };
+            if (mixed) {
+                SmallCycle<float> sc;
+                std::memset(&sc, 0, sizeof(sc));
+                fill(ctx.h32, &sc);
+                CK(cudaMemcpyAsync(ctx.small_desc, &sc, sizeof(sc), cudaMemcpyHostToDevice, ctx.s));
+                ctx.small_bytes = 4;
+            } else {
+                SmallCycle<double> sc;
+                std::memset(&sc, 0, sizeof(sc));
+                fill(ctx.h64, &sc);
+                CK(cudaMemcpyAsync(ctx.small_desc, &sc, sizeof(sc), cudaMemcpyHostToDevice, ctx.s));
+                ctx.small_bytes = 8;
+            }
+            CK(cudaStreamSynchronize(ctx.s));  // the host copy of the descriptor goes out of scope
+            ctx.small_first = l0;
+        }
+    }
     if (prepare_only) {
         inf.levels = nl;
         if (info) *info = inf;
@@ -1180,7 +1267,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     gk.kc = sig.kuni ? k0 : 0.0;
     gk.dexc = sig.has_reac ? 0.0 : dtinv;
     gk.ws = ctx.ar.blocks.empty() ? nullptr : ctx.ar.blocks[0];
-    gk.prof = ctx.prof.on;  // profiled graphs carry event-record nodes
+    gk.prof = ctx.prof.on ? 1 + ctx.prof.level : 0;  // profiled graphs carry event-record nodes
     // graphs need the buffer parities to return after one iteration
     const bool graphs = o->use_graph && ((o->nu1 + o->nu2) % 2 == 0);
 
@@ -1246,9 +1333,9 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
             for (int c = 0; c < inner; c++)
                 if ((s2 = vcycle(ctx, H, sig.opclass, o, c == 0))) return s2;
             const unsigned ab = std::min<unsigned>(nblk(L.half), 4736);
-            k_axpy<float, double><<<ab, TPB, 0, ctx.s>>>(L.half, 1.0, H.U[0][H.ri[0]], ctx.x64);
+            pdl_launch(k_axpy<float, double>, ab, TPB, 0, ctx.s, L.half, 1.0, H.U[0][H.ri[0]], ctx.x64);
             CKL();
-            k_axpy<float, double><<<ab, TPB, 0, ctx.s>>>(L.half, 1.0, H.U[0][H.bi[0]] + L.half, ctx.x64 + L.half);
+            pdl_launch(k_axpy<float, double>, ab, TPB, 0, ctx.s, L.half, 1.0, H.U[0][H.bi[0]] + L.half, ctx.x64 + L.half);
             CKL();
             return residual();
         };
@@ -1304,7 +1391,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
             // v0 = w / beta
             ctx.hpin[0] = beta;
             CK(cudaMemcpyAsync(ctx.hcol, ctx.hpin, sizeof(double), cudaMemcpyHostToDevice, ctx.s));
-            k_scale_to<<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, ctx.w, ctx.hcol, 0, ctx.V, nullptr);
+            pdl_launch(k_scale_to, std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s, n, ctx.w, ctx.hcol, 0, ctx.V, nullptr);
             CKL();
             std::fill(H.begin(), H.end(), 0.0);
             std::fill(gq.begin(), gq.end(), 0.0);
@@ -1316,7 +1403,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 // z_j = M^{-1} v_j (one V-cycle from zero), then w = A z_j in FP64
                 if (mixed) {
                     Hier<float>& P = ctx.h32;
-                    k_cast_field<float><<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, vj, P.F[0], 1.0, 0.0);
+                    pdl_launch(k_cast_field<float>, std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s, n, vj, P.F[0], 1.0, 0.0);
                     CKL();
                     if (graphs) {
                         gk.kind = 3;
@@ -1331,10 +1418,10 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                     CK(cudaMemcpyAsync(zj + L.half, P.U[0][P.bi[0]] + L.half, sizeof(float) * L.half,
                                        cudaMemcpyDeviceToDevice, ctx.s));
                     if (sig.opclass == 0)
-                        k_apply<double, KOp<double>, float><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                        pdl_launch(k_apply<double, KOp<double>, float>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, 
                             L, ctx.kop64, csplit<float>(zj, L), split<double>(ctx.w, L));
                     else
-                        k_apply<double, ROp<double>, float><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                        pdl_launch(k_apply<double, ROp<double>, float>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, 
                             L, ctx.rop64, csplit<float>(zj, L), split<double>(ctx.w, L));
                     CKL();
                 } else {
@@ -1353,10 +1440,10 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                     CK(cudaMemcpyAsync(zj + L.half, P.U[0][P.bi[0]] + L.half, sizeof(double) * L.half,
                                        cudaMemcpyDeviceToDevice, ctx.s));
                     if (sig.opclass == 0)
-                        k_apply<double, KOp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                        pdl_launch(k_apply<double, KOp<double>, double>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, 
                             L, ctx.kop64, csplit<double>(zj, L), split<double>(ctx.w, L));
                     else
-                        k_apply<double, ROp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, ctx.s>>>(
+                        pdl_launch(k_apply<double, ROp<double>, double>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, 
                             L, ctx.rop64, csplit<double>(zj, L), split<double>(ctx.w, L));
                     CKL();
                 }
@@ -1365,17 +1452,17 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 // hcol[m+2 ..]; the Hessenberg column is their sum
                 for (int pass = 0; pass < 2; pass++) {
                     double* hp = ctx.hcol + (pass ? m + 2 : 0);
-                    k_multidot<<<db, TPB, 0, ctx.s>>>(n, j + 1, ctx.Vptr, ctx.w, ctx.dpart);
+                    pdl_launch(k_multidot, db, TPB, 0, ctx.s, n, j + 1, ctx.Vptr, ctx.w, ctx.dpart);
                     CKL();
-                    k_multidot_finish<<<j + 1, TPB, 0, ctx.s>>>(j + 1, db, ctx.dpart, hp, 0);
+                    pdl_launch(k_multidot_finish, j + 1, TPB, 0, ctx.s, j + 1, db, ctx.dpart, hp, 0);
                     CKL();
-                    k_multiaxpy<<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, j + 1, ctx.Vptr, hp, ctx.w);
+                    pdl_launch(k_multiaxpy, std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s, n, j + 1, ctx.Vptr, hp, ctx.w);
                     CKL();
                 }
                 // ||w||^2 (Vptr[m+1] points at w) into hcol[j+1]
-                k_multidot<<<db, TPB, 0, ctx.s>>>(n, 1, ctx.Vptr + m + 1, ctx.w, ctx.dpart);
+                pdl_launch(k_multidot, db, TPB, 0, ctx.s, n, 1, ctx.Vptr + m + 1, ctx.w, ctx.dpart);
                 CKL();
-                k_multidot_finish<<<1, TPB, 0, ctx.s>>>(1, db, ctx.dpart, ctx.hcol + j + 1, 0);
+                pdl_launch(k_multidot_finish, 1, TPB, 0, ctx.s, 1, db, ctx.dpart, ctx.hcol + j + 1, 0);
                 CKL();
                 CK(cudaMemcpyAsync(ctx.hpin, ctx.hcol, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, ctx.s));
                 CK(cudaMemcpyAsync(ctx.hpin + 256, ctx.hcol + m + 2, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost,
@@ -1388,7 +1475,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 ctx.hpin[0] = hn;
                 CK(cudaMemcpyAsync(ctx.hcol + j + 1, ctx.hpin, sizeof(double), cudaMemcpyHostToDevice, ctx.s));
                 if (hn > 0.0) {
-                    k_scale_to<<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, ctx.w, ctx.hcol, j + 1,
+                    pdl_launch(k_scale_to, std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s, n, ctx.w, ctx.hcol, j + 1,
                                                                                     ctx.V + (size_t)(j + 1) * n, nullptr);
                     CKL();
                 }
@@ -1417,9 +1504,9 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
             }
             for (int i = 0; i < j; i++) {
                 if (mixed)
-                    k_axpy<float, double><<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, y[i], (float*)ctx.Z + (size_t)i * n, ctx.x64);
+                    pdl_launch(k_axpy<float, double>, std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s, n, y[i], (float*)ctx.Z + (size_t)i * n, ctx.x64);
                 else
-                    k_axpy<double, double><<<std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s>>>(n, y[i], (double*)ctx.Z + (size_t)i * n, ctx.x64);
+                    pdl_launch(k_axpy<double, double>, std::min<unsigned>(nblk(n), 2368), TPB, 0, ctx.s, n, y[i], (double*)ctx.Z + (size_t)i * n, ctx.x64);
                 CKL();
             }
         }
@@ -1427,13 +1514,13 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     // ---- output ----
     int gst = 0;
     CK(cudaMemcpyAsync(&gst, ctx.dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx.s));
-    k_unpack<double><<<nblk(ncell), TPB, 0, ctx.s>>>(L0, csplit<double>(ctx.x64, L0), in.soln);
+    pdl_launch(k_unpack<double>, nblk(ncell), TPB, 0, ctx.s, L0, csplit<double>(ctx.x64, L0), in.soln);
     CKL();
     if (o->fill_ghosts) {
         const int mx = std::max(std::max(L0.ny * L0.nz, L0.nx * L0.nz), L0.nx * L0.ny);
         const double* zf[6];
         for (int f = 0; f < 6; f++) zf[f] = in.bcval[f];
-        k_fill_ghosts<<<nblk(mx), TPB, 0, ctx.s>>>(L0, in.soln, zf[0], zf[1], zf[2], zf[3], zf[4], zf[5]);
+        pdl_launch(k_fill_ghosts, nblk(mx), TPB, 0, ctx.s, L0, in.soln, zf[0], zf[1], zf[2], zf[3], zf[4], zf[5]);
         CKL();
     }
     CK(cudaEventRecord(ctx.e1, ctx.s));
@@ -1524,6 +1611,7 @@ int mps_destroy(mps_handle h)
     cudaStreamSynchronize(ctx.s);
     destroy_batch(ctx);
     destroy_graphs(ctx);
+    if (ctx.small_desc) cudaFree(ctx.small_desc);
     ctx.ar.clear();
     ctx.kar.clear();
     ctx.inbuf.clear();
@@ -1612,6 +1700,7 @@ int mps_set_profile(mps_handle h, int on)
 {
     if (!h) return MPS_ERR_BAD_ARG;
     h->ctx.prof.on = on != 0;
+    h->ctx.prof.level = on > 1 ? on - 1 : 0;
     return MPS_OK;
 }
 
