@@ -548,12 +548,10 @@ struct RestrictShape {
 };
 
 template <class T, int W>
-__global__ void __launch_bounds__(TPB, RestrictShape<T>::MINB) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
-                                                                                 const T* __restrict__ fred, Lev C,
-                                                                                 Split<T> fc, FastDiv divG, Box bx)
+__device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& op, const CSplit<T>& u,
+                                                    const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
+                                                    const FastDiv& divG, const Box& bx, unsigned t)
 {
-    pdl_wait();
-    const unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned R = divG.div(t);  // coarse row J + Cny K
     if (R >= C.rows) return;
     const int K = (int)C.divNy.div(R);
@@ -620,13 +618,13 @@ __device__ __forceinline__ void shell_cell(unsigned t, const int n[3], const Box
     I = (int)(m < (unsigned)b.lo[0] ? m : b.hi[0] + 1 + (m - b.lo[0]));
 }
 
-// eight lanes per shell cell, each summing a share of the children
+// eight lanes per shell cell, each summing a share of the children (every
+// lane of the warp takes part in the shuffles)
 template <class T, class Op>
-__global__ void __launch_bounds__(TPB) k_resid_restrict_shell(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
-                                                              Split<T> fc, int geom, Box bx, unsigned count)
+__device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op, const CSplit<T>& u,
+                                                     const CSplit<T>& f, const Lev& C, const Split<T>& fc, int geom,
+                                                     const Box& bx, unsigned count, unsigned t)
 {
-    pdl_wait();
-    const unsigned t = blockIdx.x * TPB + threadIdx.x;
     const unsigned cell = t >> 3;
     const int part = (int)(t & 7);
     const bool ok = cell < count;
@@ -637,13 +635,33 @@ __global__ void __launch_bounds__(TPB) k_resid_restrict_shell(Lev F, Op op, CSpl
         shell_cell(cell, n, bx, I, J, K);
         resid_restrict_part<T, Op>(F, op, u, f, C, geom, I, J, K, part, 8, s, vol);
     }
-    // every lane of the warp takes part in the shuffles
 #pragma unroll
     for (int o = 4; o > 0; o >>= 1) {
         s += __shfl_xor_sync(0xffffffffu, s, o, 8);
         vol += __shfl_xor_sync(0xffffffffu, vol, o, 8);
     }
     if (ok && part == 0) fc.half(scol(I, J, K))[soff(C, I, J, K)] = geom ? s / vol : s * (T(1) / vol);
+}
+
+// bulk and shell in one launch: blocks [0, nb_bulk) take the bulk rows,
+// the rest the shell cells
+template <class T, int W>
+__global__ void __launch_bounds__(TPB, RestrictShape<T>::MINB) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
+                                                                                 const T* __restrict__ fred, Lev C,
+                                                                                 Split<T> fc, FastDiv divG, Box bx,
+                                                                                 unsigned nb_bulk, int geom,
+                                                                                 unsigned shell)
+{
+    pdl_wait();
+    if (blockIdx.x < nb_bulk) {
+        resid_restrict_bulk<T, W>(F, op, u, fred, C, fc, divG, bx, blockIdx.x * TPB + threadIdx.x);
+    } else {
+        CSplit<T> f;
+        f.c[0] = fred;
+        f.c[1] = fred + F.half;
+        resid_restrict_shell<T, KOp<T>>(F, op, u, f, C, fc, geom, bx, shell,
+                                        (blockIdx.x - nb_bulk) * TPB + threadIdx.x);
+    }
 }
 
 // coarse ghost rule for the correction (update_boundary_ghostvalues applied
@@ -838,13 +856,36 @@ struct ProlongDiv {
     int g_lo, g_hi;  // the groups in the box: [g_lo, g_hi]
 };
 
+// the four parts of a prolongation in one launch: consecutive block ranges
+// take modes 0, 3, 1, 2 (cnt: threads of each part; mode 2 has its own box
+// and divisors)
+struct ProlongParts {
+    unsigned cnt[4];   // modes 0, 3, 1, 2
+    unsigned blk0[5];  // first block of each part, and the total
+};
+
 template <class T, int W>
-__global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, Box bx, int mode,
-                                                   unsigned count, ProlongDiv dv)
+__global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, Box pbox,
+                                                   ProlongDiv pdiv, Box sbox, ProlongDiv sdiv, ProlongParts pp)
 {
     pdl_wait();
-    const unsigned t = blockIdx.x * TPB + threadIdx.x;
-    if (t >= count) return;
+    int part = 0;
+    while (part < 3 && blockIdx.x >= pp.blk0[part + 1]) part++;
+    const int mode = part == 0 ? 0 : (part == 1 ? 3 : (part == 2 ? 1 : 2));
+    const unsigned t = (blockIdx.x - pp.blk0[part]) * TPB + threadIdx.x;
+    if (t >= pp.cnt[part]) return;
+    // field-wise selection keeps both parameter structs out of local memory
+    const bool m2 = mode == 2;
+    Box bx;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        bx.lo[a] = m2 ? sbox.lo[a] : pbox.lo[a];
+        bx.hi[a] = m2 ? sbox.hi[a] : pbox.hi[a];
+    }
+    ProlongDiv dv = pdiv;
+    dv.yin.M = m2 ? sdiv.yin.M : pdiv.yin.M;
+    dv.yin.l = m2 ? sdiv.yin.l : pdiv.yin.l;
+    dv.yin.d = m2 ? sdiv.yin.d : pdiv.yin.d;
     int j, k, h0, c, nel;
     if (mode == 0 || mode == 3) {
         // rows inside the box; mode 0: the groups inside along x (every cell

@@ -640,16 +640,11 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
             const long long nt = (long long)C.rows * (L.P / W);
-            pdl_launch(k_resid_restrict_v<T, W>, nblk(nt), TPB, 0, ctx.s, L, ops[l], ccur(H, L, l), H.F[l], C,
-                                                                  split<T>(H.F[l + 1], C), dg, bx);
-            CKL();
             const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
-            if (shell > 0) {
-                pdl_launch(k_resid_restrict_shell<T, Op>, nblk(8 * shell), TPB, 0, ctx.s, 
-                    L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, bx,
-                    (unsigned)shell);
-                CKL();
-            }
+            const unsigned nbb = nblk(nt), nbs = shell > 0 ? nblk(8 * shell) : 0;
+            pdl_launch(k_resid_restrict_v<T, W>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l), H.F[l], C,
+                       split<T>(H.F[l + 1], C), dg, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
+            CKL();
             done = true;
         }
     }
@@ -682,42 +677,28 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         if (gin == 0) { dv.g_lo = 0; dv.g_hi = -1; }
         dv.gin.init((unsigned)std::max<long long>(gin, 1));
         dv.gout.init((unsigned)std::max<long long>(G - gin, 1));
-        if (gin > 0) {
-            pdl_launch(k_prolong_v<T, W>, nblk(rin * gin), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
-                                                                   pb, 0, (unsigned)(rin * gin), dv);
-            CKL();
-        }
-        if (G > gin) {
-            pdl_launch(k_prolong_v<T, W>, nblk(rin * (G - gin)), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1),
-                                                                         ctx.xf[l], pb, 3,
-                                                                         (unsigned)(rin * (G - gin)), dv);
-            CKL();
-        }
-        if (rall > rin) {
-            pdl_launch(k_prolong_v<T, W>, nblk((rall - rin) * G), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1),
-                                                                          ctx.xf[l], pb, 1, (unsigned)((rall - rin) * G),
-                                                                          dv);
-            CKL();
-        }
-        if (odd_periodic(L)) {  // red cells on the seams are read by the next red pass
-            Box sb;
-            const int sy = L.per[1] && (L.ny & 1), sz = L.per[2] && (L.nz & 1), sx = L.per[0] && (L.nx & 1);
-            sb.lo[0] = 0;
-            sb.hi[0] = L.nx - 1;
-            sb.lo[1] = sy;
-            sb.hi[1] = L.ny - 1 - sy;
-            sb.lo[2] = sz;
-            sb.hi[2] = L.nz - 1 - sz;
-            const long long rin2 = (long long)(sb.hi[1] - sb.lo[1] + 1) * (sb.hi[2] - sb.lo[2] + 1);
-            const long long cnt = (rall - rin2) * ((L.nx + 1) / 2) + (sx ? 2 * rin2 : 0);
-            if (cnt > 0) {
-                ProlongDiv sv = dv;
-                sv.yin.init((unsigned)(sb.hi[1] - sb.lo[1] + 1));
-                pdl_launch(k_prolong_v<T, W>, nblk(cnt), TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
-                                                                 sb, 2, (unsigned)cnt, sv);
-                CKL();
-            }
-        }
+        // red cells on odd periodic seams (read by the next red pass)
+        Box sb;
+        const int sy = L.per[1] && (L.ny & 1), sz = L.per[2] && (L.nz & 1), sx = L.per[0] && (L.nx & 1);
+        sb.lo[0] = 0;
+        sb.hi[0] = L.nx - 1;
+        sb.lo[1] = sy;
+        sb.hi[1] = L.ny - 1 - sy;
+        sb.lo[2] = sz;
+        sb.hi[2] = L.nz - 1 - sz;
+        const long long rin2 = (long long)(sb.hi[1] - sb.lo[1] + 1) * (sb.hi[2] - sb.lo[2] + 1);
+        ProlongDiv sv = dv;
+        sv.yin.init((unsigned)(sb.hi[1] - sb.lo[1] + 1));
+        ProlongParts pp;
+        pp.cnt[0] = (unsigned)(rin * gin);
+        pp.cnt[1] = (unsigned)(rin * (G - gin));
+        pp.cnt[2] = (unsigned)((rall - rin) * G);
+        pp.cnt[3] = odd_periodic(L) ? (unsigned)((rall - rin2) * ((L.nx + 1) / 2) + (sx ? 2 * rin2 : 0)) : 0u;
+        pp.blk0[0] = 0;
+        for (int q = 0; q < 4; q++) pp.blk0[q + 1] = pp.blk0[q] + nblk(pp.cnt[q]);
+        pdl_launch(k_prolong_v<T, W>, pp.blk0[4], TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
+                   pb, dv, sb, sv, pp);
+        CKL();
     } else if (o->nu2 >= 1) {
         pdl_launch(k_prolong_correct<T>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, L, cur(H, L, l), C,
                                                                                ccur(H, C, l + 1), ctx.xf[l], 1);
