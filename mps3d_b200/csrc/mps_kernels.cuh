@@ -1027,134 +1027,6 @@ __global__ void __launch_bounds__(512) k_coarse_solve(Lev C, const double* __res
     coarse_solve_body<T>(C, AinvT, f, u, fs);
 }
 
-// ---------------------------------------------------------------------
-// the lower part of a V-cycle in one CTA: every level from `first` down to
-// the coarsest has at most SMALL_CELLS cells, where a launch per colour pass
-// costs more than the pass.  The same device bodies as the single-level
-// kernels, over thread-strided indices with a block barrier between phases:
-// pre-smoothing and residual restriction down, the dense coarsest solve,
-// prolongation (all cells) and post-smoothing up.  The buffer parities start
-// from the host's and advance exactly as the host's do.
-// ---------------------------------------------------------------------
-constexpr int SMALL_CELLS = 512;
-constexpr int SMALL_MAXL = 8;
-constexpr int SMALL_TPB = 1024;
-
-template <class T>
-struct SmallLevel {
-    Lev L;
-    KOp<T> op;
-    Xfer X;  // to the next coarser level
-    T* U[2];
-    T* F;
-};
-template <class T>
-struct SmallCycle {
-    int n;  // levels, the last is the coarsest
-    int nu1, nu2;
-    const double* AinvT;
-    SmallLevel<T> lev[SMALL_MAXL];
-};
-
-template <class T>
-__global__ void __launch_bounds__(SMALL_TPB) k_vcycle_small(const SmallCycle<T>* __restrict__ sc, int zero_first,
-                                                            unsigned ri_bits, unsigned bi_bits)
-{
-    pdl_wait();
-    __shared__ double fs[1024];
-    const SmallCycle<T>& S = *sc;
-    const int n = S.n;
-    unsigned ri = ri_bits, bi = bi_bits;  // bit l: parity of level l
-    auto cur = [&](int l) {
-        CSplit<T> u;
-        u.c[0] = S.lev[l].U[(ri >> l) & 1];
-        u.c[1] = S.lev[l].U[(bi >> l) & 1] + S.lev[l].L.half;
-        return u;
-    };
-    auto colour = [&](int l, int c, int zs) {
-        const SmallLevel<T>& Lv = S.lev[l];
-        const Lev& L = Lv.L;
-        const unsigned par = c == 0 ? (ri >> l) & 1 : (bi >> l) & 1;
-        T* out = Lv.U[par ^ 1] + (c ? L.half : 0);
-        const T* fh = Lv.F + (c ? L.half : 0);
-        const unsigned nt = (unsigned)L.P * L.rows;
-        if (zs == 2) {
-            for (unsigned t = threadIdx.x; t < nt; t += blockDim.x)
-                colour_body<T, KOp<T>, ZeroU<T>>(L, Lv.op, c, ZeroU<T>(), out, fh, t);
-        } else if (zs == 1) {
-            OtherOnlyU<T> u;
-            u.c = c;
-            const CSplit<T> cu = cur(l);
-            u.other = c == 0 ? cu.c[1] : cu.c[0];
-            for (unsigned t = threadIdx.x; t < nt; t += blockDim.x)
-                colour_body<T, KOp<T>, OtherOnlyU<T>>(L, Lv.op, c, u, out, fh, t);
-        } else {
-            const CSplit<T> u = cur(l);
-            for (unsigned t = threadIdx.x; t < nt; t += blockDim.x)
-                colour_body<T, KOp<T>, CSplit<T>>(L, Lv.op, c, u, out, fh, t);
-        }
-        if (c == 0) ri ^= 1u << l;
-        else bi ^= 1u << l;
-        __syncthreads();
-    };
-    for (int l = 0; l + 1 < n; l++) {
-        const bool z = l > 0 || zero_first;
-        for (int s2 = 0; s2 < S.nu1; s2++) {
-            colour(l, 0, z && s2 == 0 ? 2 : 0);
-            colour(l, 1, z && s2 == 0 ? 1 : 0);
-        }
-        const SmallLevel<T>& Lv = S.lev[l];
-        const SmallLevel<T>& Cv = S.lev[l + 1];
-        if (S.nu1 == 0 && z) {  // the zero initial guess of this level
-            const CSplit<T> u = cur(l);
-            for (long long t = threadIdx.x; t < Lv.L.half; t += blockDim.x) {
-                const_cast<T*>(u.c[0])[t] = T(0);
-                const_cast<T*>(u.c[1])[t] = T(0);
-            }
-            __syncthreads();
-        }
-        CSplit<T> f;
-        f.c[0] = Lv.F;
-        f.c[1] = Lv.F + Lv.L.half;
-        Split<T> fc;
-        fc.c[0] = Cv.F;
-        fc.c[1] = Cv.F + Cv.L.half;
-        const unsigned nc = (unsigned)Cv.L.nx * Cv.L.ny * Cv.L.nz;
-        const CSplit<T> u = cur(l);
-        for (unsigned t = threadIdx.x; t < nc; t += blockDim.x)
-            resid_restrict_body<T, KOp<T>>(Lv.L, Lv.op, u, f, Cv.L, fc, Lv.X.geom, t);
-        __syncthreads();
-    }
-    {
-        const SmallLevel<T>& Cv = S.lev[n - 1];
-        CSplit<T> f;
-        f.c[0] = Cv.F;
-        f.c[1] = Cv.F + Cv.L.half;
-        const CSplit<T> cu = cur(n - 1);
-        Split<T> u;
-        u.c[0] = const_cast<T*>(cu.c[0]);
-        u.c[1] = const_cast<T*>(cu.c[1]);
-        coarse_solve_body<T>(Cv.L, S.AinvT, f, u, fs);
-        __syncthreads();
-    }
-    for (int l = n - 2; l >= 0; l--) {
-        const SmallLevel<T>& Lv = S.lev[l];
-        const SmallLevel<T>& Cv = S.lev[l + 1];
-        const CSplit<T> cu = cur(l);
-        Split<T> u;
-        u.c[0] = const_cast<T*>(cu.c[0]);
-        u.c[1] = const_cast<T*>(cu.c[1]);
-        const CSplit<T> e = cur(l + 1);
-        const unsigned nf = (unsigned)Lv.L.nx * Lv.L.ny * Lv.L.nz;
-        for (unsigned t = threadIdx.x; t < nf; t += blockDim.x) prolong_body<T>(Lv.L, u, Cv.L, e, Lv.X, -1, t);
-        __syncthreads();
-        for (int s2 = 0; s2 < S.nu2; s2++) {
-            colour(l, 0, 0);
-            colour(l, 1, 0);
-        }
-    }
-}
-
 // dense assembly of the coarsest operator (row major, FP64, pre-zeroed)
 template <class T>
 __device__ __forceinline__ void dense_row(const KOp<T>& op, const Lev& L, int i, int j, int k, double* A, int n)

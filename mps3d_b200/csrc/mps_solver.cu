@@ -160,10 +160,6 @@ struct BatchState;
 struct Ctx {
     int dev = 0;
     BatchState* batch = nullptr;  // batched solves (mps_linsolve_batched_dev)
-    // the levels at and below small_first run in one CTA (k_vcycle_small);
-    // small_bytes = word size of the hierarchy the descriptor describes
-    void* small_desc = nullptr;
-    int small_first = -1, small_bytes = 0;
     long long launches = 0;
     Prof prof;
     std::vector<GraphEntry> graphs;
@@ -596,25 +592,6 @@ static int coarse_solve(Ctx& ctx, Hier<T>& H, int l)
 template <class T, class Op>
 static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solver_opts* o, bool zero_guess)
 {
-    if constexpr (std::is_same<Op, KOp<T>>::value) {
-        if (l == ctx.small_first && ctx.small_bytes == (int)sizeof(T)) {
-            unsigned rb = 0, bb = 0;
-            for (int q = l; q < ctx.nlev; q++) {
-                rb |= (unsigned)H.ri[q] << (q - l);
-                bb |= (unsigned)H.bi[q] << (q - l);
-            }
-            pdl_launch(k_vcycle_small<T>, 1, SMALL_TPB, 0, ctx.s, (const SmallCycle<T>*)ctx.small_desc, zero_guess ? 1 : 0,
-                                                           rb, bb);
-            CKL();
-            // each level ran nu1 + nu2 passes of each colour
-            const int flip = (o->nu1 + o->nu2) & 1;
-            for (int q = l; q + 1 < ctx.nlev; q++) {
-                H.ri[q] ^= flip;
-                H.bi[q] ^= flip;
-            }
-            return 0;
-        }
-    }
     if (l == ctx.nlev - 1) return coarse_solve(ctx, H, l);
     const Lev& L = ctx.lev[l];
     const Lev& C = ctx.lev[l + 1];
@@ -1178,46 +1155,6 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         else st = coarse_inverse(ctx, ctx.h32, ctx.h32.rop[nl - 1]);
     }
     if (st) return st;
-    // ---- the small levels in one CTA ----
-    ctx.small_first = -1;
-    ctx.small_bytes = 0;
-    if (sig.opclass == 0 && !prepare_only) {
-        int l0 = nl;
-        while (l0 > 0 && (long long)ctx.lev[l0 - 1].nx * ctx.lev[l0 - 1].ny * ctx.lev[l0 - 1].nz <= SMALL_CELLS) l0--;
-        if (nl - l0 >= 2 && nl - l0 <= SMALL_MAXL) {
-            if (!ctx.small_desc) CK(cudaMalloc(&ctx.small_desc, sizeof(SmallCycle<double>)));
-            auto fill = [&](auto& H, auto* sc) {
-                sc->n = nl - l0;
-                sc->nu1 = o->nu1;
-                sc->nu2 = o->nu2;
-                sc->AinvT = H.AinvT;
-                for (int q = l0; q < nl; q++) {
-                    auto& v = sc->lev[q - l0];
-                    v.L = ctx.lev[q];
-                    v.op = H.kop[q];
-                    v.X = ctx.xf[q];
-                    v.U[0] = H.U[q][0];
-                    v.U[1] = H.U[q][1];
-                    v.F = H.F[q];
-                }
-            };
-            if (mixed) {
-                SmallCycle<float> sc;
-                std::memset(&sc, 0, sizeof(sc));
-                fill(ctx.h32, &sc);
-                CK(cudaMemcpyAsync(ctx.small_desc, &sc, sizeof(sc), cudaMemcpyHostToDevice, ctx.s));
-                ctx.small_bytes = 4;
-            } else {
-                SmallCycle<double> sc;
-                std::memset(&sc, 0, sizeof(sc));
-                fill(ctx.h64, &sc);
-                CK(cudaMemcpyAsync(ctx.small_desc, &sc, sizeof(sc), cudaMemcpyHostToDevice, ctx.s));
-                ctx.small_bytes = 8;
-            }
-            CK(cudaStreamSynchronize(ctx.s));  // the host copy of the descriptor goes out of scope
-            ctx.small_first = l0;
-        }
-    }
     if (prepare_only) {
         inf.levels = nl;
         if (info) *info = inf;
@@ -1592,7 +1529,6 @@ int mps_destroy(mps_handle h)
     cudaStreamSynchronize(ctx.s);
     destroy_batch(ctx);
     destroy_graphs(ctx);
-    if (ctx.small_desc) cudaFree(ctx.small_desc);
     ctx.ar.clear();
     ctx.kar.clear();
     ctx.inbuf.clear();
