@@ -114,6 +114,56 @@ __global__ void k_maxabs(Lev L, const double* __restrict__ g, int rel, unsigned 
     if ((threadIdx.x & 31) == 0) atomicMax(out, b);
 }
 
+// the maxima of |field| over the interior of every present field in one pass
+// (warp per row, lanes along x): out[0] vel (3 components), out[1] reac,
+// out[2] |dcoeff - dcoeff(1,1,1)|, out[3] source, out[4] soln, out[5] dcoeff;
+// NaN/Inf sort above every finite value (atomicMax on the bit patterns)
+__global__ void k_maxabs_all(Lev L, const double* __restrict__ vel, const double* __restrict__ reac,
+                             const double* __restrict__ dcoeff, const double* __restrict__ source,
+                             const double* __restrict__ soln, unsigned long long* out)
+{
+    pdl_wait();
+    const long long gx = L.nx + 2, gy = L.ny + 2;
+    const long long ng = gx * gy * (L.nz + 2);
+    const double ref = dcoeff[1 + gx * (1 + gy)];
+    long long m[6] = {0, 0, 0, 0, 0, 0};
+    auto upd = [](long long& cur, double v) {
+        v = fabs(v);
+        if (!(v <= 1.0e308)) v = __longlong_as_double(0x7ff8000000000000LL);
+        const long long b = __double_as_longlong(v);
+        cur = b > cur ? b : cur;
+    };
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (unsigned row = warp; row < L.rows; row += nwarp) {
+        const unsigned k = L.divNy.div(row), j = row - k * (unsigned)L.ny;
+        const long long base = 1 + gx * ((long long)(j + 1) + gy * (long long)(k + 1));
+        for (int i = lane; i < L.nx; i += 32) {
+            const long long g = base + i;
+            if (vel) {
+                upd(m[0], vel[g]);
+                upd(m[0], vel[g + ng]);
+                upd(m[0], vel[g + 2 * ng]);
+            }
+            if (reac) upd(m[1], reac[g]);
+            const double d = dcoeff[g];
+            upd(m[2], d - ref);
+            upd(m[5], d);
+            upd(m[3], source[g]);
+            upd(m[4], soln[g]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        long long b = m[q];
+        for (int o = 16; o > 0; o >>= 1) {
+            const long long ob = __shfl_down_sync(0xffffffffu, b, o);
+            b = ob > b ? ob : b;
+        }
+        if (lane == 0 && b > 0) atomicMax(out + q, (unsigned long long)b);
+    }
+}
+
 __global__ void k_fill_ghosts(Lev L, double* __restrict__ g, const double* bl, const double* br, const double* bb,
                               const double* bt, const double* bk, const double* bf)
 {
@@ -170,11 +220,18 @@ __global__ void k_find_bvec(Lev L, const double* __restrict__ vel, const double*
     unsigned i = rem - j * nx;
     const long long ng = (long long)(nx + 2) * (ny + 2) * (nz + 2);
     const long long gi = (long long)(i + 1) + (long long)(nx + 2) * ((long long)(j + 1) + (long long)(ny + 2) * (k + 1));
+    double v = (sterm ? sterm[t] : 0.0) + source[gi];
+    // interior cells: the source alone (the face terms below touch boundary cells)
+    if (i > 0 && i + 1 < nx && j > 0 && j + 1 < ny && k > 0 && k + 1 < nz) {
+        b.half(scol(i, j, k))[soff(L, i, j, k)] = v;
+        return;
+    }
+    v = 0.0;
     const double kc = dcoeff[gi];
-    double v = 0.0;
     const double* faceval[6] = {bl, br, bb, bt, bk, bf};
     const unsigned pos[3] = {i, j, k};
     const unsigned len[3] = {nx, ny, nz};
+#pragma unroll
     for (int f = 0; f < 6; f++) {
         const int ax = f >> 1, side = f & 1;
         if (L.per[ax]) continue;

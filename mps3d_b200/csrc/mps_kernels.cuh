@@ -1209,6 +1209,9 @@ __global__ void k_unpack_nat(Lev L, CSplit<T> in, double* __restrict__ g)
 // max |x| over the interior of a ghosted field (x - x(1,1,1) when rel=1),
 // reduced with an integer atomicMax on the bit pattern (valid for >= 0)
 __global__ void k_maxabs(Lev L, const double* __restrict__ g, int rel, unsigned long long* out);
+__global__ void k_maxabs_all(Lev L, const double* __restrict__ vel, const double* __restrict__ reac,
+                             const double* __restrict__ dcoeff, const double* __restrict__ source,
+                             const double* __restrict__ soln, unsigned long long* out);
 
 // update_boundary_ghostvalues (discretepde.f90:1121-1267) + periodic wrap,
 // on a ghosted FP64 field; faces only (edges/corners untouched, as in the

@@ -1003,16 +1003,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     const long long ncell = (long long)L0.nx * L0.ny * L0.nz;
     const long long ng = (long long)(L0.nx + 2) * (L0.ny + 2) * (L0.nz + 2);
     const unsigned mb = std::min<unsigned>(nblk(ncell), 1184);
-    if (in.vel)
-        for (int a = 0; a < 3; a++) { pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.vel + a * ng, 0, dm + 0); CKL(); }
-    if (in.reac) { pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.reac, 0, dm + 1); CKL(); }
-    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.dcoeff, 1, dm + 2);
-    CKL();
-    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.source, 0, dm + 3);
-    CKL();
-    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.soln, 0, dm + 4);
-    CKL();
-    pdl_launch(k_maxabs, mb, TPB, 0, ctx.s, L0, in.dcoeff, 0, dm + 5);
+    pdl_launch(k_maxabs_all, mb, TPB, 0, ctx.s, L0, in.vel, in.reac, in.dcoeff, in.source, in.soln, dm);
     CKL();
     unsigned long long hm[8];
     CK(cudaMemcpyAsync(hm, dm, sizeof(hm), cudaMemcpyDeviceToHost, ctx.s));
