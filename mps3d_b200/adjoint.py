@@ -48,6 +48,7 @@ class OperatorSpec:
     krylov: Optional[str] = None
     maxit: int = 100
     handle: Optional[capi.Handle] = None
+    handle_t: Optional[capi.Handle] = None  # for the transposed solves (None: ``handle``)
 
 
 def _ghosted(t):
@@ -77,7 +78,7 @@ def device_solve(spec: OperatorSpec, rhs, vel_g, dc_g, transpose: bool):
     values."""
     import torch
 
-    h = spec.handle or solver.default_handle()
+    h = (spec.handle_t if transpose and spec.handle_t is not None else spec.handle) or solver.default_handle()
     dev = rhs.device
     shape = (spec.lz + 2, spec.ly + 2, spec.lx + 2)
     src = torch.zeros(shape, dtype=torch.float64, device=dev)
@@ -185,10 +186,22 @@ class ElectronFluxAdjoint:
         self.n_old = t(case["n_old"])
         bc_p = tuple(BC_CODES[c] for c in ["PERI", "PERI", "PERI", "PERI", "DIRC", "DIRC"])
         bc_s = tuple(BC_CODES[c] for c in ["PERI", "PERI", "PERI", "PERI", "ZGRD", "ZGRD"])
+        # A handle keeps the workspace and the captured graphs of one operator
+        # signature; a solve of another signature replaces them.  The device
+        # solves therefore take one handle per operator kind -- Poisson
+        # (``handle``, forward and transposed: the operator is symmetric), SG
+        # forward, SG transposed -- and every solve of a gradient replays its
+        # own graphs.
+        hp = hs = hst = handle
+        if solve_fn is None:
+            d = torch.device(device)
+            di = d.index if d.index is not None else torch.cuda.current_device()
+            hp = handle or capi.Handle(di)
+            hs, hst = capi.Handle(di), capi.Handle(di)
         self.pspec = OperatorSpec(n, n, n, (L, L, L), bc_p, flux=0, tol=tol, precision=poisson_precision,
-                                  handle=handle)
+                                  handle=hp)
         self.sspec = OperatorSpec(n, n, n, (L, L, L), bc_s, flux=1, timederiv=True, dt=self.dt, tol=tol,
-                                  precision=sg_precision, krylov="fgmres", handle=handle)
+                                  precision=sg_precision, krylov="fgmres", handle=hs, handle_t=hst)
         self.solve_fn = solve_fn or linear_solve
         bvec = bvec_fn or self._device_bvec
         zero = np.zeros_like(case["rho"])

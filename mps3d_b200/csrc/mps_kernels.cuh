@@ -853,12 +853,14 @@ struct ProlongDiv {
     FastDiv nh;   // by the cells of one colour per row, (nx+1)/2
     FastDiv gin;  // by the groups whose cells all lie in the box along x
     FastDiv gout; // by the other groups of a row
+    FastDiv yin2; // by the row pairs of the box along y
     int g_lo, g_hi;  // the groups in the box: [g_lo, g_hi]
 };
 
 // the four parts of a prolongation in one launch: consecutive block ranges
 // take modes 0, 3, 1, 2 (cnt: threads of each part; mode 2 has its own box
-// and divisors)
+// and divisors).  Mode 0 threads take W cells of a 2 x 2 block of rows (the
+// box starts at odd j, k and spans an even number of rows along y and z).
 struct ProlongParts {
     unsigned cnt[4];   // modes 0, 3, 1, 2
     unsigned blk0[5];  // first block of each part, and the total
@@ -892,17 +894,20 @@ __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSp
         // regular, no divergent path in the warp), mode 3: the row ends
         unsigned r, g;
         if (mode == 0) {
-            r = dv.gin.div(t);
+            r = dv.gin.div(t);  // the row pair
             g = dv.g_lo + (t - r * dv.gin.d);
+            const unsigned kk = dv.yin2.div(r);
+            k = bx.lo[2] + 2 * (int)kk;
+            j = bx.lo[1] + 2 * (int)(r - kk * dv.yin2.d);
         } else {
-            r = dv.gout.div(t);
+            r = dv.gout.div(t);  // the row
             const unsigned e = t - r * dv.gout.d;
             g = e < (unsigned)dv.g_lo ? e : dv.g_hi + 1 + (e - dv.g_lo);
+            const unsigned kk = dv.yin.div(r);
+            k = bx.lo[2] + (int)kk;
+            j = bx.lo[1] + (int)(r - kk * dv.yin.d);
         }
         h0 = W * (int)g;
-        const unsigned kk = dv.yin.div(r);
-        k = bx.lo[2] + (int)kk;
-        j = bx.lo[1] + (int)(r - kk * dv.yin.d);
         c = 1;
         nel = W;
     } else if (mode == 1) {
@@ -943,46 +948,65 @@ __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSp
         return;
     }
     (void)nel;
-    const int q = (j + k + c) & 1;
-    const long long o0 = h0 + (long long)F.P * (j + (long long)F.ny * k);
-    const bool yreg = mode != 1, zreg = mode != 1;
-    int y0, y1, z0, z1;
-    T ty, tz;
-    lin_axis<T>(X, 1, j, yreg, y0, y1, ty);
-    lin_axis<T>(X, 2, k, zreg, z0, z1, tz);
-    T* base = u.half(c) + o0;
     if (mode == 0) {
-        // all W cells regular: coarse x = X0 .. X0+W of four coarse rows,
-        // shared by the W cells (same lerp order as trilinear())
-        const T tx = q ? T(0.25) : T(0.75);
-        const int X0 = h0 - 1 + q;
-        VecW<T, W> xi[2][2];
+        // rows (j, k), (j+1, k), (j, k+1), (j+1, k+1) with j, k odd: along y
+        // both rows lie between coarse rows J0 and J0+1 (weights 0.25 for j,
+        // 0.75 for j+1), likewise along z; all 4W cells regular.  The four
+        // coarse rows, interpolated along x once for each cell parity, serve
+        // the four fine rows (same lerp order as trilinear())
+        const int J0 = j >> 1, K0 = k >> 1;
+        const int q0 = (j + k + c) & 1;  // rows (j+1, k) and (j, k+1) have 1 - q0
+        VecW<T, W> xi[2][2][2];          // [parity][y][z]
 #pragma unroll
         for (int zz = 0; zz < 2; zz++)
 #pragma unroll
             for (int yy = 0; yy < 2; yy++) {
-                const int y = yy ? y1 : y0, z = zz ? z1 : z0;
-                const int rb = C.P * (y + C.ny * z);
-                const int par = (y + z) & 1;
-                T cv[W + 1];
+                const int rb = C.P * ((J0 + yy) + C.ny * (K0 + zz));
+                const int par = (J0 + yy + K0 + zz) & 1;
+                T cv[W + 2];  // coarse x = h0 - 1 .. h0 + W
 #pragma unroll
-                for (int m = 0; m <= W; m++) {
-                    const int x = X0 + m;
+                for (int m = 0; m < W + 2; m++) {
+                    const int x = h0 - 1 + m;
                     cv[m] = __ldg(&e.half((x + par) & 1)[(x >> 1) + rb]);
                 }
 #pragma unroll
-                for (int el = 0; el < W; el++) xi[yy][zz].v[el] = cv[el] + tx * (cv[el + 1] - cv[el]);
-            }
-        VecW<T, W> u4 = ldv<T, W>(base);
+                for (int qq = 0; qq < 2; qq++) {
+                    const T tx = qq ? T(0.25) : T(0.75);
 #pragma unroll
-        for (int el = 0; el < W; el++) {
-            const T a0 = xi[0][0].v[el] + ty * (xi[1][0].v[el] - xi[0][0].v[el]);
-            const T a1 = xi[0][1].v[el] + ty * (xi[1][1].v[el] - xi[0][1].v[el]);
-            u4.v[el] += a0 + tz * (a1 - a0);
-        }
-        stv<T, W>(base, u4);
+                    for (int el = 0; el < W; el++)
+                        xi[qq][yy][zz].v[el] = cv[el + qq] + tx * (cv[el + qq + 1] - cv[el + qq]);
+                }
+            }
+#pragma unroll
+        for (int dk = 0; dk < 2; dk++)
+#pragma unroll
+            for (int dj = 0; dj < 2; dj++) {
+                const bool qq = (q0 ^ dj ^ dk) != 0;  // selects, not an index: xi stays in registers
+                const T ty = dj ? T(0.75) : T(0.25), tz = dk ? T(0.75) : T(0.25);
+                T* base = u.half(c) + h0 + (long long)F.P * ((j + dj) + (long long)F.ny * (k + dk));
+                VecW<T, W> u4 = ldv<T, W>(base);
+#pragma unroll
+                for (int el = 0; el < W; el++) {
+                    const T x00 = qq ? xi[1][0][0].v[el] : xi[0][0][0].v[el];
+                    const T x10 = qq ? xi[1][1][0].v[el] : xi[0][1][0].v[el];
+                    const T x01 = qq ? xi[1][0][1].v[el] : xi[0][0][1].v[el];
+                    const T x11 = qq ? xi[1][1][1].v[el] : xi[0][1][1].v[el];
+                    const T a0 = x00 + ty * (x10 - x00);
+                    const T a1 = x01 + ty * (x11 - x01);
+                    u4.v[el] += a0 + tz * (a1 - a0);
+                }
+                stv<T, W>(base, u4);
+            }
         return;
     }
+    const int q = (j + k + c) & 1;
+    const long long o0 = h0 + (long long)F.P * (j + (long long)F.ny * k);
+    const bool reg = mode != 1;  // mode 3 rows lie in the box along y and z
+    int y0, y1, z0, z1;
+    T ty, tz;
+    lin_axis<T>(X, 1, j, reg, y0, y1, ty);
+    lin_axis<T>(X, 2, k, reg, z0, z1, tz);
+    T* base = u.half(c) + o0;
 #pragma unroll
     for (int el = 0; el < W; el++) {
         const int i = 2 * (h0 + el) + q;

@@ -517,6 +517,9 @@ static bool prolong_box(const Lev& F, const Lev& C, const Xfer& X, Box& b)
         const int creg = nc[a] - ((nf[a] != 2 * nc[a] || !F.uniform) ? 1 : 0);
         b.lo[a] = 1;
         b.hi[a] = 2 * creg - 3;
+        // along y and z the regular rows go in pairs (2J+1, 2J+2) between
+        // coarse rows J and J+1: an odd count leaves its last row to the shell
+        if (a > 0 && ((b.hi[a] - b.lo[a] + 1) & 1)) b.hi[a]--;
         if (b.hi[a] < b.lo[a]) return false;
     }
     return true;
@@ -639,12 +642,13 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     Box pb;
     if (o->nu2 >= 1 && L.nx >= 16 && prolong_box(L, C, ctx.xf[l], pb)) {
         constexpr int W = 4;
-        const long long G = L.P / W;
+        const long long G = (L.nh + W - 1) / W;  // groups holding a cell (the rest of the P / W are pads)
         const long long rall = (long long)L.ny * L.nz;
         const long long rin = (long long)(pb.hi[1] - pb.lo[1] + 1) * (pb.hi[2] - pb.lo[2] + 1);
         ProlongDiv dv;
         dv.g.init((unsigned)G);
         dv.yin.init((unsigned)(pb.hi[1] - pb.lo[1] + 1));
+        dv.yin2.init((unsigned)(pb.hi[1] - pb.lo[1] + 1) / 2);
         dv.nh.init((unsigned)((L.nx + 1) / 2));
         // groups with every cell in the box for both row parities: 2Wg >= lo,
         // 2W(g+1) - 1 <= hi
@@ -667,7 +671,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         ProlongDiv sv = dv;
         sv.yin.init((unsigned)(sb.hi[1] - sb.lo[1] + 1));
         ProlongParts pp;
-        pp.cnt[0] = (unsigned)(rin * gin);
+        pp.cnt[0] = (unsigned)(rin / 4 * gin);  // 2 x 2 row blocks
         pp.cnt[1] = (unsigned)(rin * (G - gin));
         pp.cnt[2] = (unsigned)((rall - rin) * G);
         pp.cnt[3] = odd_periodic(L) ? (unsigned)((rall - rin2) * ((L.nx + 1) / 2) + (sx ? 2 * rin2 : 0)) : 0u;
@@ -1172,7 +1176,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     gk.nu2 = o->nu2;
     gk.nlev = nl;
     gk.flux = o->flux;
-    gk.transpose = o->transpose;
+    gk.transpose = sig.transpose;  // a symmetric operator's transposed solve replays the forward graphs
     gk.kc = sig.kuni ? k0 : 0.0;
     gk.dexc = sig.has_reac ? 0.0 : dtinv;
     gk.ws = ctx.ar.blocks.empty() ? nullptr : ctx.ar.blocks[0];
