@@ -336,6 +336,7 @@ struct BatchState {
 static int sub_init(Ctx& parent, Ctx& sc)
 {
     sc.dev = parent.dev;
+    sc.nsm = parent.nsm;
     sc.s = parent.s;
     if (cudaEventCreate(&sc.e0) != cudaSuccess || cudaEventCreate(&sc.e1) != cudaSuccess ||
         cudaMallocHost((void**)&sc.hpin, sizeof(double) * 512) != cudaSuccess ||
@@ -636,7 +637,8 @@ static std::vector<long long> batch_key(BatchState& B, const BatchPlan<T>& P, co
     return k;
 }
 
-static const int kTuneGrids[] = {148, 296, 592, 1184, 2368, 4736};
+// candidate grids, in blocks per SM
+static const int kTuneBlocksPerSM[] = {1, 2, 4, 8, 16, 32};
 
 // time the candidate grids on the colour pass of every depth (the passes
 // read and write only the V-cycle state, which the first pass of a solve
@@ -645,7 +647,7 @@ template <class T>
 static int autotune(Ctx& ctx, BatchState& B, BatchPlan<T>& P, const unsigned char* ddesc, const int* dtask)
 {
     const int D = P.maxdepth;
-    B.tune_grid.assign(D + 1, 1184);
+    B.tune_grid.assign(D + 1, 8 * ctx.nsm);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
@@ -655,8 +657,9 @@ static int autotune(Ctx& ctx, BatchState& B, BatchPlan<T>& P, const unsigned cha
             if (s.kind == B_COLOUR && s.depth == d && s.zs == 0) { st = &s; break; }
         if (!st) continue;
         float best = 1e30f;
-        for (int g : kTuneGrids) {
-            if (g > std::max(st->total, 148)) break;
+        for (int bps : kTuneBlocksPerSM) {
+            const int g = bps * ctx.nsm;
+            if (g > std::max(st->total, ctx.nsm)) break;
             BStep s2 = *st;
             s2.grid = g;
             launch_step<T>(ctx.s, s2, ddesc, dtask, B.dst, B.dpart);  // warm

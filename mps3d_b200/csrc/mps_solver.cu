@@ -159,6 +159,7 @@ struct BatchState;
 
 struct Ctx {
     int dev = 0;
+    int nsm = 148;  // streaming multiprocessors of the device
     BatchState* batch = nullptr;  // batched solves (mps_linsolve_batched_dev)
     long long launches = 0;
     Prof prof;
@@ -720,7 +721,12 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             constexpr int W = ColourShape<T>::W;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
-            const unsigned nbv = std::min<unsigned>(nblk((long long)(L.P / W) * L.rows), 148 * 8);
+            // grid-stride over one wave of resident blocks: no partial last
+            // wave, and few partials for the norm reduction (measured at 257^3:
+            // 193 us against 220 us for 8 blocks per SM and 233 us for one
+            // thread per group)
+            const unsigned nall = nblk((long long)(L.P / W) * L.rows);
+            const unsigned nbv = std::min<unsigned>(nall, (unsigned)(ctx.nsm * ColourShape<T>::MINB));
             // both colours in one pass (f and rout as split bases, halves L.half apart)
             pdl_launch(k_residv<T, W, R>, nbv, TPB, 0, ctx.s, L, op, -1, u, f.half(0), rout.c[0] ? rout.half(0) : nullptr,
                                                        ctx.rb, 0, dg);
@@ -1505,6 +1511,10 @@ int mps_create(mps_handle* h, int device)
     if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) { delete H; return MPS_ERR_CUDA; }
     if (cudaSetDevice(dev) != cudaSuccess) { delete H; return MPS_ERR_CUDA; }
     ctx.dev = dev;
+    if (cudaDeviceGetAttribute(&ctx.nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || ctx.nsm < 1) {
+        delete H;
+        return MPS_ERR_CUDA;
+    }
     if (cudaStreamCreateWithFlags(&ctx.s, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx.e0) != cudaSuccess || cudaEventCreate(&ctx.e1) != cudaSuccess ||
         cudaMallocHost((void**)&ctx.hpin, sizeof(double) * 512) != cudaSuccess ||
