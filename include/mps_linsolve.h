@@ -4,7 +4,18 @@
  *
  * The entry points replace the solver calls of the reference's equation
  * modules (plain C types only: no CUDA or torch types in the signatures; the
- * stream of the *_dev variants is a cudaStream_t passed as void*):
+ * stream of the *_dev variants is a cudaStream_t passed as void*).
+ *
+ * Streams: a handle runs its work on its own non-blocking stream.  A *_dev
+ * call given the caller's stream orders that work after what the caller's
+ * stream has queued (the inputs) and makes the caller's stream wait for it
+ * (the outputs).  NULL means the handle's stream itself, with no ordering
+ * against any other stream; for the legacy default stream (torch's default
+ * stream, among others) pass cudaStreamLegacy, ((void*)0x1), not NULL.
+ * Entry points without a handle queue their work on `stream` itself (NULL is
+ * then the legacy default stream).
+ *
+ * Entry points:
  *
  *   mps_vcycle_once   <- perform_vcycle, mgridlib/mgridsteps.f90:384-417
  *                        (one call, same arguments and in/out meaning)
@@ -146,7 +157,8 @@ int mps_linsolve(mps_handle h, const mps_grid* g, int timederiv, double dt,
                  const double* mgridsterm, double* soln, const mps_solver_opts* opts,
                  mps_solve_info* info);
 
-/* Same with device pointers on `stream` (cudaStream_t, NULL = handle's stream);
+/* Same with device pointers, ordered with `stream` (cudaStream_t; NULL = the
+ * handle's stream, unordered with other streams; see the top of this file);
  * no host<->device copies of the fields. */
 int mps_linsolve_dev(mps_handle h, const mps_grid* g, int timederiv, double dt,
                      const double* vel, const double* dcoeff, const double* reac,

@@ -93,7 +93,7 @@ def device_solve(spec: OperatorSpec, rhs, vel_g, dc_g, transpose: bool):
     r = rhs.contiguous()
     st = h._lib.mps_linsolve_dev(h.h, C.byref(_grid(spec)), int(spec.timederiv), float(spec.dt), _ptr(vel_g),
                                  _ptr(dc_g), None, _ptr(src), bcc, bcv, _ptr(r), _ptr(x), C.byref(o),
-                                 C.byref(info), C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+                                 C.byref(info), C.c_void_p(capi.stream_arg(torch.cuda.current_stream(dev))))
     if st != 0:
         raise capi.SolverError(st, h.last_error())
     return x[1:-1, 1:-1, 1:-1].contiguous()
@@ -111,7 +111,7 @@ def device_vjp(spec: OperatorSpec, vel_g, dc_g, lam, u):
     u = u.contiguous()
     st = capi.load().mps_operator_vjp_dev(C.byref(_grid(spec)), _ptr(vel_g), _ptr(dc_g), (C.c_int * 6)(*spec.bc),
                                           _ptr(lam), _ptr(u), C.byref(o), _ptr(gv), _ptr(gd), None,
-                                          C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+                                          C.c_void_p(capi.stream_arg(torch.cuda.current_stream(dev))))
     if st != 0:
         raise capi.SolverError(st, "mps_operator_vjp_dev")
     return gv, gd

@@ -152,6 +152,28 @@ class SolverError(RuntimeError):
         self.status = status
 
 
+# cudaStreamLegacy: the legacy default stream, named by a handle that is not NULL
+CUDA_STREAM_LEGACY = 1
+
+
+def stream_arg(stream=None) -> int:
+    """The ``stream`` argument of the *_dev entry points for a torch stream (or
+    its ``cuda_stream`` integer; None = torch's current stream).
+
+    torch's default stream is the legacy default stream, whose ``cuda_stream``
+    is 0.  The library reads NULL as "the handle's own stream", a non-blocking
+    stream that is ordered with no other stream, so a call given 0 would read
+    inputs that torch has not finished writing and return before its outputs
+    are written as torch sees them.  0 is therefore passed as cudaStreamLegacy,
+    which the library orders its work after and before like any caller stream."""
+    if stream is None:
+        import torch
+
+        stream = torch.cuda.current_stream()
+    s = stream if isinstance(stream, int) else int(stream.cuda_stream)
+    return s if s != 0 else CUDA_STREAM_LEGACY
+
+
 class Handle:
     """Owns an mps_handle (a CUDA stream and a device workspace)."""
 

@@ -1758,6 +1758,14 @@ int mps_apply_A_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, c
     double* tmp = nullptr;
     double* zsrc = nullptr;
     cudaStream_t s = ctx.s;
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user && user != s) {  // soln is read below, before the solve orders the streams
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return MPS_ERR_CUDA;
+        cudaEventRecord(ev, user);
+        cudaStreamWaitEvent(s, ev, 0);
+        cudaEventDestroy(ev);
+    }
     if (cudaMallocAsync((void**)&tmp, sizeof(double) * ng * 2, s) != cudaSuccess) return MPS_ERR_CUDA;
     zsrc = tmp + ng;
     cudaMemcpyAsync(tmp, soln, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);

@@ -139,7 +139,7 @@ def linsolve_dev(dp: DeviceProblem, soln, handle: Optional[capi.Handle] = None, 
     p = dp.prob
     o = make_opts(flux=p.flux, **kw)
     info = capi.Info()
-    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    s = capi.stream_arg(stream)
     st = h._lib.mps_linsolve_dev(h.h, C.byref(_grid(p)), int(p.timederiv), float(p.dt), dp.ptr(dp.vel),
                                  dp.ptr(dp.dcoeff), dp.ptr(dp.reac), dp.ptr(dp.source), _bc(p), dp.bcv(),
                                  dp.ptr(mgridsterm), dp.ptr(soln), C.byref(o), C.byref(info), C.c_void_p(s))
@@ -180,7 +180,7 @@ def linsolve_batched_dev(dps, solns, handle: Optional[capi.Handle] = None, strea
         keep.append((dp, x))
     o = make_opts(**kw)
     infos = (capi.Info * n)()
-    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    s = capi.stream_arg(stream)
     st = h._lib.mps_linsolve_batched_dev(h.h, n, descs, C.byref(o), infos, C.c_void_p(s))
     if st not in (0, capi.MPS_ERR_NOT_CONVERGED):
         raise capi.SolverError(st, h.last_error())
@@ -197,7 +197,7 @@ def apply_A_dev(dp: DeviceProblem, soln, handle: Optional[capi.Handle] = None, t
     o = make_opts(flux=p.flux, transpose=transpose)
     st = h._lib.mps_apply_A_dev(h.h, C.byref(_grid(p)), int(p.timederiv), float(p.dt), dp.ptr(dp.vel),
                                 dp.ptr(dp.dcoeff), dp.ptr(dp.reac), _bc(p), dp.ptr(soln), dp.ptr(out), C.byref(o),
-                                C.c_void_p(torch.cuda.current_stream().cuda_stream))
+                                C.c_void_p(capi.stream_arg()))
     if st != 0:
         raise capi.SolverError(st, h.last_error())
     return out
@@ -215,7 +215,7 @@ def apply_A_noalloc(dp: DeviceProblem, soln, out=None, transpose=False, stream=N
     if out is None:
         out = torch.empty(p.shape, dtype=torch.float64, device=soln.device)
     o = make_opts(flux=p.flux, transpose=transpose)
-    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    s = capi.stream_arg(stream)
     st = capi.load().mps_apply_A_noalloc(C.byref(_grid(p)), int(p.timederiv), float(p.dt), dp.ptr(dp.vel),
                                          dp.ptr(dp.dcoeff), dp.ptr(dp.reac), _bc(p), dp.ptr(soln), dp.ptr(out),
                                          C.byref(o), C.c_void_p(s))
@@ -233,7 +233,7 @@ def find_bvec_dev(dp: DeviceProblem, handle: Optional[capi.Handle] = None, mgrid
     o = make_opts(flux=p.flux)
     st = h._lib.mps_find_bvec_dev(h.h, C.byref(_grid(p)), dp.ptr(dp.vel), dp.ptr(dp.dcoeff), dp.ptr(dp.source),
                                   _bc(p), dp.bcv(), dp.ptr(mgridsterm), dp.ptr(out), C.byref(o),
-                                  C.c_void_p(torch.cuda.current_stream().cuda_stream))
+                                  C.c_void_p(capi.stream_arg()))
     if st != 0:
         raise capi.SolverError(st, h.last_error())
     return out
@@ -245,7 +245,7 @@ def fill_ghosts_dev(dp: DeviceProblem, soln, handle: Optional[capi.Handle] = Non
     h = handle or default_handle()
     p = dp.prob
     st = h._lib.mps_fill_ghosts_dev(h.h, C.byref(_grid(p)), _bc(p), dp.bcv(), dp.ptr(soln),
-                                    C.c_void_p(torch.cuda.current_stream().cuda_stream))
+                                    C.c_void_p(capi.stream_arg()))
     if st != 0:
         raise capi.SolverError(st, h.last_error())
     return soln

@@ -52,3 +52,16 @@ def test_no_cpu_fallback(monkeypatch, tmp_path):
     monkeypatch.setattr(capi, "_lib", None)
     with pytest.raises(RuntimeError):
         capi.load()
+
+
+def test_stream_argument_for_the_legacy_default_stream():
+    # torch's default stream is the legacy default stream (cuda_stream 0); the
+    # library reads NULL as the handle's own stream, so 0 goes out as
+    # cudaStreamLegacy and other streams pass through unchanged
+    assert capi.stream_arg(0) == capi.CUDA_STREAM_LEGACY == 1
+    assert capi.stream_arg(0x7F00AB12) == 0x7F00AB12
+
+    class FakeStream:
+        cuda_stream = 0
+
+    assert capi.stream_arg(FakeStream()) == 1
