@@ -122,13 +122,12 @@ __device__ __forceinline__ VecW<T, W> ldv(const T* p)
             const double2 a = __ldg(reinterpret_cast<const double2*>(p));
             r.v[0] = a.x; r.v[1] = a.y;
         }
-    } else if constexpr (sizeof(T) * W == 8) {
+    } else if constexpr (sizeof(T) * W == 8 && sizeof(T) == 4) {
         const float2 a = __ldg(reinterpret_cast<const float2*>(p));
         r.v[0] = a.x; r.v[1] = a.y;
     } else {
-        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
-        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-        r.v[0] = a.x; r.v[1] = a.y; r.v[2] = b.x; r.v[3] = b.y;
+        static_assert(W == 1, "vector width: 1, 2, 4 or 8 floats; 1, 2 or 4 doubles");
+        r.v[0] = __ldg(p);
     }
     return r;
 }
@@ -148,11 +147,11 @@ __device__ __forceinline__ void stv(T* p, const VecW<T, W>& r)
     } else if constexpr (sizeof(T) * W == 16) {
         if constexpr (sizeof(T) == 4) *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
         else *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
-    } else if constexpr (sizeof(T) * W == 8) {
+    } else if constexpr (sizeof(T) * W == 8 && sizeof(T) == 4) {
         *reinterpret_cast<float2*>(p) = make_float2(r.v[0], r.v[1]);
     } else {
-        reinterpret_cast<double2*>(p)[0] = make_double2(r.v[0], r.v[1]);
-        reinterpret_cast<double2*>(p)[1] = make_double2(r.v[2], r.v[3]);
+        static_assert(W == 1, "vector width: 1, 2, 4 or 8 floats; 1, 2 or 4 doubles");
+        p[0] = r.v[0];
     }
 }
 template <class T, int W>
@@ -366,9 +365,31 @@ struct ColourShape {
     static constexpr int W = sizeof(T) == 4 ? MPS_COLOUR_W32 : MPS_COLOUR_W64;
     static constexpr int MINB = sizeof(T) == 4 ? MPS_COLOUR_MINB32 : MPS_COLOUR_MINB64;
 };
+// the colour pass of the levels below the finest: half the width and 4
+// blocks per SM (at 128^3 the finest shape's 512 blocks are 1.15 waves of
+// 3 per SM); measured on the 257^3 plasma Poisson solve: 14.76 ms mixed /
+// 25.48 ms FP64 against 15.19 / 25.87 with the finest shape, 4 blocks per
+// SM at the finest width no better, 2 FP32 / 1 FP64 cells worse
+#ifndef MPS_COARSE_W32
+#define MPS_COARSE_W32 4
+#endif
+#ifndef MPS_COARSE_MINB32
+#define MPS_COARSE_MINB32 4
+#endif
+#ifndef MPS_COARSE_W64
+#define MPS_COARSE_W64 2
+#endif
+#ifndef MPS_COARSE_MINB64
+#define MPS_COARSE_MINB64 4
+#endif
+template <class T>
+struct CoarseShape {
+    static constexpr int W = sizeof(T) == 4 ? MPS_COARSE_W32 : MPS_COARSE_W64;
+    static constexpr int MINB = sizeof(T) == 4 ? MPS_COARSE_MINB32 : MPS_COARSE_MINB64;
+};
 
-template <class T, int W, class U>
-__global__ void __launch_bounds__(TPB, ColourShape<T>::MINB) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
+template <class T, int W, class U, int MB = ColourShape<T>::MINB>
+__global__ void __launch_bounds__(TPB, MB) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
                                                     const T* __restrict__ f, FastDiv divG)
 {
     pdl_wait();
@@ -391,8 +412,19 @@ __global__ void __launch_bounds__(TPB, ColourShape<T>::MINB) k_colourv(Lev L, KO
 // (u, f of type T), optional r out (type R, split half c), and the sums of
 // r^2 and f^2 reduced deterministically (accumulate = add to rb.out, for the
 // second colour)
+#ifndef MPS_RESID_W64
+#define MPS_RESID_W64 MPS_COLOUR_W64
+#endif
+#ifndef MPS_RESID_MINB64
+#define MPS_RESID_MINB64 MPS_COLOUR_MINB64
+#endif
+template <class T>
+struct ResidShape {
+    static constexpr int W = sizeof(T) == 4 ? MPS_COLOUR_W32 : MPS_RESID_W64;
+    static constexpr int MINB = sizeof(T) == 4 ? MPS_COLOUR_MINB32 : MPS_RESID_MINB64;
+};
 template <class T, int W, class R>
-__global__ void __launch_bounds__(TPB, ColourShape<T>::MINB) k_residv(Lev L, KOp<T> op, int c, CSplit<T> u,
+__global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv(Lev L, KOp<T> op, int c, CSplit<T> u,
                                                                        const T* __restrict__ f, R* __restrict__ rout,
                                                                        RedBuf rb, int accumulate, FastDiv divG)
 {
@@ -541,10 +573,53 @@ struct Box {
 
 // the fused residual + restriction keeps 4 cells per thread (its thread
 // holds the sums of four fine rows; 8 FP32 cells spill)
+#ifndef MPS_RESTRICT_W64
+#define MPS_RESTRICT_W64 4
+#endif
+#ifndef MPS_RESTRICT_MINB64
+#define MPS_RESTRICT_MINB64 3
+#endif
+#ifndef MPS_RESTRICT_W32
+#define MPS_RESTRICT_W32 4
+#endif
+// prolongation: 2 cells per thread (measured at 257^3: 41.3 / 59.4 us FP32 /
+// FP64 against 45.7 / 73.9 with 4 and 87 with 8 FP32 cells)
+#ifndef MPS_PROLONG_W32
+#define MPS_PROLONG_W32 2
+#endif
+#ifndef MPS_PROLONG_W64
+#define MPS_PROLONG_W64 2
+#endif
 template <class T>
 struct RestrictShape {
-    static constexpr int W = 4;
-    static constexpr int MINB = sizeof(T) == 4 ? 4 : 3;
+    static constexpr int W = sizeof(T) == 4 ? MPS_RESTRICT_W32 : MPS_RESTRICT_W64;
+    static constexpr int MINB = sizeof(T) == 4 ? 4 : MPS_RESTRICT_MINB64;
+};
+// cells per thread of the prolongation bulk on the finest level
+template <class T>
+struct ProlongShape {
+    static constexpr int W = sizeof(T) == 4 ? MPS_PROLONG_W32 : MPS_PROLONG_W64;
+};
+// restriction and prolongation from the levels below the finest: 2 cells
+// per thread (measured on the 257^3 plasma Poisson solve: 14.49 ms mixed /
+// 25.03 ms FP64 against 14.76 / 25.45 with 4; 1 cell per thread within
+// noise of 2)
+#ifndef MPS_XFER_COARSE_W32
+#define MPS_XFER_COARSE_W32 2
+#endif
+#ifndef MPS_XFER_COARSE_W64
+#define MPS_XFER_COARSE_W64 2
+#endif
+#ifndef MPS_XFER_COARSE_MINB32
+#define MPS_XFER_COARSE_MINB32 4
+#endif
+#ifndef MPS_XFER_COARSE_MINB64
+#define MPS_XFER_COARSE_MINB64 4
+#endif
+template <class T>
+struct CoarseXferShape {
+    static constexpr int W = sizeof(T) == 4 ? MPS_XFER_COARSE_W32 : MPS_XFER_COARSE_W64;
+    static constexpr int MINB = sizeof(T) == 4 ? MPS_XFER_COARSE_MINB32 : MPS_XFER_COARSE_MINB64;
 };
 
 template <class T, int W>
@@ -645,8 +720,8 @@ __device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op,
 
 // bulk and shell in one launch: blocks [0, nb_bulk) take the bulk rows,
 // the rest the shell cells
-template <class T, int W>
-__global__ void __launch_bounds__(TPB, RestrictShape<T>::MINB) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
+template <class T, int W, int MB>
+__global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
                                                                                  const T* __restrict__ fred, Lev C,
                                                                                  Split<T> fc, FastDiv divG, Box bx,
                                                                                  unsigned nb_bulk, int geom,

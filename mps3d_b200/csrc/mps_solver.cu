@@ -544,21 +544,29 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (L.uniform || L.nx >= 16) {
             // vector kernel, W cells per thread (faces at a merged last cell
-            // take their own coefficients inside the row evaluation)
-            constexpr int W = ColourShape<T>::W;
-            FastDiv dg;
-            dg.init((unsigned)(L.P / W));
-            const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
-            if (zero_state == 2) {
-                pdl_launch(k_colourv<T, W, ZeroU<T>>, nbv, TPB, 0, ctx.s, L, op, c, ZeroU<T>(), out, fh, dg);
-            } else if (zero_state == 1) {
-                OtherOnlyU<T> u;
-                u.c = c;
-                u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
-                pdl_launch(k_colourv<T, W, OtherOnlyU<T>>, nbv, TPB, 0, ctx.s, L, op, c, u, out, fh, dg);
-            } else {
-                pdl_launch(k_colourv<T, W, CSplit<T>>, nbv, TPB, 0, ctx.s, L, op, c, ccur(H, L, l), out, fh, dg);
-            }
+            // take their own coefficients inside the row evaluation); the
+            // levels below the finest have their own shape
+            auto launch = [&](auto wc, auto mbc) {
+                constexpr int W = decltype(wc)::value, MB = decltype(mbc)::value;
+                FastDiv dg;
+                dg.init((unsigned)(L.P / W));
+                const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
+                if (zero_state == 2) {
+                    pdl_launch(k_colourv<T, W, ZeroU<T>, MB>, nbv, TPB, 0, ctx.s, L, op, c, ZeroU<T>(), out, fh, dg);
+                } else if (zero_state == 1) {
+                    OtherOnlyU<T> u;
+                    u.c = c;
+                    u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
+                    pdl_launch(k_colourv<T, W, OtherOnlyU<T>, MB>, nbv, TPB, 0, ctx.s, L, op, c, u, out, fh, dg);
+                } else {
+                    pdl_launch(k_colourv<T, W, CSplit<T>, MB>, nbv, TPB, 0, ctx.s, L, op, c, ccur(H, L, l), out, fh,
+                               dg);
+                }
+            };
+            if (l == 0)
+                launch(std::integral_constant<int, ColourShape<T>::W>(), std::integral_constant<int, ColourShape<T>::MINB>());
+            else
+                launch(std::integral_constant<int, CoarseShape<T>::W>(), std::integral_constant<int, CoarseShape<T>::MINB>());
             if (l == ctx.prof.level) prof_end(ctx);
             CKL();
             if (c == 0) H.ri[l] ^= 1;
@@ -617,14 +625,20 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         if (o->nu1 >= 1 && L.nx >= 16 && restrict_box(L, C, bx)) {
             // red residual of the bulk's children restricted in registers, the
             // shell with the general body
-            constexpr int W = RestrictShape<T>::W;
-            FastDiv dg;
-            dg.init((unsigned)(L.P / W));
-            const long long nt = (long long)C.rows * (L.P / W);
-            const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
-            const unsigned nbb = nblk(nt), nbs = shell > 0 ? nblk(8 * shell) : 0;
-            pdl_launch(k_resid_restrict_v<T, W>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l), H.F[l], C,
-                       split<T>(H.F[l + 1], C), dg, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
+            auto launch = [&](auto wc, auto mbc) {
+                constexpr int W = decltype(wc)::value, MB = decltype(mbc)::value;
+                FastDiv dg;
+                dg.init((unsigned)(L.P / W));
+                const long long nt = (long long)C.rows * (L.P / W);
+                const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
+                const unsigned nbb = nblk(nt), nbs = shell > 0 ? nblk(8 * shell) : 0;
+                pdl_launch(k_resid_restrict_v<T, W, MB>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l), H.F[l], C,
+                           split<T>(H.F[l + 1], C), dg, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
+            };
+            if (l == 0)
+                launch(std::integral_constant<int, RestrictShape<T>::W>(), std::integral_constant<int, RestrictShape<T>::MINB>());
+            else
+                launch(std::integral_constant<int, CoarseXferShape<T>::W>(), std::integral_constant<int, CoarseXferShape<T>::MINB>());
             CKL();
             done = true;
         }
@@ -641,8 +655,8 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     // ones, so only black cells need the correction (unless an odd periodic
     // seam makes red cells read red neighbours)
     Box pb;
-    if (o->nu2 >= 1 && L.nx >= 16 && prolong_box(L, C, ctx.xf[l], pb)) {
-        constexpr int W = 4;
+    auto prolong_bulk = [&](auto wc) {
+        constexpr int W = decltype(wc)::value;
         const long long G = (L.nh + W - 1) / W;  // groups holding a cell (the rest of the P / W are pads)
         const long long rall = (long long)L.ny * L.nz;
         const long long rin = (long long)(pb.hi[1] - pb.lo[1] + 1) * (pb.hi[2] - pb.lo[2] + 1);
@@ -680,6 +694,10 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         for (int q = 0; q < 4; q++) pp.blk0[q + 1] = pp.blk0[q] + nblk(pp.cnt[q]);
         pdl_launch(k_prolong_v<T, W>, pp.blk0[4], TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
                    pb, dv, sb, sv, pp);
+    };
+    if (o->nu2 >= 1 && L.nx >= 16 && prolong_box(L, C, ctx.xf[l], pb)) {
+        if (l == 0) prolong_bulk(std::integral_constant<int, ProlongShape<T>::W>());
+        else prolong_bulk(std::integral_constant<int, CoarseXferShape<T>::W>());
         CKL();
     } else if (o->nu2 >= 1) {
         pdl_launch(k_prolong_correct<T>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, L, cur(H, L, l), C,
@@ -718,7 +736,7 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
     prof_begin(ctx, MPS_PROF_RESID);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (L.uniform) {  // vector kernel, one launch per colour, norms accumulated
-            constexpr int W = ColourShape<T>::W;
+            constexpr int W = ResidShape<T>::W;
             FastDiv dg;
             dg.init((unsigned)(L.P / W));
             // grid-stride over one wave of resident blocks: no partial last
@@ -726,7 +744,7 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             // 193 us against 220 us for 8 blocks per SM and 233 us for one
             // thread per group)
             const unsigned nall = nblk((long long)(L.P / W) * L.rows);
-            const unsigned nbv = std::min<unsigned>(nall, (unsigned)(ctx.nsm * ColourShape<T>::MINB));
+            const unsigned nbv = std::min<unsigned>(nall, (unsigned)(ctx.nsm * ResidShape<T>::MINB));
             // both colours in one pass (f and rout as split bases, halves L.half apart)
             pdl_launch(k_residv<T, W, R>, nbv, TPB, 0, ctx.s, L, op, -1, u, f.half(0), rout.c[0] ? rout.half(0) : nullptr,
                                                        ctx.rb, 0, dg);
