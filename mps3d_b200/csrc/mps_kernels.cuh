@@ -219,9 +219,14 @@ __device__ __forceinline__ double dir_c(const Lev& L, int p)
     return dcoef_ax<AX>(L, p);
 }
 
-template <class T, int W, class U, bool UNI = true>
-__device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c, const U& u, int row, int j,
-                                           int k, int h0, int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
+// The x faces and the diagonal of W cells of one row, given the y/z face
+// sums (acc = sum w u_n, wsum = sum w, byz = Dirichlet y/z boundary weight)
+// and the other colour's vectors at the row's own offsets (ax: u, akx: k).
+template <class T, int W, class U, bool UNI>
+__device__ __forceinline__ void row_finish(const Lev& L, const KOp<T>& op, int c, const U& u, int row, int j, int k,
+                                           int h0, int q, int o0, const VecW<T, W>& kc4, const VecW<T, W>& acc,
+                                           const VecW<T, W>& wsum, T byz, const VecW<T, W>& ax,
+                                           const VecW<T, W>& akx, VecW<T, W>& diag, VecW<T, W>& off)
 {
     const int cc = c, oc = c ^ 1;
     const bool kfield = op.k[0] != nullptr;
@@ -229,41 +234,7 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
     const T* us = u.ptr(cc);
     const T* ko = kfield ? sel(op.k, oc) : nullptr;
     const T* ks = kfield ? sel(op.k, cc) : nullptr;
-    // y and z face coefficients of this row (the wrapped neighbour of a
-    // periodic face is the last cell when p = 0)
-    const int ny1 = L.ny - 1, nz1 = L.nz - 1;
-    const T cym = (T)face_c<1, UNI>(L, j, j > 0 ? j - 1 : ny1), cyp = (T)face_c<1, UNI>(L, j, j < ny1 ? j + 1 : 0);
-    const T czm = (T)face_c<2, UNI>(L, k, k > 0 ? k - 1 : nz1), czp = (T)face_c<2, UNI>(L, k, k < nz1 ? k + 1 : 0);
-
-    VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
-    const VecW<T, W> kc4 = kfield ? ldv<T, W>(ks + o0) : zerov<T, W>();
-    int dcount_y = 0, dcount_z = 0;
-    // y and z faces, accumulated one at a time
-#define MPS_YZ(AXV, SV, CF, DC)                                                                               \
-    {                                                                                                         \
-        VecW<T, W> un, kn;                                                                                    \
-        int m, dd;                                                                                            \
-        yz_face<T, W, AXV, SV>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);                       \
-        DC += dd;                                                                                             \
-        if (m) {                                                                                              \
-            _Pragma("unroll") for (int e = 0; e < W; e++)                                                     \
-            {                                                                                                 \
-                const T w = kfield ? (kc4.v[e] + kn.v[e]) * (CF) : (CF);                                      \
-                wsum.v[e] += w;                                                                               \
-                acc.v[e] += w * un.v[e];                                                                      \
-            }                                                                                                 \
-        }                                                                                                     \
-    }
-    MPS_YZ(1, -1, cym, dcount_y)
-    MPS_YZ(1, 1, cyp, dcount_y)
-    MPS_YZ(2, -1, czm, dcount_z)
-    MPS_YZ(2, 1, czp, dcount_z)
-#undef MPS_YZ
-    const T byz = (T)dcount_y * (T)dir_c<1, UNI>(L, j) + (T)dcount_z * (T)dir_c<2, UNI>(L, k);
-
     // x neighbours: A = other colour at o0..o0+W-1, S = o0+W (q=1) or o0-1 (q=0)
-    const VecW<T, W> ax = uo ? ldv<T, W>(uo + o0) : zerov<T, W>();
-    const VecW<T, W> akx = kfield ? ldv<T, W>(ko + o0) : zerov<T, W>();
     const int so = q ? o0 + W : o0 - 1;
     const bool sok = q ? (h0 + W < L.P) : (h0 > 0);
     T sx = T(0), skx = T(0);
@@ -320,6 +291,59 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
         if (kfield) { diag.v[e] = d0 + T(0.5) * ws + kc * bnd; off.v[e] = T(-0.5) * ac; }
         else { diag.v[e] = d0 + kc * (ws + bnd); off.v[e] = -kc * ac; }
     }
+}
+
+// one y or z face of a group added to the face sums (mask 0: no neighbour)
+template <class T, int W>
+__device__ __forceinline__ void add_face(bool kfield, const VecW<T, W>& kc4, const VecW<T, W>& un,
+                                         const VecW<T, W>& kn, int m, T cf, VecW<T, W>& acc, VecW<T, W>& wsum)
+{
+    if (!m) return;
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const T w = kfield ? (kc4.v[e] + kn.v[e]) * cf : cf;
+        wsum.v[e] += w;
+        acc.v[e] += w * un.v[e];
+    }
+}
+
+template <class T, int W, class U, bool UNI = true>
+__device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c, const U& u, int row, int j,
+                                           int k, int h0, int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
+{
+    const int cc = c, oc = c ^ 1;
+    const bool kfield = op.k[0] != nullptr;
+    const T* uo = u.ptr(oc);
+    const T* us = u.ptr(cc);
+    const T* ko = kfield ? sel(op.k, oc) : nullptr;
+    const T* ks = kfield ? sel(op.k, cc) : nullptr;
+    // y and z face coefficients of this row (the wrapped neighbour of a
+    // periodic face is the last cell when p = 0)
+    const int ny1 = L.ny - 1, nz1 = L.nz - 1;
+    const T cym = (T)face_c<1, UNI>(L, j, j > 0 ? j - 1 : ny1), cyp = (T)face_c<1, UNI>(L, j, j < ny1 ? j + 1 : 0);
+    const T czm = (T)face_c<2, UNI>(L, k, k > 0 ? k - 1 : nz1), czp = (T)face_c<2, UNI>(L, k, k < nz1 ? k + 1 : 0);
+
+    VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
+    const VecW<T, W> kc4 = kfield ? ldv<T, W>(ks + o0) : zerov<T, W>();
+    int dcount_y = 0, dcount_z = 0;
+    // y and z faces, accumulated one at a time
+#define MPS_YZ(AXV, SV, CF, DC)                                                                      \
+    {                                                                                                \
+        VecW<T, W> un, kn;                                                                           \
+        int m, dd;                                                                                   \
+        yz_face<T, W, AXV, SV>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);              \
+        DC += dd;                                                                                    \
+        add_face<T, W>(kfield, kc4, un, kn, m, CF, acc, wsum);                                       \
+    }
+    MPS_YZ(1, -1, cym, dcount_y)
+    MPS_YZ(1, 1, cyp, dcount_y)
+    MPS_YZ(2, -1, czm, dcount_z)
+    MPS_YZ(2, 1, czp, dcount_z)
+#undef MPS_YZ
+    const T byz = (T)dcount_y * (T)dir_c<1, UNI>(L, j) + (T)dcount_z * (T)dir_c<2, UNI>(L, k);
+    const VecW<T, W> ax = uo ? ldv<T, W>(uo + o0) : zerov<T, W>();
+    const VecW<T, W> akx = kfield ? ldv<T, W>(ko + o0) : zerov<T, W>();
+    row_finish<T, W, U, UNI>(L, op, c, u, row, j, k, h0, q, o0, kc4, acc, wsum, byz, ax, akx, diag, off);
 }
 
 // decode the group index of a vector launch
@@ -406,6 +430,88 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv(Lev L, KOp<T> op, int c, U 
         res.v[e] = i < L.nx ? gs_value(f4.v[e], diag.v[e], off.v[e]) : T(0);
     }
     stv<T, W>(out + G.o0, res);
+}
+
+// Colour pass marching along z (uniform levels): thread (g, j, chunk) takes
+// W cells of colour c in row j for the planes k0 .. k0+nzc-1 of its chunk.
+// The other colour's vectors of row j at the same group offset serve three
+// planes: at plane k they are the x neighbours, at k-1 and k+1 the z
+// neighbours (cell (i, j, k+-1) has the other colour and split index i>>1).
+// So they are loaded once (one u and one k vector per plane) and carried in
+// registers; the z faces of the first and last plane of the grid (physical
+// faces, periodic wraps, odd seams) go through yz_face.  Same arithmetic,
+// in the same order, as group_rows.
+template <class T, int W, int MB>
+__global__ void __launch_bounds__(TPB, MB) k_colour_march(Lev L, KOp<T> op, int c, CSplit<T> u, T* __restrict__ out,
+                                                          const T* __restrict__ f, FastDiv divG, FastDiv divY,
+                                                          int nzc, unsigned nchunks)
+{
+    pdl_wait();
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    const unsigned r = divG.div(t);  // j + ny * chunk
+    const unsigned chunk = divY.div(r);
+    if (chunk >= nchunks) return;
+    const int j = (int)(r - chunk * (unsigned)L.ny);
+    const int h0 = W * (int)(t - r * divG.d);
+    const int k0 = (int)chunk * nzc, k1 = min(k0 + nzc, L.nz);
+    const int cc = c, oc = c ^ 1;
+    const bool kfield = op.k[0] != nullptr;
+    const T* uo = u.ptr(oc);
+    const T* us = u.ptr(cc);
+    const T* ko = kfield ? sel(op.k, oc) : nullptr;
+    const T* ks = kfield ? sel(op.k, cc) : nullptr;
+    const int ny1 = L.ny - 1, nz1 = L.nz - 1;
+    const T cym = (T)face_c<1, true>(L, j, j > 0 ? j - 1 : ny1), cyp = (T)face_c<1, true>(L, j, j < ny1 ? j + 1 : 0);
+    const T czm = (T)face_c<2, true>(L, 0, nz1), czp = (T)face_c<2, true>(L, 0, 1);
+    const long long plane = (long long)L.P * L.ny;
+    const long long ob = h0 + (long long)L.P * j;  // the group's offset in plane 0
+    auto other = [&](int kk, VecW<T, W>& u4, VecW<T, W>& k4) {
+        u4 = ldv<T, W>(uo + ob + plane * kk);
+        k4 = kfield ? ldv<T, W>(ko + ob + plane * kk) : zerov<T, W>();
+    };
+    VecW<T, W> um, km, uz, kz;  // planes k-1 and k
+    int mm = 1, dm = 0;         // z- face of plane k: neighbour present, Dirichlet
+    other(k0, uz, kz);
+    if (k0 > 0) other(k0 - 1, um, km);
+    else yz_face<T, W, 2, -1>(L, j, k0, h0, cc, uo, us, ko, ks, kfield, um, km, mm, dm);
+    for (int k = k0; k < k1; k++) {
+        VecW<T, W> up, kp;
+        int mp = 1, dp = 0;
+        if (k < nz1) other(k + 1, up, kp);
+        else yz_face<T, W, 2, 1>(L, j, k, h0, cc, uo, us, ko, ks, kfield, up, kp, mp, dp);
+        const int row = j + L.ny * k;
+        const int q = (j + k + c) & 1;
+        const int o0 = h0 + L.P * row;
+        const VecW<T, W> kc4 = kfield ? ldv<T, W>(ks + o0) : zerov<T, W>();
+        const VecW<T, W> f4 = ldv<T, W>(f + o0);
+        VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
+        int dcount_y = 0;
+        {
+            VecW<T, W> un, kn;
+            int m, dd;
+            yz_face<T, W, 1, -1>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);
+            dcount_y += dd;
+            add_face<T, W>(kfield, kc4, un, kn, m, cym, acc, wsum);
+            yz_face<T, W, 1, 1>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);
+            dcount_y += dd;
+            add_face<T, W>(kfield, kc4, un, kn, m, cyp, acc, wsum);
+        }
+        add_face<T, W>(kfield, kc4, um, km, mm, czm, acc, wsum);
+        add_face<T, W>(kfield, kc4, up, kp, mp, czp, acc, wsum);
+        const int dcount_z = dm + dp;
+        const T byz = (T)dcount_y * (T)dir_c<1, true>(L, j) + (T)dcount_z * (T)dir_c<2, true>(L, k);
+        VecW<T, W> diag, off;
+        row_finish<T, W, CSplit<T>, true>(L, op, c, u, row, j, k, h0, q, o0, kc4, acc, wsum, byz, uz, kz, diag, off);
+        VecW<T, W> res;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+            const int i = 2 * (h0 + e) + q;
+            res.v[e] = i < L.nx ? gs_value(f4.v[e], diag.v[e], off.v[e]) : T(0);
+        }
+        stv<T, W>(out + o0, res);
+        um = uz; km = kz; mm = 1; dm = 0;
+        uz = up; kz = kp;
+    }
 }
 
 // residual of colour c on a uniform level, W cells per thread: r = f - A u
