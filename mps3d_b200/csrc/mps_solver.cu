@@ -694,7 +694,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     // the first post-smoothing pass overwrites the red cells from the black
     // ones, so only black cells need the correction (unless an odd periodic
     // seam makes red cells read red neighbours)
-    Box pb;
+    Box pb{};
     auto prolong_bulk = [&](auto wc) {
         constexpr int W = decltype(wc)::value;
         const long long G = (L.nh + W - 1) / W;  // groups holding a cell (the rest of the P / W are pads)
