@@ -411,6 +411,22 @@ struct CoarseShape {
     static constexpr int W = sizeof(T) == 4 ? MPS_COARSE_W32 : MPS_COARSE_W64;
     static constexpr int MINB = sizeof(T) == 4 ? MPS_COARSE_MINB32 : MPS_COARSE_MINB64;
 };
+// the colour pass of the levels two or more below the finest (64^3 and
+// smaller at 257^3): one cell per thread -- these launches are bound by the
+// latency of a thread's work, not by bytes (measured: 14.23 ms mixed /
+// 23.64 ms FP64 with one cell per thread here and in the transfers, against
+// 14.53 / 23.92 with the 128^3 level's shapes)
+#ifndef MPS_SMALL_W32
+#define MPS_SMALL_W32 1
+#endif
+#ifndef MPS_SMALL_W64
+#define MPS_SMALL_W64 1
+#endif
+template <class T>
+struct SmallShape {
+    static constexpr int W = sizeof(T) == 4 ? MPS_SMALL_W32 : MPS_SMALL_W64;
+    static constexpr int MINB = sizeof(T) == 4 ? MPS_COARSE_MINB32 : MPS_COARSE_MINB64;
+};
 
 template <class T, int W, class U, int MB = ColourShape<T>::MINB>
 __global__ void __launch_bounds__(TPB, MB) k_colourv(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
@@ -726,6 +742,14 @@ template <class T>
 struct CoarseXferShape {
     static constexpr int W = sizeof(T) == 4 ? MPS_XFER_COARSE_W32 : MPS_XFER_COARSE_W64;
     static constexpr int MINB = sizeof(T) == 4 ? MPS_XFER_COARSE_MINB32 : MPS_XFER_COARSE_MINB64;
+};
+#ifndef MPS_XFER_SMALL_W
+#define MPS_XFER_SMALL_W 1
+#endif
+template <class T>
+struct SmallXferShape {
+    static constexpr int W = MPS_XFER_SMALL_W > 0 ? MPS_XFER_SMALL_W : CoarseXferShape<T>::W;
+    static constexpr int MINB = CoarseXferShape<T>::MINB;
 };
 
 template <class T, int W>

@@ -605,8 +605,10 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
                            ccur(H, L, l), out, fh, dg, dy, nzc, nch);
             } else if (l == 0)
                 launch(std::integral_constant<int, ColourShape<T>::W>(), std::integral_constant<int, ColourShape<T>::MINB>());
-            else
+            else if (l == 1)
                 launch(std::integral_constant<int, CoarseShape<T>::W>(), std::integral_constant<int, CoarseShape<T>::MINB>());
+            else
+                launch(std::integral_constant<int, SmallShape<T>::W>(), std::integral_constant<int, SmallShape<T>::MINB>());
             if (l == ctx.prof.level) prof_end(ctx);
             CKL();
             if (c == 0) H.ri[l] ^= 1;
@@ -677,8 +679,10 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             };
             if (l == 0)
                 launch(std::integral_constant<int, RestrictShape<T>::W>(), std::integral_constant<int, RestrictShape<T>::MINB>());
-            else
+            else if (l == 1)
                 launch(std::integral_constant<int, CoarseXferShape<T>::W>(), std::integral_constant<int, CoarseXferShape<T>::MINB>());
+            else
+                launch(std::integral_constant<int, SmallXferShape<T>::W>(), std::integral_constant<int, SmallXferShape<T>::MINB>());
             CKL();
             done = true;
         }
@@ -737,7 +741,8 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     };
     if (o->nu2 >= 1 && L.nx >= 16 && prolong_box(L, C, ctx.xf[l], pb)) {
         if (l == 0) prolong_bulk(std::integral_constant<int, ProlongShape<T>::W>());
-        else prolong_bulk(std::integral_constant<int, CoarseXferShape<T>::W>());
+        else if (l == 1) prolong_bulk(std::integral_constant<int, CoarseXferShape<T>::W>());
+        else prolong_bulk(std::integral_constant<int, SmallXferShape<T>::W>());
         CKL();
     } else if (o->nu2 >= 1) {
         pdl_launch(k_prolong_correct<T>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, L, cur(H, L, l), C,
