@@ -166,7 +166,7 @@ __device__ __forceinline__ VecW<T, W> zerov()
 // the row neighbour along y or z of a group (AX = 1 or 2, S = -1/+1): vectors
 // of u and k values and the face status (wrapped row for periodic faces,
 // same-colour arrays across an odd periodic seam)
-template <class T, int W, int AX, int S>
+template <class T, int W, int AX, int S, bool IN = false>
 __device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int cc, const T* uo, const T* us,
                                         const T* ko, const T* ks, bool kfield, VecW<T, W>& u4, VecW<T, W>& k4,
                                         int& mask, int& dirc)
@@ -178,7 +178,7 @@ __device__ __forceinline__ void yz_face(const Lev& L, int j, int k, int h0, int 
     dirc = 0;
     const T* ub = uo;
     const T* kb = ko;
-    if (pq < 0 || pq >= n) {
+    if (!IN && (pq < 0 || pq >= n)) {  // IN: rows known to be inside the grid
         if (!L.per[AX]) {  // physical face: no neighbour
             mask = 0;
             dirc = L.bc[2 * AX + (S > 0 ? 1 : 0)] == BC_DIRC;
@@ -222,7 +222,9 @@ __device__ __forceinline__ double dir_c(const Lev& L, int p)
 // The x faces and the diagonal of W cells of one row, given the y/z face
 // sums (acc = sum w u_n, wsum = sum w, byz = Dirichlet y/z boundary weight)
 // and the other colour's vectors at the row's own offsets (ax: u, akx: k).
-template <class T, int W, class U, bool UNI>
+// IN: every cell of the group has all six neighbours inside the grid (no
+// boundary code is generated)
+template <class T, int W, class U, bool UNI, bool IN = false>
 __device__ __forceinline__ void row_finish(const Lev& L, const KOp<T>& op, int c, const U& u, int row, int j, int k,
                                            int h0, int q, int o0, const VecW<T, W>& kc4, const VecW<T, W>& acc,
                                            const VecW<T, W>& wsum, T byz, const VecW<T, W>& ax,
@@ -236,7 +238,7 @@ __device__ __forceinline__ void row_finish(const Lev& L, const KOp<T>& op, int c
     const T* ks = kfield ? sel(op.k, cc) : nullptr;
     // x neighbours: A = other colour at o0..o0+W-1, S = o0+W (q=1) or o0-1 (q=0)
     const int so = q ? o0 + W : o0 - 1;
-    const bool sok = q ? (h0 + W < L.P) : (h0 > 0);
+    const bool sok = IN || (q ? (h0 + W < L.P) : (h0 > 0));
     T sx = T(0), skx = T(0);
     if (sok) {
         sx = u.ld(uo, so);
@@ -256,7 +258,7 @@ __device__ __forceinline__ void row_finish(const Lev& L, const KOp<T>& op, int c
         }
         T mxm = T(1), mxp = T(1);
         T bx = T(0);
-        if (i == 0) {  // x- boundary / periodic wrap
+        if (!IN && i == 0) {  // x- boundary / periodic wrap
             if (L.per[0]) {
                 const int a = nx1;
                 const int wo = (a >> 1) + L.P * row;
@@ -268,7 +270,7 @@ __device__ __forceinline__ void row_finish(const Lev& L, const KOp<T>& op, int c
                 if (L.bc[0] == BC_DIRC) bx += (T)dir_c<0, UNI>(L, i);
             }
         }
-        if (i == nx1) {  // x+ boundary / periodic wrap
+        if (!IN && i == nx1) {  // x+ boundary / periodic wrap
             if (L.per[0]) {
                 const int wo = L.P * row;
                 const bool same = ((j + k) & 1) == cc;
@@ -307,7 +309,7 @@ __device__ __forceinline__ void add_face(bool kfield, const VecW<T, W>& kc4, con
     }
 }
 
-template <class T, int W, class U, bool UNI = true>
+template <class T, int W, class U, bool UNI = true, bool IN = false>
 __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c, const U& u, int row, int j,
                                            int k, int h0, int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
 {
@@ -331,7 +333,7 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
     {                                                                                                \
         VecW<T, W> un, kn;                                                                           \
         int m, dd;                                                                                   \
-        yz_face<T, W, AXV, SV>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);              \
+        yz_face<T, W, AXV, SV, IN>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);          \
         DC += dd;                                                                                    \
         add_face<T, W>(kfield, kc4, un, kn, m, CF, acc, wsum);                                       \
     }
@@ -343,7 +345,7 @@ __device__ __forceinline__ void group_rows(const Lev& L, const KOp<T>& op, int c
     const T byz = (T)dcount_y * (T)dir_c<1, UNI>(L, j) + (T)dcount_z * (T)dir_c<2, UNI>(L, k);
     const VecW<T, W> ax = uo ? ldv<T, W>(uo + o0) : zerov<T, W>();
     const VecW<T, W> akx = kfield ? ldv<T, W>(ko + o0) : zerov<T, W>();
-    row_finish<T, W, U, UNI>(L, op, c, u, row, j, k, h0, q, o0, kc4, acc, wsum, byz, ax, akx, diag, off);
+    row_finish<T, W, U, UNI, IN>(L, op, c, u, row, j, k, h0, q, o0, kc4, acc, wsum, byz, ax, akx, diag, off);
 }
 
 // decode the group index of a vector launch
@@ -1222,6 +1224,85 @@ __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSp
         lin_axis<T>(X, 0, i, xreg, x0, x1, tx);
         base[el] = base[el] + trilinear<T>(C, e, x0, x1, tx, y0, y1, ty, z0, z1, tz);
     }
+}
+
+// ---------------------------------------------------------------------
+// Colour pass of a uniform level in two parts of one launch.  Blocks below
+// nb_in take the interior: groups whose cells all have six neighbours inside
+// the grid (rows 1 .. ny-2 and 1 .. nz-2, groups g_lo .. g_hi), evaluated
+// with no boundary code at all.  The other blocks take the shell: first the
+// x-end groups of the interior rows, then every group of the rows on the
+// four y/z faces, with the general row evaluation.  Same arithmetic and
+// results as k_colourv.
+// ---------------------------------------------------------------------
+struct ColourSplit {
+    FastDiv gin;      // by the interior groups of a row
+    FastDiv yin;      // by the interior rows along y (ny - 2)
+    FastDiv gx;       // by the x-end groups of a row (G - gin)
+    FastDiv g;        // by the groups of a row that hold a cell (G)
+    int g_lo, g_hi;   // interior groups
+    unsigned n_in;    // interior threads
+    unsigned n_xe;    // threads of the x ends of the interior rows
+    unsigned n_face;  // threads of the face rows
+    unsigned nb_in;   // blocks of the interior part
+    Box b;            // the interior rows: [1, ny-2] x [1, nz-2]
+};
+
+template <class T, int W, class U, int MB>
+__global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
+                                                           const T* __restrict__ f, ColourSplit cs)
+{
+    pdl_wait();
+    if (blockIdx.x < cs.nb_in) {
+        const unsigned t = blockIdx.x * TPB + threadIdx.x;
+        if (t >= cs.n_in) return;
+        const unsigned r = cs.gin.div(t);
+        const int g = cs.g_lo + (int)(t - r * cs.gin.d);
+        const unsigned kk = cs.yin.div(r);
+        const int k = 1 + (int)kk, j = 1 + (int)(r - kk * cs.yin.d);
+        const int h0 = W * g;
+        const int row = j + L.ny * k;
+        const int q = (j + k + c) & 1;
+        const int o0 = h0 + L.P * row;
+        const VecW<T, W> f4 = ldv<T, W>(f + o0);
+        VecW<T, W> diag, off;
+        group_rows<T, W, U, true, true>(L, op, c, u, row, j, k, h0, q, o0, diag, off);
+        VecW<T, W> res;
+#pragma unroll
+        for (int e = 0; e < W; e++) res.v[e] = gs_value(f4.v[e], diag.v[e], off.v[e]);
+        stv<T, W>(out + o0, res);
+        return;
+    }
+    unsigned t = (blockIdx.x - cs.nb_in) * TPB + threadIdx.x;
+    int j, k, g;
+    if (t < cs.n_xe) {
+        const unsigned r = cs.gx.div(t);
+        const unsigned e = t - r * cs.gx.d;
+        g = e < (unsigned)cs.g_lo ? (int)e : cs.g_hi + 1 + (int)(e - cs.g_lo);
+        const unsigned kk = cs.yin.div(r);
+        k = 1 + (int)kk;
+        j = 1 + (int)(r - kk * cs.yin.d);
+    } else {
+        t -= cs.n_xe;
+        if (t >= cs.n_face) return;
+        const unsigned r = cs.g.div(t);
+        g = (int)(t - r * cs.g.d);
+        shell_row(r, L.ny, cs.b, j, k);
+    }
+    const int h0 = W * g;
+    const int row = j + L.ny * k;
+    const int q = (j + k + c) & 1;
+    const int o0 = h0 + L.P * row;
+    const VecW<T, W> f4 = ldv<T, W>(f + o0);
+    VecW<T, W> diag, off;
+    group_rows<T, W, U, true, false>(L, op, c, u, row, j, k, h0, q, o0, diag, off);
+    VecW<T, W> res;
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int i = 2 * (h0 + e) + q;
+        res.v[e] = i < L.nx ? gs_value(f4.v[e], diag.v[e], off.v[e]) : T(0);
+    }
+    stv<T, W>(out + o0, res);
 }
 
 // ---------------------------------------------------------------------

@@ -539,6 +539,10 @@ static long long box_cells(const Box& b)
 #ifndef MPS_COLOUR_MARCH32
 #define MPS_COLOUR_MARCH32 0
 #endif
+// finest uniform level: interior groups and the shell as two parts of a launch
+#ifndef MPS_COLOUR_SPLIT
+#define MPS_COLOUR_SPLIT 1
+#endif
 #ifndef MPS_COLOUR_MARCH64
 #define MPS_COLOUR_MARCH64 1
 #endif
@@ -603,6 +607,42 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
                 dy.init((unsigned)L.ny);
                 pdl_launch(k_colour_march<T, W, MB>, nblk((long long)per_chunk * nch), TPB, 0, ctx.s, L, op, c,
                            ccur(H, L, l), out, fh, dg, dy, nzc, nch);
+            } else if (l == 0 && MPS_COLOUR_SPLIT && L.uniform && L.ny >= 3 && L.nz >= 3 &&
+                       (L.nx - 1) / (2 * ColourShape<T>::W) - 1 >= 1) {
+                // interior groups without boundary code, the shell apart
+                constexpr int W = ColourShape<T>::W, MB = ColourShape<T>::MINB;
+                ColourSplit cs;
+                const unsigned G = (unsigned)((L.nh + W - 1) / W);
+                cs.g_lo = 1;
+                cs.g_hi = (L.nx - 1) / (2 * W) - 1;
+                const unsigned gin = (unsigned)(cs.g_hi - cs.g_lo + 1);
+                const unsigned rin = (unsigned)(L.ny - 2) * (unsigned)(L.nz - 2);
+                cs.gin.init(gin);
+                cs.yin.init((unsigned)(L.ny - 2));
+                cs.gx.init(std::max(G - gin, 1u));
+                cs.g.init(G);
+                cs.n_in = rin * gin;
+                cs.n_xe = rin * (G - gin);
+                cs.n_face = ((unsigned)L.ny * (unsigned)L.nz - rin) * G;
+                cs.nb_in = nblk(cs.n_in);
+                cs.b.lo[0] = 0;
+                cs.b.hi[0] = L.nx - 1;
+                cs.b.lo[1] = 1;
+                cs.b.hi[1] = L.ny - 2;
+                cs.b.lo[2] = 1;
+                cs.b.hi[2] = L.nz - 2;
+                const unsigned nbt = cs.nb_in + nblk((long long)cs.n_xe + cs.n_face);
+                if (zero_state == 2) {
+                    pdl_launch(k_colourv_split<T, W, ZeroU<T>, MB>, nbt, TPB, 0, ctx.s, L, op, c, ZeroU<T>(), out, fh, cs);
+                } else if (zero_state == 1) {
+                    OtherOnlyU<T> u;
+                    u.c = c;
+                    u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
+                    pdl_launch(k_colourv_split<T, W, OtherOnlyU<T>, MB>, nbt, TPB, 0, ctx.s, L, op, c, u, out, fh, cs);
+                } else {
+                    pdl_launch(k_colourv_split<T, W, CSplit<T>, MB>, nbt, TPB, 0, ctx.s, L, op, c, ccur(H, L, l), out, fh,
+                               cs);
+                }
             } else if (l == 0)
                 launch(std::integral_constant<int, ColourShape<T>::W>(), std::integral_constant<int, ColourShape<T>::MINB>());
             else if (l == 1)
