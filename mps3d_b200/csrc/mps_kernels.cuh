@@ -1305,6 +1305,96 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
     stv<T, W>(out + o0, res);
 }
 
+// Residual r = f - A u of both colours on a uniform level (the outer
+// residual of a solve), the interior groups without boundary code and the
+// shell apart, grid-stride over each part; r optionally stored as R, the
+// sums of r^2 and f^2 reduced as in k_residv.
+template <class T, int W, class R>
+__global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L, KOp<T> op, CSplit<T> u,
+                                                                           const T* __restrict__ f,
+                                                                           R* __restrict__ rout, RedBuf rb,
+                                                                           ColourSplit cs)
+{
+    pdl_wait();
+    __shared__ double sh[32];
+    double rr = 0.0, ff = 0.0;
+    auto group = [&](int j, int k, int g, auto in) {
+        constexpr bool IN = decltype(in)::value;
+        const int row = j + L.ny * k;
+        const int h0 = W * g;
+        const int o0 = h0 + L.P * row;
+        for (int cc = 0; cc <= 1; cc++) {
+            const int q = (j + k + cc) & 1;
+            VecW<T, W> diag, off;
+            group_rows<T, W, CSplit<T>, true, IN>(L, op, cc, u, row, j, k, h0, q, o0, diag, off);
+            const VecW<T, W> f4 = ldv<T, W>(f + (cc ? L.half : 0) + o0);
+            const VecW<T, W> u4 = ldv<T, W>(u.half(cc) + o0);
+            VecW<R, W> r4;
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+                const T r = f4.v[e] - (diag.v[e] * u4.v[e] + off.v[e]);
+                const bool ok = IN || 2 * (h0 + e) + q < L.nx;
+                r4.v[e] = ok ? (R)r : R(0);
+                if (ok) {
+                    rr += (double)r * (double)r;
+                    ff += (double)f4.v[e] * (double)f4.v[e];
+                }
+            }
+            if (rout) stv<R, W>(rout + (cc ? L.half : 0) + o0, r4);
+        }
+    };
+    const unsigned stride = gridDim.x * TPB;
+    for (unsigned t = blockIdx.x * TPB + threadIdx.x; t < cs.n_in; t += stride) {
+        const unsigned r = cs.gin.div(t);
+        const int g = cs.g_lo + (int)(t - r * cs.gin.d);
+        const unsigned kk = cs.yin.div(r);
+        group(1 + (int)(r - kk * cs.yin.d), 1 + (int)kk, g, std::true_type());
+    }
+    for (unsigned t = blockIdx.x * TPB + threadIdx.x; t < cs.n_xe + cs.n_face; t += stride) {
+        int j, k, g;
+        if (t < cs.n_xe) {
+            const unsigned r = cs.gx.div(t);
+            const unsigned e = t - r * cs.gx.d;
+            g = e < (unsigned)cs.g_lo ? (int)e : cs.g_hi + 1 + (int)(e - cs.g_lo);
+            const unsigned kk = cs.yin.div(r);
+            k = 1 + (int)kk;
+            j = 1 + (int)(r - kk * cs.yin.d);
+        } else {
+            const unsigned t2 = t - cs.n_xe;
+            const unsigned r = cs.g.div(t2);
+            g = (int)(t2 - r * cs.g.d);
+            shell_row(r, L.ny, cs.b, j, k);
+        }
+        group(j, k, g, std::false_type());
+    }
+    const double a = block_sum(rr, sh);
+    const double b = block_sum(ff, sh);
+    if (!rb.partial) return;
+    // finish: last block sums the partials in block order
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        rb.partial[2 * blockIdx.x] = a;
+        rb.partial[2 * blockIdx.x + 1] = b;
+        __threadfence();
+        last = (atomicAdd(rb.counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for (unsigned qd = threadIdx.x; qd < gridDim.x; qd += blockDim.x) {
+        sa += ((volatile double*)rb.partial)[2 * qd];
+        sb += ((volatile double*)rb.partial)[2 * qd + 1];
+    }
+    sa = block_sum(sa, sh);
+    sb = block_sum(sb, sh);
+    if (threadIdx.x == 0) {
+        rb.out[0] = sa;
+        rb.out[1] = sb;
+        *rb.counter = 0u;
+    }
+}
+
 // ---------------------------------------------------------------------
 // exact coarsest solve: u = A^{-1} f with the inverse precomputed (column
 // major, FP64).  Replaces bottomsolve's full-dimension GMRES

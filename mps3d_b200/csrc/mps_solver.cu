@@ -543,6 +543,9 @@ static long long box_cells(const Box& b)
 #ifndef MPS_COLOUR_SPLIT
 #define MPS_COLOUR_SPLIT 1
 #endif
+#ifndef MPS_RESID_SPLIT
+#define MPS_RESID_SPLIT 1
+#endif
 #ifndef MPS_COLOUR_MARCH64
 #define MPS_COLOUR_MARCH64 1
 #endif
@@ -558,6 +561,34 @@ static long long box_cells(const Box& b)
 #ifndef MPS_MARCH_MINB
 #define MPS_MARCH_MINB 3
 #endif
+
+// the interior / shell decomposition of a uniform level's groups of W cells
+// (k_colourv_split, k_residv_split); false when the level has no interior
+static bool make_split(const Lev& L, int W, ColourSplit& cs)
+{
+    if (!L.uniform || L.ny < 3 || L.nz < 3) return false;
+    cs.g_lo = 1;
+    cs.g_hi = (L.nx - 1) / (2 * W) - 1;
+    if (cs.g_hi < cs.g_lo) return false;
+    const unsigned G = (unsigned)((L.nh + W - 1) / W);
+    const unsigned gin = (unsigned)(cs.g_hi - cs.g_lo + 1);
+    const unsigned rin = (unsigned)(L.ny - 2) * (unsigned)(L.nz - 2);
+    cs.gin.init(gin);
+    cs.yin.init((unsigned)(L.ny - 2));
+    cs.gx.init(std::max(G - gin, 1u));
+    cs.g.init(G);
+    cs.n_in = rin * gin;
+    cs.n_xe = rin * (G - gin);
+    cs.n_face = ((unsigned)L.ny * (unsigned)L.nz - rin) * G;
+    cs.nb_in = nblk(cs.n_in);
+    cs.b.lo[0] = 0;
+    cs.b.hi[0] = L.nx - 1;
+    cs.b.lo[1] = 1;
+    cs.b.hi[1] = L.ny - 2;
+    cs.b.lo[2] = 1;
+    cs.b.hi[2] = L.nz - 2;
+    return true;
+}
 
 // ---- one colour pass ----
 template <class T, class Op>
@@ -607,30 +638,9 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
                 dy.init((unsigned)L.ny);
                 pdl_launch(k_colour_march<T, W, MB>, nblk((long long)per_chunk * nch), TPB, 0, ctx.s, L, op, c,
                            ccur(H, L, l), out, fh, dg, dy, nzc, nch);
-            } else if (l == 0 && MPS_COLOUR_SPLIT && L.uniform && L.ny >= 3 && L.nz >= 3 &&
-                       (L.nx - 1) / (2 * ColourShape<T>::W) - 1 >= 1) {
+            } else if (ColourSplit cs; l == 0 && MPS_COLOUR_SPLIT && make_split(L, ColourShape<T>::W, cs)) {
                 // interior groups without boundary code, the shell apart
                 constexpr int W = ColourShape<T>::W, MB = ColourShape<T>::MINB;
-                ColourSplit cs;
-                const unsigned G = (unsigned)((L.nh + W - 1) / W);
-                cs.g_lo = 1;
-                cs.g_hi = (L.nx - 1) / (2 * W) - 1;
-                const unsigned gin = (unsigned)(cs.g_hi - cs.g_lo + 1);
-                const unsigned rin = (unsigned)(L.ny - 2) * (unsigned)(L.nz - 2);
-                cs.gin.init(gin);
-                cs.yin.init((unsigned)(L.ny - 2));
-                cs.gx.init(std::max(G - gin, 1u));
-                cs.g.init(G);
-                cs.n_in = rin * gin;
-                cs.n_xe = rin * (G - gin);
-                cs.n_face = ((unsigned)L.ny * (unsigned)L.nz - rin) * G;
-                cs.nb_in = nblk(cs.n_in);
-                cs.b.lo[0] = 0;
-                cs.b.hi[0] = L.nx - 1;
-                cs.b.lo[1] = 1;
-                cs.b.hi[1] = L.ny - 2;
-                cs.b.lo[2] = 1;
-                cs.b.hi[2] = L.nz - 2;
                 const unsigned nbt = cs.nb_in + nblk((long long)cs.n_xe + cs.n_face);
                 if (zero_state == 2) {
                     pdl_launch(k_colourv_split<T, W, ZeroU<T>, MB>, nbt, TPB, 0, ctx.s, L, op, c, ZeroU<T>(), out, fh, cs);
@@ -830,6 +840,14 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             // thread per group)
             const unsigned nall = nblk((long long)(L.P / W) * L.rows);
             const unsigned nbv = std::min<unsigned>(nall, (unsigned)(ctx.nsm * ResidShape<T>::MINB));
+            ColourSplit cs;
+            if (MPS_RESID_SPLIT && make_split(L, W, cs)) {  // interior without boundary code, the shell apart
+                pdl_launch(k_residv_split<T, W, R>, nbv, TPB, 0, ctx.s, L, op, u, f.half(0),
+                           rout.c[0] ? rout.half(0) : nullptr, ctx.rb, cs);
+                CKL();
+                prof_end(ctx);
+                return 0;
+            }
             // both colours in one pass (f and rout as split bases, halves L.half apart)
             pdl_launch(k_residv<T, W, R>, nbv, TPB, 0, ctx.s, L, op, -1, u, f.half(0), rout.c[0] ? rout.half(0) : nullptr,
                                                        ctx.rb, 0, dg);
