@@ -5,9 +5,23 @@
 namespace mps {
 
 // ---------------------------------------------------------------------
-__global__ void k_gj_prepare(int n, const double* A, double* M)
+__global__ void __launch_bounds__(1024) k_dense_same(int n, const double* A, double* prev, int* gj)
 {
     pdl_wait();
+    const long long nn = (long long)n * n;
+    int diff = 0;
+    for (long long t = threadIdx.x; t < nn; t += blockDim.x)
+        diff |= __double_as_longlong(A[t]) != __double_as_longlong(prev[t]);
+    const int any = __syncthreads_or(diff) || gj[3] == 0;
+    if (any)
+        for (long long t = threadIdx.x; t < nn; t += blockDim.x) prev[t] = A[t];
+    if (threadIdx.x == 0) gj[2] = any;
+}
+
+__global__ void k_gj_prepare(int n, const double* A, double* M, const int* gj)
+{
+    pdl_wait();
+    if (gj[2] == 0) return;  // the inverse in AinvT is current
     const long long n2 = 2LL * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n2;
          t += (long long)gridDim.x * blockDim.x) {
@@ -16,9 +30,14 @@ __global__ void k_gj_prepare(int n, const double* A, double* M)
     }
 }
 
-__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* Mg, double* AinvT, int* status, int smem)
+__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* Mg, double* AinvT, int* status, int smem,
+                                                       int* gj)
 {
     pdl_wait();
+    if (gj[2] == 0) {  // the inverse in AinvT is current: its singular flag again
+        if (threadIdx.x == 0 && gj[0]) atomicOr(status, 1);
+        return;
+    }
     // 32 x 32 threads: lanes stride columns, warps stride rows
     extern __shared__ double Ms[];
     __shared__ double fac[1024];
@@ -86,6 +105,12 @@ __global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* Mg, double
     }
     for (int r = wid; r < n; r += nw)
         for (int c = lane; c < n; c += 32) AinvT[(long long)c * n + r] = sing[r] ? 0.0 : M[r * ld + n + c];
+    if (threadIdx.x == 0) {
+        int any_sing = 0;
+        for (int r = 0; r < n; r++) any_sing |= sing[r];
+        gj[0] = any_sing;
+        gj[3] = 1;
+    }
 }
 
 // ---------------------------------------------------------------------

@@ -1477,9 +1477,17 @@ __global__ void k_dense_assemble(Lev L, Op op, double* A)
 // Gauss-Jordan inverse with partial pivoting of the n x n row-major A held in
 // M = [A | I] (n x 2n, row major, prepared by k_gj_prepare); writes the
 // inverse column-major to AinvT.  One CTA; status[0] |= 1 on a zero pivot.
-// smem=1: the augmented matrix is staged in dynamic shared memory (small n)
-__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* M, double* AinvT, int* status, int smem);
-__global__ void k_gj_prepare(int n, const double* A, double* M);
+// smem=1: the augmented matrix is staged in dynamic shared memory (small n).
+// gj (per hierarchy): gj[2] = 0 when k_dense_same found the matrix equal to
+// the one whose inverse AinvT already holds -- both kernels then return at
+// once and status[0] takes the saved flag gj[0]; after an inversion gj[0]
+// keeps its flag and gj[3] = 1 marks AinvT valid.
+__global__ void __launch_bounds__(1024) k_gauss_jordan(int n, double* M, double* AinvT, int* status, int smem,
+                                                       int* gj);
+__global__ void k_gj_prepare(int n, const double* A, double* M, const int* gj);
+// one CTA: gj[2] = 1 when A differs from prev (bit for bit) or no inverse
+// was computed yet, and then prev = A
+__global__ void __launch_bounds__(1024) k_dense_same(int n, const double* A, double* prev, int* gj);
 
 // ---------------------------------------------------------------------
 // residual + norm: r = f - A u; sum r^2 (and sum f^2) reduced

@@ -110,6 +110,8 @@ struct Hier {
     KOp<T> kop[MAXL];
     ROp<T> rop[MAXL];
     double* AinvT = nullptr;
+    double* Dprev = nullptr;  // the coarsest matrix whose inverse AinvT holds
+    int* gj = nullptr;        // its inversion state (k_gauss_jordan)
 };
 
 struct Signature {
@@ -896,6 +898,8 @@ static void alloc_hier(Ctx& ctx, Hier<T>& H, bool& ok)
     const Lev& C = ctx.lev[ctx.nlev - 1];
     const long long n = (long long)C.nx * C.ny * C.nz;
     H.AinvT = (double*)ctx.ar.get(sizeof(double) * n * n);
+    H.Dprev = (double*)ctx.ar.get(sizeof(double) * n * n);
+    H.gj = (int*)ctx.ar.get(sizeof(int) * 4);
     ok = ok && H.AinvT;
 }
 
@@ -1041,14 +1045,17 @@ static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
     CK(cudaMemsetAsync(ctx.dense, 0, sizeof(double) * n * n, ctx.s));
     pdl_launch(k_dense_assemble<T, Op>, nblk(n), TPB, 0, ctx.s, L, op, ctx.dense);
     CKL();
-    pdl_launch(k_gj_prepare, nblk(2LL * n * n), TPB, 0, ctx.s, n, ctx.dense, ctx.gjM);
+    // an unchanged matrix (repeated solves with one operator) keeps its inverse
+    pdl_launch(k_dense_same, 1, 1024, 0, ctx.s, n, (const double*)ctx.dense, H.Dprev, H.gj);
+    CKL();
+    pdl_launch(k_gj_prepare, nblk(2LL * n * n), TPB, 0, ctx.s, n, ctx.dense, ctx.gjM, (const int*)H.gj);
     CKL();
     const size_t smem = sizeof(double) * 2 * (size_t)n * n;
     if (smem <= 200 * 1024) {
         CK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        pdl_launch(k_gauss_jordan, 1, 1024, smem, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 1);
+        pdl_launch(k_gauss_jordan, 1, 1024, smem, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 1, H.gj);
     } else {
-        pdl_launch(k_gauss_jordan, 1, 1024, 0, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 0);
+        pdl_launch(k_gauss_jordan, 1, 1024, 0, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 0, H.gj);
     }
     CKL();
     return 0;
