@@ -1248,7 +1248,10 @@ struct ColourSplit {
     Box b;            // the interior rows: [1, ny-2] x [1, nz-2]
 };
 
-template <class T, int W, class U, int MB>
+// UNI: the level is uniform (shell rows take the regular coefficients too);
+// on a level whose last cells are merged the interior stops one cell short
+// of them, so its faces are regular either way
+template <class T, int W, class U, int MB, bool UNI = true>
 __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
                                                            const T* __restrict__ f, ColourSplit cs)
 {
@@ -1295,7 +1298,7 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
     const int o0 = h0 + L.P * row;
     const VecW<T, W> f4 = ldv<T, W>(f + o0);
     VecW<T, W> diag, off;
-    group_rows<T, W, U, true, false>(L, op, c, u, row, j, k, h0, q, o0, diag, off);
+    group_rows<T, W, U, UNI, false>(L, op, c, u, row, j, k, h0, q, o0, diag, off);
     VecW<T, W> res;
 #pragma unroll
     for (int e = 0; e < W; e++) {

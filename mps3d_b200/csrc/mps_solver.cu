@@ -568,15 +568,18 @@ static long long box_cells(const Box& b)
 // (k_colourv_split, k_residv_split); false when the level has no interior
 static bool make_split(const Lev& L, int W, ColourSplit& cs)
 {
-    if (!L.uniform || L.ny < 3 || L.nz < 3) return false;
+    // the interior: cells 1 .. n-2 along each axis; on a level with merged
+    // last cells 1 .. n-3, whose faces all have the regular coefficients
+    const int m = L.uniform ? 2 : 3;
+    if (L.ny < m + 1 || L.nz < m + 1) return false;
     cs.g_lo = 1;
-    cs.g_hi = (L.nx - 1) / (2 * W) - 1;
+    cs.g_hi = (L.nx - m + 1) / (2 * W) - 1;
     if (cs.g_hi < cs.g_lo) return false;
     const unsigned G = (unsigned)((L.nh + W - 1) / W);
     const unsigned gin = (unsigned)(cs.g_hi - cs.g_lo + 1);
-    const unsigned rin = (unsigned)(L.ny - 2) * (unsigned)(L.nz - 2);
+    const unsigned rin = (unsigned)(L.ny - m) * (unsigned)(L.nz - m);
     cs.gin.init(gin);
-    cs.yin.init((unsigned)(L.ny - 2));
+    cs.yin.init((unsigned)(L.ny - m));
     cs.gx.init(std::max(G - gin, 1u));
     cs.g.init(G);
     cs.n_in = rin * gin;
@@ -586,9 +589,9 @@ static bool make_split(const Lev& L, int W, ColourSplit& cs)
     cs.b.lo[0] = 0;
     cs.b.hi[0] = L.nx - 1;
     cs.b.lo[1] = 1;
-    cs.b.hi[1] = L.ny - 2;
+    cs.b.hi[1] = L.ny - m;
     cs.b.lo[2] = 1;
-    cs.b.hi[2] = L.nz - 2;
+    cs.b.hi[2] = L.nz - m;
     return true;
 }
 
@@ -610,6 +613,30 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
             // levels below the finest have their own shape
             auto launch = [&](auto wc, auto mbc) {
                 constexpr int W = decltype(wc)::value, MB = decltype(mbc)::value;
+                ColourSplit cs;
+                if (MPS_COLOUR_SPLIT && make_split(L, W, cs)) {
+                    // interior groups without boundary code, the shell apart
+                    const unsigned nbt = cs.nb_in + nblk((long long)cs.n_xe + cs.n_face);
+                    auto go = [&](auto uc) {
+                        constexpr bool UNI = decltype(uc)::value;
+                        if (zero_state == 2) {
+                            pdl_launch(k_colourv_split<T, W, ZeroU<T>, MB, UNI>, nbt, TPB, 0, ctx.s, L, op, c, ZeroU<T>(),
+                                       out, fh, cs);
+                        } else if (zero_state == 1) {
+                            OtherOnlyU<T> u;
+                            u.c = c;
+                            u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
+                            pdl_launch(k_colourv_split<T, W, OtherOnlyU<T>, MB, UNI>, nbt, TPB, 0, ctx.s, L, op, c, u, out,
+                                       fh, cs);
+                        } else {
+                            pdl_launch(k_colourv_split<T, W, CSplit<T>, MB, UNI>, nbt, TPB, 0, ctx.s, L, op, c,
+                                       ccur(H, L, l), out, fh, cs);
+                        }
+                    };
+                    if (L.uniform) go(std::true_type());
+                    else go(std::false_type());
+                    return;
+                }
                 FastDiv dg;
                 dg.init((unsigned)(L.P / W));
                 const unsigned nbv = nblk((long long)(L.P / W) * L.rows);
@@ -640,21 +667,6 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
                 dy.init((unsigned)L.ny);
                 pdl_launch(k_colour_march<T, W, MB>, nblk((long long)per_chunk * nch), TPB, 0, ctx.s, L, op, c,
                            ccur(H, L, l), out, fh, dg, dy, nzc, nch);
-            } else if (ColourSplit cs; l == 0 && MPS_COLOUR_SPLIT && make_split(L, ColourShape<T>::W, cs)) {
-                // interior groups without boundary code, the shell apart
-                constexpr int W = ColourShape<T>::W, MB = ColourShape<T>::MINB;
-                const unsigned nbt = cs.nb_in + nblk((long long)cs.n_xe + cs.n_face);
-                if (zero_state == 2) {
-                    pdl_launch(k_colourv_split<T, W, ZeroU<T>, MB>, nbt, TPB, 0, ctx.s, L, op, c, ZeroU<T>(), out, fh, cs);
-                } else if (zero_state == 1) {
-                    OtherOnlyU<T> u;
-                    u.c = c;
-                    u.other = c == 0 ? H.U[l][H.bi[l]] + L.half : H.U[l][H.ri[l]];
-                    pdl_launch(k_colourv_split<T, W, OtherOnlyU<T>, MB>, nbt, TPB, 0, ctx.s, L, op, c, u, out, fh, cs);
-                } else {
-                    pdl_launch(k_colourv_split<T, W, CSplit<T>, MB>, nbt, TPB, 0, ctx.s, L, op, c, ccur(H, L, l), out, fh,
-                               cs);
-                }
             } else if (l == 0)
                 launch(std::integral_constant<int, ColourShape<T>::W>(), std::integral_constant<int, ColourShape<T>::MINB>());
             else if (l == 1)
