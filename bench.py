@@ -578,7 +578,7 @@ def run_ours(args, ws, rank, local):
         "hbm_gbs_solve": gbs_m,
         "hbm_frac_solve": gbs_m / hbm_peak,
         "fp64_hbm_frac_solve": gbs_d / hbm_peak,
-        "roofline": {"bound": "hbm", "kernel": "k_colourv<float,8> (finest-level red/black pass, FP32, mixed solve)",
+        "roofline": {"bound": "hbm", "kernel": "k_colourv_split<float,4> (finest-level red/black pass, FP32, mixed solve)",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "peak_kind": peak_kind, "traffic": traffic, "bytes_per_launch": cp_bytes,
                      "launch_ms": cp_ms, "fp64_achieved": achieved64, "fp64_frac": achieved64 / hbm_peak},

@@ -370,18 +370,20 @@ __device__ __forceinline__ bool group_decode(const Lev& L, const FastDiv& divG, 
 
 // colour pass, W cells of colour c per thread (vector loads).  Elements past
 // the end of the row (pads) are written as 0.  Same results as k_colour.
-// cells per thread and minimum resident blocks of the vector stencil kernels
-// (colour pass, residual, fused residual + restriction); measured on the
-// 257^3 plasma Poisson solve: 8 FP32 / 4 FP64 cells per thread (one 256-bit
-// access per field and row) with 3 blocks of 256 threads per SM
+// cells per thread and minimum resident blocks of the finest level's colour
+// pass and residual; measured on the 257^3 plasma Poisson solve with the
+// interior / shell split: FP32 4 cells (128-bit accesses) at 4 blocks of 256
+// per SM, 52.1 us per pass (8 cells at 3 blocks: 54.7, at 4: 56.2, at 2:
+// 54.1; 4 cells at 3 blocks: 53.4, at 5: 54.9; 2 cells at 6: 57.7); FP64 4
+// cells (256-bit accesses) at 3 blocks
 #ifndef MPS_COLOUR_W32
-#define MPS_COLOUR_W32 8
+#define MPS_COLOUR_W32 4
 #endif
 #ifndef MPS_COLOUR_W64
 #define MPS_COLOUR_W64 4
 #endif
 #ifndef MPS_COLOUR_MINB32
-#define MPS_COLOUR_MINB32 3
+#define MPS_COLOUR_MINB32 4
 #endif
 #ifndef MPS_COLOUR_MINB64
 #define MPS_COLOUR_MINB64 3
