@@ -533,11 +533,11 @@ static long long box_cells(const Box& b)
 }
 
 // finest uniform level: colour pass marching along z (planes per thread; 0 =
-// as many as one wave of resident blocks needs).  Measured on the 257^3
-// plasma Poisson solve: FP64 118 us per pass at 2 cells and 8 planes per
-// thread (119 at 4 planes, 133 at 16, 155 for one wave) against 126 us for
-// k_colourv; FP32 62 us at 4 cells and 4 planes against 58 us for k_colourv
-// at 8 cells (8 cells and three carried planes do not fit the registers)
+// as many as one wave of resident blocks needs).  Off: measured on the 257^3
+// plasma Poisson solve, the interior / shell split pass takes 91 us (FP64)
+// and 52 us (FP32) against 118 us (FP64, 2 cells and 8 planes per thread;
+// 119 at 4 planes, 133 at 16, 155 for one wave) and 62 us (FP32, 4 cells, 4
+// planes) marching
 #ifndef MPS_COLOUR_MARCH32
 #define MPS_COLOUR_MARCH32 0
 #endif
@@ -549,7 +549,7 @@ static long long box_cells(const Box& b)
 #define MPS_RESID_SPLIT 1
 #endif
 #ifndef MPS_COLOUR_MARCH64
-#define MPS_COLOUR_MARCH64 1
+#define MPS_COLOUR_MARCH64 0
 #endif
 #ifndef MPS_MARCH_NZ
 #define MPS_MARCH_NZ 8
