@@ -716,10 +716,13 @@ struct Box {
 #ifndef MPS_PROLONG_W64
 #define MPS_PROLONG_W64 2
 #endif
+#ifndef MPS_RESTRICT_MINB32
+#define MPS_RESTRICT_MINB32 4
+#endif
 template <class T>
 struct RestrictShape {
     static constexpr int W = sizeof(T) == 4 ? MPS_RESTRICT_W32 : MPS_RESTRICT_W64;
-    static constexpr int MINB = sizeof(T) == 4 ? 4 : MPS_RESTRICT_MINB64;
+    static constexpr int MINB = sizeof(T) == 4 ? MPS_RESTRICT_MINB32 : MPS_RESTRICT_MINB64;
 };
 // cells per thread of the prolongation bulk on the finest level
 template <class T>
@@ -756,18 +759,37 @@ struct SmallXferShape {
     static constexpr int MINB = CoarseXferShape<T>::MINB;
 };
 
-template <class T, int W>
-__device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& op, const CSplit<T>& u,
-                                                    const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
-                                                    const FastDiv& divG, const Box& bx, unsigned t)
+// the r-th row (j,k) of an ny x nz set outside the rectangle [lo1,hi1] x [lo2,hi2]
+__device__ __forceinline__ void shell_row(unsigned r, int ny, const Box& b, int& j, int& k)
 {
-    const unsigned R = divG.div(t);  // coarse row J + Cny K
-    if (R >= C.rows) return;
-    const int K = (int)C.divNy.div(R);
-    const int J = (int)R - K * C.ny;
-    if (J < bx.lo[1] || J > bx.hi[1] || K < bx.lo[2] || K > bx.hi[2]) return;
-    const int h0 = W * (int)(t - R * (unsigned)(F.P / W));
-    if (h0 > bx.hi[0] || h0 + W - 1 < bx.lo[0]) return;
+    const unsigned uny = (unsigned)ny;
+    const unsigned yin = (unsigned)(b.hi[1] - b.lo[1] + 1), yout = uny - yin;
+    const unsigned s1 = (unsigned)b.lo[2] * uny;
+    if (r < s1) { k = (int)(r / uny); j = (int)(r - (unsigned)k * uny); return; }
+    r -= s1;
+    const unsigned zin = (unsigned)(b.hi[2] - b.lo[2] + 1);
+    const unsigned s2 = zin * yout;
+    if (r < s2) {
+        const unsigned kk = r / yout;
+        k = b.lo[2] + (int)kk;
+        const unsigned q = r - kk * yout;
+        j = (int)(q < (unsigned)b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
+        return;
+    }
+    r -= s2;
+    const unsigned kk = r / uny;
+    k = b.hi[2] + 1 + (int)kk;
+    j = (int)(r - kk * uny);
+}
+
+// the W coarse cells I = h0 .. h0+W-1 of coarse row (J, K) from their four
+// red fine rows; IN: every fine cell involved has its neighbours inside the
+// grid and regular faces (no boundary code)
+template <class T, int W, bool UNI, bool IN>
+__device__ __forceinline__ void restrict_cells(const Lev& F, const KOp<T>& op, const CSplit<T>& u,
+                                               const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
+                                               const Box& bx, int J, int K, int h0)
+{
     VecW<T, W> s = zerov<T, W>();
 #pragma unroll
     for (int dk = 0; dk < 2; dk++)
@@ -778,8 +800,7 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& 
             const int q = (j + k) & 1;
             const int o0 = h0 + F.P * row;
             VecW<T, W> diag, off;
-            if (F.uniform) group_rows<T, W, CSplit<T>, true>(F, op, 0, u, row, j, k, h0, q, o0, diag, off);
-            else group_rows<T, W, CSplit<T>, false>(F, op, 0, u, row, j, k, h0, q, o0, diag, off);
+            group_rows<T, W, CSplit<T>, UNI, IN>(F, op, 0, u, row, j, k, h0, q, o0, diag, off);
             const VecW<T, W> f4 = ldv<T, W>(fred + o0);
             const VecW<T, W> u4 = ldv<T, W>(u.c[0] + o0);
 #pragma unroll
@@ -791,6 +812,58 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& 
         const int I = h0 + e;
         if (I >= bx.lo[0] && I <= bx.hi[0]) fc.half((I + J + K) & 1)[(I >> 1) + cb] = s.v[e] * T(0.125);
     }
+}
+
+// the bulk of the restriction in two parts: interior coarse rows [J0, J0+nJ)
+// x [K0, K0+nK) with groups [ga, gb] (no boundary code), then the rest of
+// the bulk -- the other groups of those rows, and every group of the coarse
+// rows outside that rectangle (cells outside the box return)
+struct RestrictSplit {
+    FastDiv gin;      // by the interior groups
+    FastDiv yin;      // by nJ
+    FastDiv gx;       // by the other groups of a row (G - gin)
+    FastDiv g;        // by the groups of a row (G = fine P / W)
+    int ga, gb, J0, K0;
+    unsigned n_in, n_xe, n_out;
+    unsigned nb_in;   // blocks of the interior part
+    Box rect;         // the interior coarse rows (y/z bounds)
+};
+
+template <class T, int W, bool UNI>
+__device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& op, const CSplit<T>& u,
+                                                    const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
+                                                    const Box& bx, const RestrictSplit& rs, unsigned blk)
+{
+    if (blk < rs.nb_in) {
+        const unsigned t = blk * TPB + threadIdx.x;
+        if (t >= rs.n_in) return;
+        const unsigned r = rs.gin.div(t);
+        const int g = rs.ga + (int)(t - r * rs.gin.d);
+        const unsigned kk = rs.yin.div(r);
+        restrict_cells<T, W, true, true>(F, op, u, fred, C, fc, bx, rs.J0 + (int)(r - kk * rs.yin.d),
+                                         rs.K0 + (int)kk, W * g);
+        return;
+    }
+    unsigned t = (blk - rs.nb_in) * TPB + threadIdx.x;
+    int J, K, g;
+    if (t < rs.n_xe) {
+        const unsigned r = rs.gx.div(t);
+        const unsigned e = t - r * rs.gx.d;
+        g = e < (unsigned)rs.ga ? (int)e : rs.gb + 1 + (int)(e - rs.ga);
+        const unsigned kk = rs.yin.div(r);
+        J = rs.J0 + (int)(r - kk * rs.yin.d);
+        K = rs.K0 + (int)kk;
+    } else {
+        t -= rs.n_xe;
+        if (t >= rs.n_out) return;
+        const unsigned r = rs.g.div(t);
+        g = (int)(t - r * rs.g.d);
+        shell_row(r, C.ny, rs.rect, J, K);
+    }
+    if (J < bx.lo[1] || J > bx.hi[1] || K < bx.lo[2] || K > bx.hi[2]) return;
+    const int h0 = W * g;
+    if (h0 > bx.hi[0] || h0 + W - 1 < bx.lo[0]) return;
+    restrict_cells<T, W, UNI, false>(F, op, u, fred, C, fc, bx, J, K, h0);
 }
 
 // the t-th cell of an n[0] x n[1] x n[2] grid outside box b: z slabs first,
@@ -854,16 +927,17 @@ __device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op,
 
 // bulk and shell in one launch: blocks [0, nb_bulk) take the bulk rows,
 // the rest the shell cells
-template <class T, int W, int MB>
+// UNI: the fine level is uniform
+template <class T, int W, int MB, bool UNI>
 __global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
                                                                                  const T* __restrict__ fred, Lev C,
-                                                                                 Split<T> fc, FastDiv divG, Box bx,
+                                                                                 Split<T> fc, RestrictSplit rs, Box bx,
                                                                                  unsigned nb_bulk, int geom,
                                                                                  unsigned shell)
 {
     pdl_wait();
     if (blockIdx.x < nb_bulk) {
-        resid_restrict_bulk<T, W>(F, op, u, fred, C, fc, divG, bx, blockIdx.x * TPB + threadIdx.x);
+        resid_restrict_bulk<T, W, UNI>(F, op, u, fred, C, fc, bx, rs, blockIdx.x);
     } else {
         CSplit<T> f;
         f.c[0] = fred;
@@ -994,29 +1068,6 @@ __global__ void __launch_bounds__(TPB) k_prolong_correct(Lev F, Split<T> u, Lev 
 // mode 3: the other groups of the rows inside the box in (y,z); mode 1:
 // black cells of the other rows; mode 2: red cells on odd periodic seam
 // planes (read by the next red pass), one cell per thread.
-// ---------------------------------------------------------------------
-// the r-th row (j,k) of an ny x nz set outside the rectangle [lo1,hi1] x [lo2,hi2]
-__device__ __forceinline__ void shell_row(unsigned r, int ny, const Box& b, int& j, int& k)
-{
-    const unsigned uny = (unsigned)ny;
-    const unsigned yin = (unsigned)(b.hi[1] - b.lo[1] + 1), yout = uny - yin;
-    const unsigned s1 = (unsigned)b.lo[2] * uny;
-    if (r < s1) { k = (int)(r / uny); j = (int)(r - (unsigned)k * uny); return; }
-    r -= s1;
-    const unsigned zin = (unsigned)(b.hi[2] - b.lo[2] + 1);
-    const unsigned s2 = zin * yout;
-    if (r < s2) {
-        const unsigned kk = r / yout;
-        k = b.lo[2] + (int)kk;
-        const unsigned q = r - kk * yout;
-        j = (int)(q < (unsigned)b.lo[1] ? q : b.hi[1] + 1 + (q - b.lo[1]));
-        return;
-    }
-    r -= s2;
-    const unsigned kk = r / uny;
-    k = b.hi[2] + 1 + (int)kk;
-    j = (int)(r - kk * uny);
-}
 
 template <class T>
 __device__ __forceinline__ void lin_axis(const Xfer& X, int ax, int i, bool regular, int& a, int& b, T& t)

@@ -595,6 +595,45 @@ static bool make_split(const Lev& L, int W, ColourSplit& cs)
     return true;
 }
 
+// the restriction bulk's interior coarse rows and groups (every fine cell
+// evaluated has its neighbours inside the grid and regular faces: fine cells
+// 1 .. n-2, or 1 .. n-3 on a level with merged last cells) and the rest; an
+// empty interior leaves everything to the rest part
+static RestrictSplit make_restrict_split(const Lev& F, const Lev& C, const Box& bx, int W)
+{
+    RestrictSplit rs;
+    std::memset(&rs, 0, sizeof(rs));
+    const int m = F.uniform ? 2 : 3;
+    const int G = F.P / W;
+    rs.J0 = std::max(bx.lo[1], 1);
+    rs.K0 = std::max(bx.lo[2], 1);
+    const int J1 = std::min(bx.hi[1], (F.ny - m - 1) / 2), K1 = std::min(bx.hi[2], (F.nz - m - 1) / 2);
+    rs.ga = 1;
+    rs.gb = ((F.nx - m - 1) / 2 - W + 1) / W;
+    int nJ = J1 - rs.J0 + 1, nK = K1 - rs.K0 + 1, ng = rs.gb - rs.ga + 1;
+    if (nJ < 1 || nK < 1 || ng < 1) {  // no interior: the rectangle is empty
+        nJ = nK = 0;
+        ng = 0;
+        rs.ga = 0;
+        rs.gb = -1;
+    }
+    rs.gin.init((unsigned)std::max(ng, 1));
+    rs.yin.init((unsigned)std::max(nJ, 1));
+    rs.gx.init((unsigned)std::max(G - ng, 1));
+    rs.g.init((unsigned)G);
+    rs.n_in = (unsigned)nJ * (unsigned)nK * (unsigned)ng;
+    rs.n_xe = (unsigned)nJ * (unsigned)nK * (unsigned)(G - ng);
+    rs.n_out = ((unsigned)C.ny * (unsigned)C.nz - (unsigned)nJ * (unsigned)nK) * (unsigned)G;
+    rs.nb_in = nblk(rs.n_in);
+    rs.rect.lo[0] = 0;
+    rs.rect.hi[0] = C.nx - 1;
+    rs.rect.lo[1] = rs.J0;
+    rs.rect.hi[1] = rs.J0 + nJ - 1;
+    rs.rect.lo[2] = rs.K0;
+    rs.rect.hi[2] = rs.K0 + nK - 1;
+    return rs;
+}
+
 // ---- one colour pass ----
 template <class T, class Op>
 static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zero_state)
@@ -733,13 +772,16 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
             // shell with the general body
             auto launch = [&](auto wc, auto mbc) {
                 constexpr int W = decltype(wc)::value, MB = decltype(mbc)::value;
-                FastDiv dg;
-                dg.init((unsigned)(L.P / W));
-                const long long nt = (long long)C.rows * (L.P / W);
+                const RestrictSplit rs = make_restrict_split(L, C, bx, W);
                 const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
-                const unsigned nbb = nblk(nt), nbs = shell > 0 ? nblk(8 * shell) : 0;
-                pdl_launch(k_resid_restrict_v<T, W, MB>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l), H.F[l], C,
-                           split<T>(H.F[l + 1], C), dg, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
+                const unsigned nbb = rs.nb_in + nblk((long long)rs.n_xe + rs.n_out);
+                const unsigned nbs = shell > 0 ? nblk(8 * shell) : 0;
+                if (L.uniform)
+                    pdl_launch(k_resid_restrict_v<T, W, MB, true>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l),
+                               H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
+                else
+                    pdl_launch(k_resid_restrict_v<T, W, MB, false>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l),
+                               H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
             };
             if (l == 0)
                 launch(std::integral_constant<int, RestrictShape<T>::W>(), std::integral_constant<int, RestrictShape<T>::MINB>());
