@@ -452,88 +452,6 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv(Lev L, KOp<T> op, int c, U 
     stv<T, W>(out + G.o0, res);
 }
 
-// Colour pass marching along z (uniform levels): thread (g, j, chunk) takes
-// W cells of colour c in row j for the planes k0 .. k0+nzc-1 of its chunk.
-// The other colour's vectors of row j at the same group offset serve three
-// planes: at plane k they are the x neighbours, at k-1 and k+1 the z
-// neighbours (cell (i, j, k+-1) has the other colour and split index i>>1).
-// So they are loaded once (one u and one k vector per plane) and carried in
-// registers; the z faces of the first and last plane of the grid (physical
-// faces, periodic wraps, odd seams) go through yz_face.  Same arithmetic,
-// in the same order, as group_rows.
-template <class T, int W, int MB>
-__global__ void __launch_bounds__(TPB, MB) k_colour_march(Lev L, KOp<T> op, int c, CSplit<T> u, T* __restrict__ out,
-                                                          const T* __restrict__ f, FastDiv divG, FastDiv divY,
-                                                          int nzc, unsigned nchunks)
-{
-    pdl_wait();
-    const unsigned t = blockIdx.x * TPB + threadIdx.x;
-    const unsigned r = divG.div(t);  // j + ny * chunk
-    const unsigned chunk = divY.div(r);
-    if (chunk >= nchunks) return;
-    const int j = (int)(r - chunk * (unsigned)L.ny);
-    const int h0 = W * (int)(t - r * divG.d);
-    const int k0 = (int)chunk * nzc, k1 = min(k0 + nzc, L.nz);
-    const int cc = c, oc = c ^ 1;
-    const bool kfield = op.k[0] != nullptr;
-    const T* uo = u.ptr(oc);
-    const T* us = u.ptr(cc);
-    const T* ko = kfield ? sel(op.k, oc) : nullptr;
-    const T* ks = kfield ? sel(op.k, cc) : nullptr;
-    const int ny1 = L.ny - 1, nz1 = L.nz - 1;
-    const T cym = (T)face_c<1, true>(L, j, j > 0 ? j - 1 : ny1), cyp = (T)face_c<1, true>(L, j, j < ny1 ? j + 1 : 0);
-    const T czm = (T)face_c<2, true>(L, 0, nz1), czp = (T)face_c<2, true>(L, 0, 1);
-    const long long plane = (long long)L.P * L.ny;
-    const long long ob = h0 + (long long)L.P * j;  // the group's offset in plane 0
-    auto other = [&](int kk, VecW<T, W>& u4, VecW<T, W>& k4) {
-        u4 = ldv<T, W>(uo + ob + plane * kk);
-        k4 = kfield ? ldv<T, W>(ko + ob + plane * kk) : zerov<T, W>();
-    };
-    VecW<T, W> um, km, uz, kz;  // planes k-1 and k
-    int mm = 1, dm = 0;         // z- face of plane k: neighbour present, Dirichlet
-    other(k0, uz, kz);
-    if (k0 > 0) other(k0 - 1, um, km);
-    else yz_face<T, W, 2, -1>(L, j, k0, h0, cc, uo, us, ko, ks, kfield, um, km, mm, dm);
-    for (int k = k0; k < k1; k++) {
-        VecW<T, W> up, kp;
-        int mp = 1, dp = 0;
-        if (k < nz1) other(k + 1, up, kp);
-        else yz_face<T, W, 2, 1>(L, j, k, h0, cc, uo, us, ko, ks, kfield, up, kp, mp, dp);
-        const int row = j + L.ny * k;
-        const int q = (j + k + c) & 1;
-        const int o0 = h0 + L.P * row;
-        const VecW<T, W> kc4 = kfield ? ldv<T, W>(ks + o0) : zerov<T, W>();
-        const VecW<T, W> f4 = ldv<T, W>(f + o0);
-        VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
-        int dcount_y = 0;
-        {
-            VecW<T, W> un, kn;
-            int m, dd;
-            yz_face<T, W, 1, -1>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);
-            dcount_y += dd;
-            add_face<T, W>(kfield, kc4, un, kn, m, cym, acc, wsum);
-            yz_face<T, W, 1, 1>(L, j, k, h0, cc, uo, us, ko, ks, kfield, un, kn, m, dd);
-            dcount_y += dd;
-            add_face<T, W>(kfield, kc4, un, kn, m, cyp, acc, wsum);
-        }
-        add_face<T, W>(kfield, kc4, um, km, mm, czm, acc, wsum);
-        add_face<T, W>(kfield, kc4, up, kp, mp, czp, acc, wsum);
-        const int dcount_z = dm + dp;
-        const T byz = (T)dcount_y * (T)dir_c<1, true>(L, j) + (T)dcount_z * (T)dir_c<2, true>(L, k);
-        VecW<T, W> diag, off;
-        row_finish<T, W, CSplit<T>, true>(L, op, c, u, row, j, k, h0, q, o0, kc4, acc, wsum, byz, uz, kz, diag, off);
-        VecW<T, W> res;
-#pragma unroll
-        for (int e = 0; e < W; e++) {
-            const int i = 2 * (h0 + e) + q;
-            res.v[e] = i < L.nx ? gs_value(f4.v[e], diag.v[e], off.v[e]) : T(0);
-        }
-        stv<T, W>(out + o0, res);
-        um = uz; km = kz; mm = 1; dm = 0;
-        uz = up; kz = kp;
-    }
-}
-
 // residual of colour c on a uniform level, W cells per thread: r = f - A u
 // (u, f of type T), optional r out (type R, split half c), and the sums of
 // r^2 and f^2 reduced deterministically (accumulate = add to rb.out, for the

@@ -532,39 +532,18 @@ static long long box_cells(const Box& b)
     return (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
 }
 
-// finest uniform level: colour pass marching along z (planes per thread; 0 =
-// as many as one wave of resident blocks needs).  Off: measured on the 257^3
-// plasma Poisson solve, the interior / shell split pass takes 91 us (FP64)
-// and 52 us (FP32) against 118 us (FP64, 2 cells and 8 planes per thread;
-// 119 at 4 planes, 133 at 16, 155 for one wave) and 62 us (FP32, 4 cells, 4
-// planes) marching
-#ifndef MPS_COLOUR_MARCH32
-#define MPS_COLOUR_MARCH32 0
-#endif
-// finest uniform level: interior groups and the shell as two parts of a launch
+// colour passes and the outer residual: interior groups (no boundary code)
+// and the shell as two parts of a launch (measured at 257^3: FP32 colour
+// pass 54.6 against 58.3 us, FP64 91 against 126 us, outer residual 156
+// against 201 us)
 #ifndef MPS_COLOUR_SPLIT
 #define MPS_COLOUR_SPLIT 1
 #endif
 #ifndef MPS_RESID_SPLIT
 #define MPS_RESID_SPLIT 1
 #endif
-#ifndef MPS_COLOUR_MARCH64
-#define MPS_COLOUR_MARCH64 0
-#endif
-#ifndef MPS_MARCH_NZ
-#define MPS_MARCH_NZ 8
-#endif
-#ifndef MPS_MARCH_W32
-#define MPS_MARCH_W32 4
-#endif
-#ifndef MPS_MARCH_W64
-#define MPS_MARCH_W64 2
-#endif
-#ifndef MPS_MARCH_MINB
-#define MPS_MARCH_MINB 3
-#endif
 
-// the interior / shell decomposition of a uniform level's groups of W cells
+// the interior / shell decomposition of a level's groups of W cells
 // (k_colourv_split, k_residv_split); false when the level has no interior
 static bool make_split(const Lev& L, int W, ColourSplit& cs)
 {
@@ -691,22 +670,7 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
                                dg);
                 }
             };
-            constexpr bool march = sizeof(T) == 4 ? MPS_COLOUR_MARCH32 : MPS_COLOUR_MARCH64;
-            if (march && l == 0 && L.uniform && zero_state == 0) {
-                constexpr int W = sizeof(T) == 4 ? MPS_MARCH_W32 : MPS_MARCH_W64, MB = MPS_MARCH_MINB;
-                const unsigned G = (unsigned)(L.P / W), per_chunk = G * (unsigned)L.ny;
-                int nzc = MPS_MARCH_NZ;
-                if (nzc <= 0) {  // one wave of resident blocks
-                    const unsigned cap = (unsigned)(ctx.nsm * MB * TPB) / per_chunk;
-                    nzc = (L.nz + (int)std::max(cap, 1u) - 1) / (int)std::max(cap, 1u);
-                }
-                const unsigned nch = (unsigned)((L.nz + nzc - 1) / nzc);
-                FastDiv dg, dy;
-                dg.init(G);
-                dy.init((unsigned)L.ny);
-                pdl_launch(k_colour_march<T, W, MB>, nblk((long long)per_chunk * nch), TPB, 0, ctx.s, L, op, c,
-                           ccur(H, L, l), out, fh, dg, dy, nzc, nch);
-            } else if (l == 0)
+            if (l == 0)
                 launch(std::integral_constant<int, ColourShape<T>::W>(), std::integral_constant<int, ColourShape<T>::MINB>());
             else if (l == 1)
                 launch(std::integral_constant<int, CoarseShape<T>::W>(), std::integral_constant<int, CoarseShape<T>::MINB>());
