@@ -732,6 +732,30 @@ __device__ __forceinline__ void restrict_cells(const Lev& F, const KOp<T>& op, c
     }
 }
 
+// Block (or block-sized chunk) b of a split launch: the interior and x-end
+// chunks are interleaved in proportion, so that the ends of a row run while
+// the row's neighbours are still in L2 (the x-end chunks follow the same
+// row order as the interior ones); the face rows come last.  part: 0
+// interior, 1 x ends, 2 face rows; idx: the chunk within its part.
+__device__ __forceinline__ void split_chunk(unsigned nb_in, unsigned nb_xe, unsigned b, int& part, unsigned& idx)
+{
+    const unsigned m = nb_in + nb_xe;
+    if (b >= m) {
+        part = 2;
+        idx = b - m;
+        return;
+    }
+    const unsigned lo = (unsigned)(((unsigned long long)b * nb_xe) / m);
+    const unsigned hi = (unsigned)(((unsigned long long)(b + 1) * nb_xe) / m);
+    if (hi > lo) {
+        part = 1;
+        idx = lo;
+    } else {
+        part = 0;
+        idx = b - lo;
+    }
+}
+
 // the bulk of the restriction in two parts: interior coarse rows [J0, J0+nJ)
 // x [K0, K0+nK) with groups [ga, gb] (no boundary code), then the rest of
 // the bulk -- the other groups of those rows, and every group of the coarse
@@ -743,7 +767,7 @@ struct RestrictSplit {
     FastDiv g;        // by the groups of a row (G = fine P / W)
     int ga, gb, J0, K0;
     unsigned n_in, n_xe, n_out;
-    unsigned nb_in;   // blocks of the interior part
+    unsigned nb_in, nb_xe, nb_out;  // blocks of the three parts (interleaved by split_chunk)
     Box rect;         // the interior coarse rows (y/z bounds)
 };
 
@@ -752,8 +776,11 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& 
                                                     const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
                                                     const Box& bx, const RestrictSplit& rs, unsigned blk)
 {
-    if (blk < rs.nb_in) {
-        const unsigned t = blk * TPB + threadIdx.x;
+    int part;
+    unsigned idx;
+    split_chunk(rs.nb_in, rs.nb_xe, blk, part, idx);
+    if (part == 0) {
+        const unsigned t = idx * TPB + threadIdx.x;
         if (t >= rs.n_in) return;
         const unsigned r = rs.gin.div(t);
         const int g = rs.ga + (int)(t - r * rs.gin.d);
@@ -762,9 +789,10 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& 
                                          rs.K0 + (int)kk, W * g);
         return;
     }
-    unsigned t = (blk - rs.nb_in) * TPB + threadIdx.x;
+    const unsigned t = idx * TPB + threadIdx.x;
     int J, K, g;
-    if (t < rs.n_xe) {
+    if (part == 1) {
+        if (t >= rs.n_xe) return;
         const unsigned r = rs.gx.div(t);
         const unsigned e = t - r * rs.gx.d;
         g = e < (unsigned)rs.ga ? (int)e : rs.gb + 1 + (int)(e - rs.ga);
@@ -772,7 +800,6 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& 
         J = rs.J0 + (int)(r - kk * rs.yin.d);
         K = rs.K0 + (int)kk;
     } else {
-        t -= rs.n_xe;
         if (t >= rs.n_out) return;
         const unsigned r = rs.g.div(t);
         g = (int)(t - r * rs.g.d);
@@ -1215,9 +1242,12 @@ struct ColourSplit {
     unsigned n_in;    // interior threads
     unsigned n_xe;    // threads of the x ends of the interior rows
     unsigned n_face;  // threads of the face rows
-    unsigned nb_in;   // blocks of the interior part
+    unsigned nb_in;   // blocks (or block-sized chunks) of the interior part
+    unsigned nb_xe;   // of the x ends
+    unsigned nb_face; // of the face rows
     Box b;            // the interior rows: [1, ny-2] x [1, nz-2]
 };
+
 
 // UNI: the level is uniform (shell rows take the regular coefficients too);
 // on a level whose last cells are merged the interior stops one cell short
@@ -1227,8 +1257,11 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
                                                            const T* __restrict__ f, ColourSplit cs)
 {
     pdl_wait();
-    if (blockIdx.x < cs.nb_in) {
-        const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    int part;
+    unsigned idx;
+    split_chunk(cs.nb_in, cs.nb_xe, blockIdx.x, part, idx);
+    if (part == 0) {
+        const unsigned t = idx * TPB + threadIdx.x;
         if (t >= cs.n_in) return;
         const unsigned r = cs.gin.div(t);
         const int g = cs.g_lo + (int)(t - r * cs.gin.d);
@@ -1247,9 +1280,10 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
         stv<T, W>(out + o0, res);
         return;
     }
-    unsigned t = (blockIdx.x - cs.nb_in) * TPB + threadIdx.x;
+    const unsigned t = idx * TPB + threadIdx.x;
     int j, k, g;
-    if (t < cs.n_xe) {
+    if (part == 1) {
+        if (t >= cs.n_xe) return;
         const unsigned r = cs.gx.div(t);
         const unsigned e = t - r * cs.gx.d;
         g = e < (unsigned)cs.g_lo ? (int)e : cs.g_hi + 1 + (int)(e - cs.g_lo);
@@ -1257,7 +1291,6 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
         k = 1 + (int)kk;
         j = 1 + (int)(r - kk * cs.yin.d);
     } else {
-        t -= cs.n_xe;
         if (t >= cs.n_face) return;
         const unsigned r = cs.g.div(t);
         g = (int)(t - r * cs.g.d);
@@ -1317,16 +1350,24 @@ __global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L
             if (rout) stv<R, W>(rout + (cc ? L.half : 0) + o0, r4);
         }
     };
-    const unsigned stride = gridDim.x * TPB;
-    for (unsigned t = blockIdx.x * TPB + threadIdx.x; t < cs.n_in; t += stride) {
-        const unsigned r = cs.gin.div(t);
-        const int g = cs.g_lo + (int)(t - r * cs.gin.d);
-        const unsigned kk = cs.yin.div(r);
-        group(1 + (int)(r - kk * cs.yin.d), 1 + (int)kk, g, std::true_type());
-    }
-    for (unsigned t = blockIdx.x * TPB + threadIdx.x; t < cs.n_xe + cs.n_face; t += stride) {
+    // block-sized chunks, grid-stride, in the interleaved order of split_chunk
+    const unsigned nchunks = cs.nb_in + cs.nb_xe + cs.nb_face;
+    for (unsigned ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        int part;
+        unsigned idx;
+        split_chunk(cs.nb_in, cs.nb_xe, ch, part, idx);
+        const unsigned t = idx * TPB + threadIdx.x;
+        if (part == 0) {
+            if (t >= cs.n_in) continue;
+            const unsigned r = cs.gin.div(t);
+            const int g = cs.g_lo + (int)(t - r * cs.gin.d);
+            const unsigned kk = cs.yin.div(r);
+            group(1 + (int)(r - kk * cs.yin.d), 1 + (int)kk, g, std::true_type());
+            continue;
+        }
         int j, k, g;
-        if (t < cs.n_xe) {
+        if (part == 1) {
+            if (t >= cs.n_xe) continue;
             const unsigned r = cs.gx.div(t);
             const unsigned e = t - r * cs.gx.d;
             g = e < (unsigned)cs.g_lo ? (int)e : cs.g_hi + 1 + (int)(e - cs.g_lo);
@@ -1334,9 +1375,9 @@ __global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L
             k = 1 + (int)kk;
             j = 1 + (int)(r - kk * cs.yin.d);
         } else {
-            const unsigned t2 = t - cs.n_xe;
-            const unsigned r = cs.g.div(t2);
-            g = (int)(t2 - r * cs.g.d);
+            if (t >= cs.n_face) continue;
+            const unsigned r = cs.g.div(t);
+            g = (int)(t - r * cs.g.d);
             shell_row(r, L.ny, cs.b, j, k);
         }
         group(j, k, g, std::false_type());

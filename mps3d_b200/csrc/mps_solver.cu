@@ -565,6 +565,8 @@ static bool make_split(const Lev& L, int W, ColourSplit& cs)
     cs.n_xe = rin * (G - gin);
     cs.n_face = ((unsigned)L.ny * (unsigned)L.nz - rin) * G;
     cs.nb_in = nblk(cs.n_in);
+    cs.nb_xe = nblk(cs.n_xe);
+    cs.nb_face = nblk(cs.n_face);
     cs.b.lo[0] = 0;
     cs.b.hi[0] = L.nx - 1;
     cs.b.lo[1] = 1;
@@ -604,6 +606,8 @@ static RestrictSplit make_restrict_split(const Lev& F, const Lev& C, const Box& 
     rs.n_xe = (unsigned)nJ * (unsigned)nK * (unsigned)(G - ng);
     rs.n_out = ((unsigned)C.ny * (unsigned)C.nz - (unsigned)nJ * (unsigned)nK) * (unsigned)G;
     rs.nb_in = nblk(rs.n_in);
+    rs.nb_xe = nblk(rs.n_xe);
+    rs.nb_out = nblk(rs.n_out);
     rs.rect.lo[0] = 0;
     rs.rect.hi[0] = C.nx - 1;
     rs.rect.lo[1] = rs.J0;
@@ -634,7 +638,7 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
                 ColourSplit cs;
                 if (MPS_COLOUR_SPLIT && make_split(L, W, cs)) {
                     // interior groups without boundary code, the shell apart
-                    const unsigned nbt = cs.nb_in + nblk((long long)cs.n_xe + cs.n_face);
+                    const unsigned nbt = cs.nb_in + cs.nb_xe + cs.nb_face;
                     auto go = [&](auto uc) {
                         constexpr bool UNI = decltype(uc)::value;
                         if (zero_state == 2) {
@@ -738,7 +742,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
                 constexpr int W = decltype(wc)::value, MB = decltype(mbc)::value;
                 const RestrictSplit rs = make_restrict_split(L, C, bx, W);
                 const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
-                const unsigned nbb = rs.nb_in + nblk((long long)rs.n_xe + rs.n_out);
+                const unsigned nbb = rs.nb_in + rs.nb_xe + rs.nb_out;
                 const unsigned nbs = shell > 0 ? nblk(8 * shell) : 0;
                 if (L.uniform)
                     pdl_launch(k_resid_restrict_v<T, W, MB, true>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l),
