@@ -77,14 +77,22 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, out_dir=None):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        self.out_dir = out_dir
+        self.path = None
 
     def __enter__(self):
+        import tempfile
+
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            if self.out_dir:
+                os.makedirs(self.out_dir, exist_ok=True)
+                self.path = os.path.join(self.out_dir, f"clocks_gpu{self.gpu}.csv")
+            else:
+                fd, self.path = tempfile.mkstemp(prefix=f"mps_clocks_gpu{self.gpu}_", suffix=".csv")
+                os.close(fd)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-i", str(self.gpu), "-lms", "200"], stdout=self.f,
@@ -103,7 +111,7 @@ class ClockSampler:
             self.f.close()
 
     def summary(self):
-        if self.proc is None or not os.path.exists(self.path):
+        if self.proc is None or not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -119,38 +127,61 @@ class ClockSampler:
             for nm, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        if not self.out_dir:
+            try:
+                os.remove(self.path)
+            except OSError:
+                pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
 
 # ---------------------------------------------------------------------------
-def oracle_cpu_sample(n, cycles, problem=None):
-    """Consecutive V-cycles of the FP64 restatement of perform_vcycle (the
-    reference hierarchy, mgridlib/mgridsteps.f90:384-579) on the full problem,
-    OpenMP over all host cores.  Returns (seconds per cycle list, rel-residual
-    history, cycles needed to reach 1e-10 at the measured asymptotic rate)."""
-    from mps3d_b200 import workloads as W
+def host_cpu():
+    """nproc, the CPU model (as lscpu names it) and the OpenMP threads used."""
     from oracle import oracle as orc
 
-    p = problem or W.plasma_poisson(n)
+    return {"nproc": os.cpu_count(), "cpu_model": orc.cpu_model(), "threads": orc.get_threads(),
+            "build": "gcc -O3 -march=native -fopenmp (built on this host)" if orc.native_loaded()
+            else "gcc -O3 -march=x86-64-v2 -fopenmp"}
+
+
+def oracle_cpu_solve(p, max_cycles=40, single_thread_cycles=1, tol=1e-10):
+    """The FP64 restatement of perform_vcycle (the reference hierarchy,
+    mgridlib/mgridsteps.f90:384-579) solving ``p`` from a zero guess: V-cycles
+    on all host threads until the relative residual reaches ``tol`` (the
+    reference's caller loop, poissoneq.f90:427-450, with the relative stop
+    test), then ``single_thread_cycles`` more V-cycles on one thread.
+    Returns per-cycle seconds (all threads), the residual history, the cycles
+    the solve needed and the single-thread seconds per cycle."""
+    from oracle import oracle as orc
+
     x = p.zeros_ghosted()
     b = orc.find_bvec(p)
     bn = np.linalg.norm(b)
     times, rel = [], []
-    for _ in range(cycles):
+    while len(rel) < max_cycles:
         t0 = time.perf_counter()
         rms = orc.vcycle(p, x)
         times.append(time.perf_counter() - t0)
         # the reference's RMS residual is sqrt(sum r^2 / N): relative L2 = rms*sqrt(N)/||b||
         rel.append(rms * np.sqrt(p.ncells) / bn)
-    # iterations to 1e-10 from the measured history (asymptotic rate = last ratio)
-    if rel[-1] <= 1e-10:
-        need = next(i + 1 for i, r in enumerate(rel) if r <= 1e-10)
-    else:
-        rate = rel[-1] / rel[-2] if len(rel) > 1 else 0.5
-        rate = min(max(rate, 1e-6), 0.999)
-        need = len(rel) + int(np.ceil(np.log(1e-10 / rel[-1]) / np.log(rate)))
-    return times, rel, need
+        if rel[-1] <= tol:
+            break
+    need = len(rel) if rel[-1] <= tol else None
+    t1 = None
+    if single_thread_cycles:
+        nthr = orc.get_threads()
+        orc.set_threads(1)
+        try:
+            xs = x.copy()
+            t0 = time.perf_counter()
+            for _ in range(single_thread_cycles):
+                orc.vcycle(p, xs)
+            t1 = (time.perf_counter() - t0) / single_thread_cycles
+        finally:
+            orc.set_threads(nthr)
+    return times, rel, need, t1
 
 
 def reference_twin(n):
@@ -161,34 +192,104 @@ def reference_twin(n):
     return n - 1 if n % 2 == 1 else n
 
 
-def run_reference(args, ws, rank):
-    if rank != 0:
-        return 0
-    n = args.n
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+def cpu_baseline_figures(n, problem=None, single_thread_cycles=1):
+    """The reference's own V-cycle loop (oracle port, -march=native, OpenMP)
+    solving the power-of-two twin of the workload to 1e-10 on the host cores:
+    all-thread solves/s from the measured cycles, single-thread solves/s from
+    ``single_thread_cycles`` cycles times the same cycle count."""
     from mps3d_b200 import workloads as W
 
     nt = reference_twin(n)
+    p = problem if (problem is not None and nt == n) else W.plasma_poisson(nt)
+    times, rel, need, t1 = oracle_cpu_solve(p, single_thread_cycles=single_thread_cycles)
+    if need is None:
+        raise RuntimeError(f"the oracle's V-cycle did not reach 1e-10 in {len(rel)} cycles: {rel[-3:]}")
+    t_solve = float(sum(times))
+    hc = host_cpu()
+    out = {"value": 1.0 / t_solve, "unit": UNIT, "cores": hc["threads"], "kind": "port",
+           "s_per_solve": t_solve, "vcycles": need, "s_per_cycle": t_solve / need,
+           "single_thread": None if t1 is None else {"value": 1.0 / (t1 * need), "s_per_cycle": t1,
+                                                     "cycles_timed": single_thread_cycles},
+           "nproc": hc["nproc"], "cpu_model": hc["cpu_model"], "build": hc["build"],
+           "rel_residual_history": rel,
+           "sample": f"one full solve from zero to 1e-10 relative residual ({need} V-cycles, {t_solve:.1f} s) of the "
+                     f"FP64 restatement of perform_vcycle on the {nt}^3 power-of-two twin of the {n}^3 problem "
+                     f"(the reference hierarchy cannot coarsen {n}), {hc['threads']} OpenMP threads; single-thread: "
+                     f"{single_thread_cycles} V-cycle(s) on one thread x {need}"}
+    return out, nt
+
+
+def run_reference(args, ws, rank):
+    """The reference arm: one step = one V-cycle of the reference's own loop
+    (oracle port of perform_vcycle, -march=native, all host threads) on the
+    power-of-two twin, W warm-up cycles then K timed cycles of one solve from
+    zero; solves/s = 1 / (mean timed cycle x the cycles the same run needed to
+    reach 1e-10)."""
+    if rank != 0:
+        return 0
+    from mps3d_b200 import workloads as W
+
+    n = args.n
+    os.environ.setdefault("MPS_ORACLE_NATIVE", "1")
+    nt = reference_twin(n)
     p = W.plasma_poisson(nt)
-    times, rel, need = oracle_cpu_sample(nt, args.warmup + args.steps, problem=p)
-    t_cycle = float(np.mean(times[args.warmup:])) if args.steps > 0 else float(np.mean(times))
-    value = 1.0 / (t_cycle * need)
-    sample = (f"{args.steps} timed V-cycles (after {args.warmup}) of the FP64 restatement of perform_vcycle on the "
-              f"{nt}^3 power-of-two twin of the {n}^3 problem (the reference hierarchy diverges on odd periodic "
-              f"sizes), {cores} OpenMP threads; {t_cycle:.3f} s/cycle x {need} cycles to 1e-10 (rate measured "
-              f"from the same cycles)")
+    times, rel, need, _ = oracle_cpu_solve(p, max_cycles=args.warmup + args.steps, single_thread_cycles=0, tol=0.0)
+    timed = times[args.warmup:] if args.steps > 0 else times
+    t_cycle = float(np.mean(timed))
+    reached = next((i + 1 for i, r in enumerate(rel) if r <= 1e-10), None)
+    if reached is None:  # the run was too short to reach the tolerance: asymptotic rate of its last cycles
+        rate = min(max(rel[-1] / rel[-2], 1e-6), 0.999) if len(rel) > 1 else 0.5
+        reached = len(rel) + int(np.ceil(np.log(1e-10 / rel[-1]) / np.log(rate)))
+        how = f"{reached} cycles to 1e-10 extrapolated from the last cycles' rate"
+    else:
+        how = f"{reached} cycles to 1e-10 measured in the same run"
+    value = 1.0 / (t_cycle * reached)
+    hc = host_cpu()
+    sample = (f"{len(timed)} timed V-cycles (after {args.warmup}) of one solve from zero with the FP64 restatement of "
+              f"perform_vcycle on the {nt}^3 power-of-two twin of the {n}^3 problem (the reference hierarchy cannot "
+              f"coarsen {n}), {hc['threads']} OpenMP threads, {hc['build']}; {t_cycle:.3f} s/cycle x {how}")
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_cycle * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(n, {"reference_twin_cells": nt ** 3,
                                       "hierarchy": "reference CELL (l/2 integer division), RB-GS 2/2, GMRES bottom"}),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": hc["threads"], "kind": "port", "sample": sample,
+                         "nproc": hc["nproc"], "cpu_model": hc["cpu_model"], "build": hc["build"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_rel_residual_history": rel,
     }
     print(json.dumps(out))
     return 0
+
+
+# ---------------------------------------------------------------------------
+def oracle_reference(p, krylov=False):
+    """The FP64 oracle's solution of ``p`` (GEOM hierarchy, converged to
+    1e-13), its right-hand side and fine-level rows: the checker of the GPU
+    solutions reported beside each figure."""
+    from oracle import oracle as orc
+
+    mg = orc.RowsMG(p, hier=orc.HIER_GEOM)
+    b = orc.build_rhs(p)
+    if krylov:
+        x, hist = mg.fgmres(b, m=30, maxit=200, tol=1e-13)
+    else:
+        x, hist = mg.solve(b, maxit=80, tol=1e-13)
+    return x, b, mg.rows(0), float(hist[-1])
+
+
+def vs_oracle(p, x_ghosted, ref):
+    """Relative residual of a GPU solution evaluated by the oracle (its rows
+    and right-hand side) and its relative error against the oracle's
+    converged FP64 solution."""
+    from oracle import oracle as orc
+
+    x_ref, b, rows, _ = ref
+    xi = np.ascontiguousarray(np.asarray(x_ghosted)[1:-1, 1:-1, 1:-1])
+    rr = float(np.linalg.norm(b - orc.rows_apply(p, rows, xi)) / np.linalg.norm(b))
+    err = float(np.linalg.norm(xi - x_ref) / np.linalg.norm(x_ref))
+    return {"rel_res_by_oracle": rr, "rel_err_vs_oracle": err}
 
 
 # ---------------------------------------------------------------------------
@@ -259,9 +360,13 @@ def bench_poisson65(args, ws, rank, h, dev):
     x = torch.zeros(p.ghost_shape, dtype=torch.float64, device=f"cuda:{dev}")
     out = {"workload": "Poisson 65^3, unit cube, coefficient 1, Dirichlet 0, U[-1,1] source, 1e-10 rel. residual",
            "unit": "solves/s"}
+    check = rank == 0 and ws == 1 and not args.skip_oracle
+    ref = oracle_reference(p) if check else None
     for prec in ("mixed", "fp64"):
         ms, info = timed_solves(dp, x, h, args.steps, ws, precision=prec, tol=1e-10, maxit=60)
         out[prec] = {"value": ws * 1e3 / ms, "ms_per_solve": ms, "iters": info["iters"], "rel_res": info["rel_res"]}
+        if check:
+            out[prec].update(vs_oracle(p, x.cpu().numpy(), ref))
     if rank == 0 and ws == 1 and not args.skip_cpu:
         from oracle import oracle as orc
 
@@ -275,7 +380,7 @@ def bench_poisson65(args, ws, rank, h, dev):
     return out
 
 
-def bench_sg_step(args, ws, h, phi_fine, dev):
+def bench_sg_step(args, ws, h, phi_fine, dev, check=False):
     """Implicit SG electron step, 129^3: the potential is the 257^3 plasma
     Poisson solution injected onto 129^3; FGMRES(30) preconditioned by an FP32
     (mixed) or FP64 V-cycle, to 1e-10 relative residual."""
@@ -289,11 +394,14 @@ def bench_sg_step(args, ws, h, phi_fine, dev):
     out = {"workload": "implicit electron drift-diffusion step 129^3, Scharfetter-Gummel faces, dt 1e-11 s, "
                        "periodic x/y, ZGRD z; potential = 257^3 plasma Poisson solution injected",
            "unit": "solves/s", "tol_rel_residual": 1e-10}
+    ref = oracle_reference(p3, krylov=True) if check else None
     for prec in ("mixed", "fp64"):
         ms, info = timed_solves(dp3, x3, h, args.steps, ws, precision=prec, krylov="fgmres", restart=30,
                                 tol=1e-10, maxit=60)
         out[prec] = {"value": ws * 1e3 / ms, "ms_per_solve": ms, "iters": info["iters"],
                      "rel_res": info["rel_res"]}
+        if check:
+            out[prec].update(vs_oracle(p3, x3.cpu().numpy(), ref))
     return out
 
 
@@ -338,6 +446,8 @@ def bench_batch(args, ws, rank, h, dev):
     out = {"workload": "64 Poisson problems, unit cube, cubic sizes from {33,49,65,97,129} (seeded), Dirichlet 0, "
                        "U[-1,1] right-hand sides, 1e-10 relative residual",
            "cells": cells, "unit": "solves/s"}
+    # the oracle's converged FP64 solution of every problem (N=1 only)
+    refs = [oracle_reference(pp) for pp in ps] if (ws == 1 and not args.skip_oracle) else None
     for name, fn, prec in (("batched_mixed", batched, "mixed"), ("batched_fp64", batched, "fp64"),
                            ("sequential_fp64", sequential, "fp64"), ("sequential_mixed", sequential, "mixed")):
         for _ in range(3):
@@ -359,6 +469,10 @@ def bench_batch(args, ws, rank, h, dev):
             out[name] = {"value": 64 * 1e3 / ms, "ms_per_batch": ms,
                          "max_rel_res": max(i["rel_res"] for i in every),
                          "iters": sorted({i["iters"] for i in every})}
+        if refs is not None:
+            checks = [vs_oracle(pp, xx.cpu().numpy(), rr) for pp, xx, rr in zip(ps, xs, refs)]
+            out[name]["max_rel_res_by_oracle"] = max(c["rel_res_by_oracle"] for c in checks)
+            out[name]["max_rel_err_vs_oracle"] = max(c["rel_err_vs_oracle"] for c in checks)
     if rank == 0:
         out["batched_mixed_over_sequential_fp64"] = out["batched_mixed"]["value"] / out["sequential_fp64"]["value"]
         out["ranks"] = ws
@@ -397,7 +511,7 @@ def bench_adjoint(args, ws, h, dev):
     ms = dist_max(e0.elapsed_time(e1), ws) / steps
     # central differences on the FP64 model (mobility perturbed in FP64)
     tight = ElectronFluxAdjoint(case, device=f"cuda:{dev}", handle=h, tol=1e-13)
-    _, gV_t, gmu_t = tight.gradient(V, mu)
+    _, gV_t, gmu_t = tight.gradient(V, mu.double())  # FP64 mobility: the FP64 gradient
     mu64 = mu.double()
     f = lambda v, m: float(tight.loss(torch.tensor(v, dtype=torch.float64, device=mu.device), m))  # noqa: E731
     hv = 1e-4 * V
@@ -405,11 +519,23 @@ def bench_adjoint(args, ws, h, dev):
     d = torch.from_numpy(np.random.default_rng(5005).uniform(-1.0, 1.0, size=mu.shape)).to(mu.device) * mu64 * 1e-4
     fd_mu = (f(V, mu64 + d) - f(V, mu64 - d)) / 2.0
     an_mu = float((gmu_t.double() * d).sum())
+    oracle = None
+    if ws == 1 and not args.skip_oracle:
+        # the same model over the FP64 oracle's solves and VJP on the host cores
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from adjoint_oracle import oracle_bvec, oracle_solve
+
+        ref = ElectronFluxAdjoint(case, device="cpu", solve_fn=oracle_solve, bvec_fn=oracle_bvec)
+        L_r, gV_r, gmu_r = ref.gradient(V, mu.double().cpu())
+        g64 = gmu_t.cpu()
+        oracle = {"rel_err_loss": abs(L0 - L_r) / abs(L_r), "rel_err_dL_dV": abs(gV_t - gV_r) / abs(gV_r),
+                  "rel_err_dL_dmu": float((g64 - gmu_r).norm() / gmu_r.norm()),
+                  "note": "FP64 mobility on both sides; tolerance 1e-12 (GPU) / 1e-14 (oracle)"}
     return {"workload": "electron flux through z=L after 5 implicit SG steps, 129^3 (plasma Poisson potential with "
                         "electrode voltage V; mobility mu FP32 field); gradients w.r.t. V and mu",
             "unit": "gradients/s", "value": ws * 1e3 / ms, "ms_per_gradient": ms, "loss": L0,
             "dL_dV": gV, "fd_dL_dV": fd_V, "rel_err_V": abs(fd_V - gV_t) / abs(gV_t),
-            "rel_err_mu_directional": abs(fd_mu - an_mu) / abs(an_mu),
+            "rel_err_mu_directional": abs(fd_mu - an_mu) / abs(an_mu), "vs_fp64_oracle_gradient": oracle,
             "fd_step": "1e-4 relative (V; every mobility cell along a random direction)"}
 
 
@@ -448,7 +574,7 @@ def run_ours(args, ws, rank, local):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         infos = []
-        with ClockSampler(dev) as cs:
+        with ClockSampler(dev, args.clocks_out) as cs:
             e0.record()
             for _ in range(args.steps):
                 infos.append(solve(prec))
@@ -469,6 +595,11 @@ def run_ours(args, ws, rank, local):
     _, _, _, prof64 = timed("fp64", profile=True)
     per_mixed = ms_mixed / args.steps
     per_fp64 = ms_fp64 / args.steps
+    # the solutions of both precisions, compared with the oracle below
+    sol = {}
+    for prec in ("mixed", "fp64"):
+        solve(prec)
+        sol[prec] = x.cpu().numpy()
     value = ws * 1e3 / per_mixed
     fp64_value = ws * 1e3 / per_fp64
 
@@ -542,20 +673,22 @@ def run_ours(args, ws, rank, local):
     # ---- CPU baseline: the oracle port on the host cores (rank 0, N=1) ----
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
-        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-        nt = reference_twin(n)
-        times, rel, need = oracle_cpu_sample(nt, args.cpu_cycles, problem=W.plasma_poisson(nt) if nt != n else p)
-        t_cycle = float(np.mean(times[1:] if len(times) > 1 else times))
-        cpu = {"value": 1.0 / (t_cycle * need), "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{len(times)} V-cycles of the FP64 restatement of perform_vcycle on the {nt}^3 power-of-two "
-                         f"twin of the {n}^3 problem ({cores} OpenMP threads), {t_cycle:.3f} s/cycle x {need} "
-                         f"cycles to 1e-10 at the measured rate"}
+        cpu, _ = cpu_baseline_figures(n, problem=p)
+
+    # ---- parity of the reported solutions against the FP64 oracle (rank 0, N=1) ----
+    parity = None
+    if rank == 0 and ws == 1 and not args.skip_oracle:
+        ref = oracle_reference(p)
+        parity = {prec: vs_oracle(p, sol[prec], ref) for prec in ("mixed", "fp64")}
+        parity["oracle_final_rel_res"] = ref[3]
+        del ref
 
     # ---- secondary configurations (figures beside the headline line) ----
     others = {}
     if not args.skip_others and n == 257:
         others["poisson_65"] = bench_poisson65(args, ws, rank, h, dev)
-        others["sg_step_129"] = bench_sg_step(args, ws, h, x, dev)
+        others["sg_step_129"] = bench_sg_step(args, ws, h, x, dev,
+                                              check=rank == 0 and ws == 1 and not args.skip_oracle)
         others["batch64"] = bench_batch(args, ws, rank, h, dev)
         others["adjoint_129"] = bench_adjoint(args, ws, h, dev)
 
@@ -587,6 +720,10 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "final_rel_residual": inf_mixed[-1]["rel_res"],
+        # the headline solutions checked by the FP64 oracle on the same inputs
+        # (relative residual evaluated by the oracle; relative error against
+        # its solve converged to 1e-13)
+        "vs_oracle": parity,
         # live CUDA-event timings of the finest-level launches, per class:
         # launches per solve and microseconds per launch
         "finest_level_us": {
@@ -612,11 +749,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
-    ap.add_argument("--cpu-cycles", type=int, default=3)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-oracle", action="store_true", help="no parity figures against the FP64 oracle")
+    ap.add_argument("--clocks-out", default=None, help="folder for the nvidia-smi clock samples (default: a temp file)")
     ap.add_argument("--skip-others", action="store_true", help="only the headline configuration")
     args = ap.parse_args()
+    # CPU timings use the oracle built for this host's CPU (-march=native)
+    os.environ.setdefault("MPS_ORACLE_NATIVE", "1")
     ws, rank, local = dist_init()
     try:
         if args.impl == "reference":

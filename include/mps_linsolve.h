@@ -257,10 +257,15 @@ int mps_operator_vjp_dev(const mps_grid* g, const double* vel, const double* dco
  *
  * No handle: the call works on the current device and calls no cudaMalloc,
  * cudaFree or allocating library routine.  Its scratch is one static device
- * array of MPS_NOALLOC_SCRATCH_BYTES (32 MiB) that every device which loads
- * this library holds until the process exits.  The first call on a device
- * looks up that array's address on the device; make that first call before
- * any stream capture begins.  Sizes: round_up(lx, 16) * ly * lz must not
+ * array of MPS_NOALLOC_SCRATCH_BYTES (32 MiB).  The CUDA runtime reserves it
+ * on a device when it loads this library's code there -- under the default
+ * lazy module loading that is the first mps_apply_A_noalloc call on that
+ * device (with CUDA_MODULE_LOADING=EAGER, the creation of the device's
+ * context) -- and keeps it until the process exits.  That first call also
+ * looks up the array's address on the device.  So make the first call on
+ * each device early: before the caller's memory pool takes the free HBM
+ * (else the reservation itself can fail, as MPS_ERR_CUDA) and before any
+ * stream capture begins.  Sizes: round_up(lx, 16) * ly * lz must not
  * exceed MPS_NOALLOC_MAX_CELLS (64^3), else MPS_ERR_TOO_LARGE and nothing is
  * launched.  The work is queued on `stream` (NULL = the default stream) and
  * AX is ready when the stream reaches that point.  All calls share the one

@@ -16,10 +16,10 @@ LIB = os.path.join(LIBDIR, "libmps3d_b200.so")
 SOURCES = ["mps_solver.cu", "mps_kernels.cu", "mps_noalloc.cu", "mps_adjoint.cu"]
 HEADERS = ["mps_core.cuh", "mps_kernels.cuh", "mps_batch.cuh", os.path.join("..", "..", "include", "mps_linsolve.h")]
 
-NVCC_FLAGS = [
+ARCH_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "-static-global-template-stub=false",
 ]
 
@@ -40,16 +40,35 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    """Compile every source to an object in parallel (one nvcc per file),
+    then link the shared library."""
     if not force and not _stale():
         return LIB
-    os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    cc = nvcc()
+    jobs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [cc] + ARCH_FLAGS + list(extra or []) + ["-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        jobs.append((subprocess.Popen(cmd, cwd=CSRC, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True),
+                     obj))
+    errors = []
+    for proc, _ in jobs:
+        out, _ = proc.communicate()
+        if proc.returncode != 0:
+            errors.append(out)
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + NVCC_FLAGS + list(extra or []) + ["-o", tmp] + SOURCES
+    link = [cc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp] + [o for _, o in jobs]
     if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+        print(" ".join(link))
+    r = subprocess.run(link, cwd=CSRC, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(tmp, LIB)
     return LIB
 

@@ -9,9 +9,12 @@
 // it takes no handle, owns no workspace and calls no cudaMalloc, cudaFree or
 // allocating library routine.  Its scratch -- the split red/black copies of
 // the coefficient fields, the seven operator rows and the split soln / AX --
-// is one file-scope device array of MPS_NOALLOC_SCRATCH_BYTES (32 MiB),
-// which the CUDA runtime places on every device that loads this library and
-// keeps until the process exits.
+// is one file-scope device array of MPS_NOALLOC_SCRATCH_BYTES (32 MiB).
+// The CUDA runtime reserves it on a device when it loads this file's module
+// there: with the default lazy module loading, at the first call on that
+// device (the cudaGetSymbolAddress below), with CUDA_MODULE_LOADING=EAGER at
+// context creation.  It stays reserved until the process exits, so every
+// later call takes no device memory at all.
 //
 // The kernels are the ones the handle-based mps_apply_A_dev path uses for
 // the row form of the operator (k_pack, k_build_rows, k_transpose_rows,

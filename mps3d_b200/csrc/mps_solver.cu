@@ -16,12 +16,37 @@
 #include <cstdint>
 #include <memory>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
 #include <vector>
 
 #include "../../include/mps_linsolve.h"
+
+#include <cstddef>
+
+// The Fortran module include/mps_linsolve_c.f90 declares bind(C) twins of
+// these structs with the same components in the same order; a Fortran
+// compiler lays them out by the C rules.  These offsets are what that module
+// (and the ctypes mirror in mps3d_b200/capi.py) assume: a change of a struct
+// that moves one fails here instead of corrupting a caller's arguments.
+static_assert(offsetof(mps_grid, llenx) == 16 && sizeof(mps_grid) == 40, "mps_grid layout");
+static_assert(offsetof(mps_solver_opts, tol_kind) == 8 && offsetof(mps_solver_opts, ranks) == 28 &&
+                  offsetof(mps_solver_opts, max_coarse) == 40 && offsetof(mps_solver_opts, flux) == 72 &&
+                  sizeof(mps_solver_opts) == 80,
+              "mps_solver_opts layout");
+static_assert(offsetof(mps_solve_info, rel_res) == 16 && offsetof(mps_solve_info, launches) == 48 &&
+                  sizeof(mps_solve_info) == 56,
+              "mps_solve_info layout");
+static_assert(offsetof(mps_profile, ms) == 32 && offsetof(mps_profile, precision_bytes) == 96 &&
+                  offsetof(mps_profile, cells) == 104 && sizeof(mps_profile) == 112,
+              "mps_profile layout");
+static_assert(offsetof(mps_problem, timederiv) == 40 && offsetof(mps_problem, dt) == 48 &&
+                  offsetof(mps_problem, vel) == 56 && offsetof(mps_problem, bc_code) == 88 &&
+                  offsetof(mps_problem, bcval) == 112 && offsetof(mps_problem, mgridsterm) == 160 &&
+                  offsetof(mps_problem, soln) == 168 && sizeof(mps_problem) == 176,
+              "mps_problem layout");
 #include "mps_kernels.cuh"
 
 namespace mps {
@@ -83,10 +108,12 @@ struct Err {
 struct Arena {
     std::vector<void*> blocks;
     size_t bytes = 0;
+    size_t limit = 0;  // 0: no cap; else get() fails once the arena would exceed it
     void* get(size_t n)
     {
         void* p = nullptr;
         if (n == 0) n = 16;
+        if (limit && bytes + n > limit) return nullptr;
         if (cudaMalloc(&p, n) != cudaSuccess) return nullptr;
         if (cudaMemset(p, 0, n) != cudaSuccess) { cudaFree(p); return nullptr; }
         blocks.push_back(p);
@@ -922,7 +949,7 @@ static void alloc_hier(Ctx& ctx, Hier<T>& H, bool& ok)
     H.AinvT = (double*)ctx.ar.get(sizeof(double) * n * n);
     H.Dprev = (double*)ctx.ar.get(sizeof(double) * n * n);
     H.gj = (int*)ctx.ar.get(sizeof(int) * 4);
-    ok = ok && H.AinvT;
+    ok = ok && H.AinvT && H.Dprev && H.gj;
 }
 
 static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts* o, int need64, int need32)
@@ -1661,6 +1688,12 @@ int mps_create(mps_handle* h, int device)
     if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) { delete H; return MPS_ERR_CUDA; }
     if (cudaSetDevice(dev) != cudaSuccess) { delete H; return MPS_ERR_CUDA; }
     ctx.dev = dev;
+    // optional cap on the grid-dependent workspace (bytes, per arena), for
+    // callers that share the device with other large allocations
+    if (const char* cap = std::getenv("MPS_WORKSPACE_LIMIT_BYTES")) {
+        const long long v = std::atoll(cap);
+        if (v > 0) ctx.ar.limit = ctx.kar.limit = (size_t)v;
+    }
     if (cudaDeviceGetAttribute(&ctx.nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || ctx.nsm < 1) {
         delete H;
         return MPS_ERR_CUDA;
@@ -1920,44 +1953,49 @@ int mps_apply_A_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, c
     zsrc = tmp + ng;
     cudaMemcpyAsync(tmp, soln, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
     cudaMemsetAsync(zsrc, 0, sizeof(double) * ng, s);
-    const double* nob[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     int bcfix[6];
     for (int f = 0; f < 6; f++) bcfix[f] = bc_code[f];
     mps_solve_info info;
     // DIRC/FLUX faces need value arrays for find_bvec; they do not enter A
+    int st = MPS_OK;
     std::vector<double*> fb;
-    const double* bv[6];
-    for (int f = 0; f < 6; f++) {
-        bv[f] = nob[f];
+    const double* bv[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (int f = 0; f < 6 && st == MPS_OK; f++) {
         if (bc_code[f] == BC_DIRC || bc_code[f] == BC_FLUX) {
             size_t n = (f < 2) ? (size_t)g->ly * g->lz : (f < 4 ? (size_t)g->lx * g->lz : (size_t)g->lx * g->ly);
             double* d = nullptr;
-            if (cudaMallocAsync((void**)&d, sizeof(double) * n, s) != cudaSuccess) return MPS_ERR_CUDA;
+            if (cudaMallocAsync((void**)&d, sizeof(double) * n, s) != cudaSuccess) {
+                st = MPS_ERR_CUDA;
+                break;
+            }
             cudaMemsetAsync(d, 0, sizeof(double) * n, s);
             fb.push_back(d);
             bv[f] = d;
         }
     }
-    int st = run_dev(h, g, timederiv, dt, vel, dcoeff, reac, zsrc, bcfix, bv, nullptr, tmp, &o, &info, stream, 1);
-    if (!st) {
+    if (st == MPS_OK)
+        st = run_dev(h, g, timederiv, dt, vel, dcoeff, reac, zsrc, bcfix, bv, nullptr, tmp, &o, &info, stream, 1);
+    if (st == MPS_OK) {
         const Lev& L = ctx.lev[0];
-        double* out = ctx.w ? ctx.w : nullptr;
-        double* buf = nullptr;
-        if (cudaMallocAsync((void**)&buf, sizeof(double) * 2 * L.half, s) != cudaSuccess) return MPS_ERR_CUDA;
-        out = buf;
-        if (ctx.sig.opclass == 0)
-            k_apply<double, KOp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, s>>>(
-                L, ctx.kop64, csplit<double>(ctx.x64, L), split<double>(out, L));
-        else
-            k_apply<double, ROp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, s>>>(
-                L, ctx.rop64, csplit<double>(ctx.x64, L), split<double>(out, L));
-        k_unpack_nat<double><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, s>>>(L, csplit<double>(out, L), AX);
-        cudaFreeAsync(buf, s);
-        if (cudaGetLastError() != cudaSuccess) st = MPS_ERR_CUDA;
+        double* out = nullptr;
+        if (cudaMallocAsync((void**)&out, sizeof(double) * 2 * L.half, s) != cudaSuccess) {
+            st = MPS_ERR_CUDA;
+        } else {
+            if (ctx.sig.opclass == 0)
+                k_apply<double, KOp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, s>>>(
+                    L, ctx.kop64, csplit<double>(ctx.x64, L), split<double>(out, L));
+            else
+                k_apply<double, ROp<double>, double><<<nblk((long long)L.P * L.rows), TPB, 0, s>>>(
+                    L, ctx.rop64, csplit<double>(ctx.x64, L), split<double>(out, L));
+            k_unpack_nat<double><<<nblk((long long)L.nx * L.ny * L.nz), TPB, 0, s>>>(L, csplit<double>(out, L), AX);
+            cudaFreeAsync(out, s);
+            if (cudaGetLastError() != cudaSuccess) st = MPS_ERR_CUDA;
+        }
     }
+    // every exit path frees what this call allocated and waits for the stream
     for (double* d : fb) cudaFreeAsync(d, s);
     cudaFreeAsync(tmp, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess && st == MPS_OK) st = MPS_ERR_CUDA;
     return st;
 }
 

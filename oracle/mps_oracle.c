@@ -1516,6 +1516,7 @@ static void mg_rec(orc_mg* mg, int l, double* u, const double* f)
         orc_grid gl = mg->g; gl.lx = fd.lx; gl.ly = fd.ly; gl.lz = fd.lz;
         orc_rows_apply(&gl, mg->bc, mg->rows[l], u, r);
     }
+#pragma omp parallel for schedule(static)
     for (long c = 0; c < n; c++) r[c] = f[c] - r[c];
     double* fc = mg->f[l + 1];
     double* uc = mg->u[l + 1];
@@ -1544,6 +1545,7 @@ static void mg_rec(orc_mg* mg, int l, double* u, const double* f)
     prolongg(&mg->g, &mg->geo[l], &mg->geo[l + 1], mg->bc, eg, ef);
     {
         int lx = fd.lx, ly = fd.ly;
+#pragma omp parallel for schedule(static)
         for (int k = 1; k <= fd.lz; k++)
             for (int j = 1; j <= fd.ly; j++)
                 for (int i = 1; i <= fd.lx; i++)
@@ -1559,9 +1561,15 @@ void orc_mg_vcycle(orc_mg* mg, double* u, const double* f) { mg_rec(mg, 0, u, f)
 static double dot(const double* a, const double* b, long n)
 {
     double s = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : s)
     for (long i = 0; i < n; i++) s += a[i] * b[i];
     return s;
 }
+
+/* host threads of the oracle's OpenMP loops (the CPU baseline times one
+ * thread and all threads) */
+void orc_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }
+int orc_get_threads(void) { return omp_get_max_threads(); }
 
 int orc_mg_solve(orc_mg* mg, const double* b, double* x, int maxit, double tol, double* relres_out)
 {
@@ -1576,12 +1584,14 @@ int orc_mg_solve(orc_mg* mg, const double* b, double* x, int maxit, double tol, 
     double rel = 0.0;
     for (;;) {
         orc_rows_apply(&gl, mg->bc, mg->rows[0], x, r);
+#pragma omp parallel for schedule(static)
         for (long c = 0; c < n; c++) r[c] = b[c] - r[c];
         rel = sqrt(dot(r, r, n)) / bn;
         if (relres_out) relres_out[it] = rel;
         if (rel <= tol || it >= maxit) break;
         memset(e, 0, sizeof(double) * n);
         orc_mg_vcycle(mg, e, r);
+#pragma omp parallel for schedule(static)
         for (long c = 0; c < n; c++) x[c] += e[c];
         it++;
     }
@@ -1631,6 +1641,7 @@ int orc_fgmres(orc_mg* mg, const double* b, double* x, int m, int maxit, double 
                 for (int i = 0; i <= j; i++) {
                     double h = dot(V + n * i, w, n);
                     HH(i, j) += h;
+#pragma omp parallel for schedule(static)
                     for (long c = 0; c < n; c++) w[c] -= h * V[n * i + c];
                 }
             double hn = sqrt(dot(w, w, n));
@@ -1659,6 +1670,7 @@ int orc_fgmres(orc_mg* mg, const double* b, double* x, int m, int maxit, double 
             y[i] = s / HH(i, i);
         }
         for (int i = 0; i < j; i++)
+#pragma omp parallel for schedule(static)
             for (long c = 0; c < n; c++) x[c] += y[i] * Z[n * i + c];
     }
 #undef HH

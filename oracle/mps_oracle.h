@@ -112,6 +112,10 @@ int orc_fgmres(orc_mg* mg, const double* b, double* x, int m, int maxit, double 
 int orc_mg_solve(orc_mg* mg, const double* b, double* x, int maxit, double tol,
                  double* relres_out);
 
+/* OpenMP threads of the oracle's parallel loops (<= 0: unchanged) */
+void orc_set_threads(int n);
+int orc_get_threads(void);
+
 #ifdef __cplusplus
 }
 #endif

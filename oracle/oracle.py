@@ -15,6 +15,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "_build", "libmps_oracle.so")
+# the -march=native build used for CPU-baseline timings: compiled on the host
+# that runs it, into a folder named after that host's CPU, never shipped
+NATIVE_ENV = "MPS_ORACLE_NATIVE"
 
 HIER_CELL = 0
 HIER_GEOM = 1
@@ -22,6 +25,31 @@ HIER_GEOM = 1
 
 def build():
     subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (as lscpu prints it)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _native_path():
+    import hashlib
+    import platform
+
+    tag = hashlib.sha1((cpu_model() + platform.machine()).encode()).hexdigest()[:10]
+    return os.path.join(HERE, "_build", "native-" + tag)
+
+
+def build_native() -> str:
+    d = _native_path()
+    subprocess.check_call(["make", "-s", "-C", HERE, "native", f"NATIVE_DIR={d}"])
+    return os.path.join(d, "libmps_oracle.so")
 
 
 class _Grid(C.Structure):
@@ -39,9 +67,13 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIBPATH):
-            build()
-        L = C.CDLL(LIBPATH)
+        if os.environ.get(NATIVE_ENV) == "1":
+            path = build_native()  # make rebuilds it only when the sources changed
+        else:
+            path = LIBPATH
+            if not os.path.exists(path):
+                build()
+        L = C.CDLL(path)
         dp = C.POINTER(C.c_double)
         ip = C.POINTER(C.c_int)
         gp = C.POINTER(_Grid)
@@ -74,8 +106,23 @@ def lib():
         L.orc_fgmres.restype = C.c_int
         L.orc_mg_solve.argtypes = [C.c_void_p, dp, dp, C.c_int, C.c_double, dp]
         L.orc_mg_solve.restype = C.c_int
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_get_threads.restype = C.c_int
         _lib = L
     return _lib
+
+
+def set_threads(n: int):
+    lib().orc_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return lib().orc_get_threads()
+
+
+def native_loaded() -> bool:
+    """True when the -march=native build is the one loaded."""
+    return _lib is not None and os.environ.get(NATIVE_ENV) == "1"
 
 
 def _p(a):

@@ -168,6 +168,23 @@ def test_failures_return_status(handle):
     assert info["status"] == 0
 
 
+def test_workspace_allocation_failure_is_a_clean_status(monkeypatch):
+    """A handle whose workspace cap (MPS_WORKSPACE_LIMIT_BYTES, read by
+    mps_create) is too small for the grid fails the set-up with
+    MPS_ERR_NOMEM before any kernel runs, and stays usable for a grid that
+    fits."""
+    monkeypatch.setenv("MPS_WORKSPACE_LIMIT_BYTES", str(4 << 20))
+    h = capi.Handle(0)
+    monkeypatch.delenv("MPS_WORKSPACE_LIMIT_BYTES")
+    for prec in ("fp64", "mixed"):
+        with pytest.raises(capi.SolverError) as e:
+            solver.linsolve(W.poisson_dirichlet(65), handle=h, precision=prec)
+        assert e.value.status == capi.MPS_ERR_NOMEM
+    x, info = solver.linsolve(W.poisson_dirichlet(9), handle=h)
+    assert info["status"] == 0
+    h.close()
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_electron_sg_step_matches_oracle(handle, prec):
     """Implicit SG electron step (potential: a 33^3 plasma Poisson solve

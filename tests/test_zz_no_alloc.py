@@ -8,10 +8,17 @@ a row with different grids (the second smaller, so the first call's data is
 still in the array) and checks each against the handle-based mps_apply_A_dev
 at the operator tolerance of the other parity tests.  It also checks that a
 call leaves the device's free memory unchanged and that a grid past the limit
-is refused before anything runs.  The file name makes pytest collect it last;
-it passes alone in a fresh process as well.
+is refused before anything runs, and, in a fresh process, that the first
+call on a device takes no more device memory than the static array itself
+(the CUDA runtime reserves the array when that call loads the library's code
+on the device) while later calls take none.  The file name makes pytest
+collect it last; it passes alone in a fresh process as well.
 """
 import gc
+import json
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -19,6 +26,7 @@ import pytest
 torch = pytest.importorskip("torch")
 
 from mps3d_b200 import capi, solver, workloads as W  # noqa: E402
+from oracle import oracle as O  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -49,6 +57,13 @@ def test_noalloc_matches_apply_A_dev_on_consecutive_calls():
         torch.cuda.synchronize()
         assert torch.isfinite(out).all()
         assert _rel(out, ref) <= OP_TOL
+        # and against the FP64 oracle's rows directly (upwind or SG, A or A^T)
+        rows = O.build_rows(p)
+        if transpose:
+            rows = O.rows_transpose(p, rows)
+        ui = np.ascontiguousarray(u.cpu().numpy()[1:-1, 1:-1, 1:-1])
+        want = torch.from_numpy(O.rows_apply(p, rows, ui))
+        assert _rel(out.cpu(), want) <= OP_TOL
 
 
 def test_noalloc_leaves_free_memory_unchanged():
@@ -87,3 +102,44 @@ def test_noalloc_refuses_grids_past_the_limit():
     got = solver.apply_A_noalloc(dq, v)
     torch.cuda.synchronize()
     assert _rel(got, ref) <= OP_TOL
+
+
+_FIRST_CALL = r"""
+import json, sys
+import numpy as np
+import torch
+sys.path.insert(0, %r)
+from mps3d_b200 import solver, workloads as W
+p = W.random_operator(17, 16, 15, bc=["PERI", "PERI", "DIRC", "ZGRD", "DIRC", "FLUX"], seed=21, vel=True,
+                      reac=True, timederiv=True, flux=1)
+dp = solver.DeviceProblem(p)
+u = torch.from_numpy(np.random.default_rng(28).standard_normal(p.ghost_shape)).cuda()
+out = torch.empty(p.shape, dtype=torch.float64, device="cuda")
+torch.cuda.synchronize()
+free0, _ = torch.cuda.mem_get_info()
+solver.apply_A_noalloc(dp, u, out=out)
+torch.cuda.synchronize()
+free1, _ = torch.cuda.mem_get_info()
+for _ in range(3):
+    solver.apply_A_noalloc(dp, u, out=out)
+torch.cuda.synchronize()
+free2, _ = torch.cuda.mem_get_info()
+print(json.dumps({"free0": free0, "free1": free1, "free2": free2, "finite": bool(torch.isfinite(out).all())}))
+"""
+
+
+def test_noalloc_first_call_in_fresh_process_reserves_only_the_scratch():
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ)
+    env.pop("CUDA_MODULE_LOADING", None)  # the default: lazy loading
+    r = subprocess.run([sys.executable, "-c", _FIRST_CALL % root], capture_output=True, text=True, env=env,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["finite"]
+    # the first call loads the library's module on the device: the 32 MiB
+    # array plus the module's code (a few MiB at most)
+    taken = d["free0"] - d["free1"]
+    assert taken <= capi.NOALLOC_SCRATCH_BYTES + (16 << 20), taken
+    # from then on no call takes device memory
+    assert d["free2"] >= d["free1"]
