@@ -121,13 +121,15 @@ def test_config4_batch_of_64(handle, batch64, prec):
         check(p, x.cpu().numpy(), ref)
 
 
-def test_config5_gradient_33_matches_fp64_oracle():
+@pytest.mark.parametrize("n", [33, 129])
+def test_config5_gradient_matches_fp64_oracle(n):
     """The electron-flux gradient (5 implicit SG steps, V and the FP32
-    mobility field) at 33^3 against the same model over the FP64 oracle."""
+    mobility field) at 33^3 and at the configuration's 129^3 against the same
+    model over the FP64 oracle."""
     from adjoint_oracle import oracle_bvec, oracle_solve
     from mps3d_b200.adjoint import ElectronFluxAdjoint
 
-    case = W.electron_adjoint_case(33)
+    case = W.electron_adjoint_case(n)
     V = case["v_front"]
     mu = torch.from_numpy(case["mu"])
     gpu = ElectronFluxAdjoint(case, device="cuda", tol=1e-12)
