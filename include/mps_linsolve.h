@@ -247,6 +247,85 @@ int mps_operator_vjp_dev(const mps_grid* g, const double* vel, const double* dco
                          const mps_solver_opts* opts, double* gvel, double* gdcoeff,
                          double* greac, void* stream);
 
+/* ---- on-device operator assembly and the implicit plasma step ----------
+ * The producers the reference runs on the host before each solve, as
+ * kernels writing the solver's inputs (ghosted Fortran-order fields) in
+ * device memory.  Queued on `stream` (NULL = the legacy default stream), not
+ * waited for; they allocate nothing.  Mobility and diffusivity come in as
+ * fields (the reference's chemistry tables are not part of this library). */
+
+/* update_efield, plasma_pde/poissoneq.f90:565-680: first the ghosts of phi
+ * (update_boundary_ghostvalues with the potential's codes and face values, in
+ * place, :586-587), then E = -scale * grad(phi) by central differences
+ * (:593-611; scale = potscale/lscale, :667), minmod-limited per direction
+ * when limiter != 0 (gradient_limiter_flag, :614-662); efield = 3 ghosted
+ * fields whose ghosts copy the first interior value (codes 'ZGRD', :582),
+ * periodic faces wrapping. */
+int mps_efield_dev(const mps_grid* g, const int phi_bc[6], const double* const phi_bcval[6], double* phi,
+                   double scale, int limiter, double* efield, void* stream);
+
+/* eden_update_transport, plasma_pde/edeneq.f90:360-444: vel = mu_e E *
+ * scaling[0] (mu_e signed, negative for electrons), dcoeff = D * scaling[1]
+ * (D = |mu_e| te when dco is NULL), source = prod * scaling[2] (prod may be
+ * NULL) + n_old/dt when timederiv (:441); ghosts zero.  scaling NULL = 1,1,1
+ * (SI units; the reference's vel/dcoeff/source_scaling, edeneq.f90:82-85). */
+int mps_eden_transport_dev(const mps_grid* g, const double* efield, const double* mu_e, const double* dco,
+                           const double* te, const double* prod, const double* n_old, int timederiv, double dt,
+                           const double scaling[3], double* vel, double* dcoeff, double* source, void* stream);
+
+/* poisson_update_transport, plasma_pde/poissoneq.f90:335-385: source =
+ * (sum_s charge[s] n_ion[s] - n_e) * scale (scale = ECHARGE/EPS0 *
+ * source_scaling) + phi_old/dt when phi_old is given (:382); n_ion holds
+ * nspec ghosted fields one after another, charge is a device array. */
+int mps_poisson_source_dev(const mps_grid* g, const double* n_e, int nspec, const double* n_ion,
+                           const double* charge, double scale, const double* phi_old, double dt, double* source,
+                           void* stream);
+
+/* The potential and electron parts of one implicit time step
+ * (plasma_pde/solve_manager.f90:363-502): Poisson source, potential solve,
+ * E field, electron operator, implicit electron solve from n_old, the floor
+ * n_e >= nemin and the electron ghosts (eden_solve, edeneq.f90:446-525).
+ * All fields are device pointers in the reference's ghosted layout. */
+typedef struct mps_plasma_step {
+    mps_grid g;
+    /* potential */
+    int phi_bc[6];
+    const double* phi_bcval[6];   /* face values of DIRC/FLUX faces */
+    const double* eps;            /* permittivity: the Poisson operator's dcoeff */
+    double* phi;                  /* in: initial guess; out: potential with its ghosts */
+    double rho_scale;             /* ECHARGE/EPS0 * source_scaling */
+    int nion;                     /* ion species in n_ion */
+    const double* n_ion;          /* nion ghosted densities, one after another */
+    const double* ion_charge;     /* nion charge numbers (device) */
+    double* phi_source;           /* workspace: the Poisson source */
+    /* electrons */
+    int ne_bc[6];
+    const double* ne_bcval[6];
+    double* n_e;                  /* in: n_old; out: n_new, floored, ghosts set */
+    const double* mu_e;           /* signed electron mobility */
+    const double* d_e;            /* diffusivity, or NULL: |mu_e| te */
+    const double* te;             /* electron temperature in volts (when d_e is NULL) */
+    const double* prod_e;         /* production, or NULL */
+    double dt;
+    double nemin;                 /* floor of n_e */
+    double efield_scale;          /* potscale/lscale; 1 in SI units */
+    int limiter;                  /* 1: minmod-limited E */
+    double vel_scaling, dcoeff_scaling, source_scaling;
+    double* efield;               /* out: E (3 fields) */
+    double* vel;                  /* out: electron drift (3 fields) */
+    double* dcoeff;               /* out: electron diffusivity */
+    double* source;               /* out: electron source */
+} mps_plasma_step;
+
+/* hp solves the potential (opts_phi), he the electrons (opts_e: typically
+ * flux SG with FGMRES); two handles keep both workspaces resident.  The step
+ * is ordered on `stream` (NULL = the legacy default stream).  Returns the
+ * first failing status (MPS_ERR_NOT_CONVERGED of a solve is passed on after
+ * the step completes). */
+int mps_plasma_step_dev(mps_handle hp, mps_handle he, const mps_plasma_step* step,
+                        const mps_solver_opts* opts_phi, const mps_solver_opts* opts_e,
+                        mps_solve_info* info_phi, mps_solve_info* info_e, void* stream);
+
 /* AX = A soln like mps_apply_A_dev, for callers that must not allocate device
  * memory.  No counterpart in the reference: its find_AX works on arrays the
  * caller already owns, so it never needed one.  Callers that cannot allocate

@@ -75,6 +75,24 @@ module mps_linsolve_c
         type(c_ptr) :: mgridsterm, soln
     end type
 
+    ! the fields of one implicit potential + electron step (device pointers)
+    type, bind(C) :: mps_plasma_step
+        type(mps_grid) :: g
+        integer(c_int) :: phi_bc(6)
+        type(c_ptr) :: phi_bcval(6)
+        type(c_ptr) :: eps, phi
+        real(c_double) :: rho_scale
+        integer(c_int) :: nion
+        type(c_ptr) :: n_ion, ion_charge, phi_source
+        integer(c_int) :: ne_bc(6)
+        type(c_ptr) :: ne_bcval(6)
+        type(c_ptr) :: n_e, mu_e, d_e, te, prod_e
+        real(c_double) :: dt, nemin, efield_scale
+        integer(c_int) :: limiter
+        real(c_double) :: vel_scaling, dcoeff_scaling, source_scaling
+        type(c_ptr) :: efield, vel, dcoeff, source
+    end type
+
     interface
         subroutine mps_default_opts(o) bind(C, name="mps_default_opts")
             import :: mps_solver_opts
@@ -223,6 +241,59 @@ module mps_linsolve_c
             type(c_ptr), value :: lam, u
             type(c_ptr), value :: opts          ! c_null_ptr: upwind flux
             type(c_ptr), value :: gvel, gdcoeff, greac
+            type(c_ptr), value :: stream
+        end function
+
+        ! update_efield, plasma_pde/poissoneq.f90:565-680
+        integer(c_int) function mps_efield_dev(g, phi_bc, phi_bcval, phi, scale, limiter, efield, stream) &
+                bind(C, name="mps_efield_dev")
+            import :: c_ptr, c_int, c_double, mps_grid
+            type(mps_grid), intent(in) :: g
+            integer(c_int), intent(in) :: phi_bc(6)
+            type(c_ptr), intent(in) :: phi_bcval(6)
+            type(c_ptr), value :: phi
+            real(c_double), value :: scale
+            integer(c_int), value :: limiter
+            type(c_ptr), value :: efield
+            type(c_ptr), value :: stream
+        end function
+
+        ! eden_update_transport, plasma_pde/edeneq.f90:360-444
+        integer(c_int) function mps_eden_transport_dev(g, efield, mu_e, dco, te, prod, n_old, timederiv, dt, &
+                scaling, vel, dcoeff, source, stream) bind(C, name="mps_eden_transport_dev")
+            import :: c_ptr, c_int, c_double, mps_grid
+            type(mps_grid), intent(in) :: g
+            type(c_ptr), value :: efield, mu_e, dco, te, prod, n_old
+            integer(c_int), value :: timederiv
+            real(c_double), value :: dt
+            real(c_double), intent(in) :: scaling(3)
+            type(c_ptr), value :: vel, dcoeff, source
+            type(c_ptr), value :: stream
+        end function
+
+        ! poisson_update_transport, plasma_pde/poissoneq.f90:335-385
+        integer(c_int) function mps_poisson_source_dev(g, n_e, nspec, n_ion, charge, scale, phi_old, dt, &
+                source, stream) bind(C, name="mps_poisson_source_dev")
+            import :: c_ptr, c_int, c_double, mps_grid
+            type(mps_grid), intent(in) :: g
+            type(c_ptr), value :: n_e
+            integer(c_int), value :: nspec
+            type(c_ptr), value :: n_ion, charge
+            real(c_double), value :: scale
+            type(c_ptr), value :: phi_old
+            real(c_double), value :: dt
+            type(c_ptr), value :: source
+            type(c_ptr), value :: stream
+        end function
+
+        ! potential + electron part of the time step, solve_manager.f90:363-502
+        integer(c_int) function mps_plasma_step_dev(hp, he, step, opts_phi, opts_e, info_phi, info_e, stream) &
+                bind(C, name="mps_plasma_step_dev")
+            import :: c_ptr, c_int, mps_plasma_step, mps_solver_opts, mps_solve_info
+            type(c_ptr), value :: hp, he
+            type(mps_plasma_step), intent(in) :: step
+            type(mps_solver_opts), intent(in) :: opts_phi, opts_e
+            type(mps_solve_info), intent(out) :: info_phi, info_e
             type(c_ptr), value :: stream
         end function
 

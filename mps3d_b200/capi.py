@@ -41,6 +41,7 @@ EXPORTS = [
     "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once", "mps_apply_A_dev", "mps_find_bvec_dev",
     "mps_fill_ghosts_dev", "mps_set_profile", "mps_get_profile", "mps_apply_A_noalloc",
     "mps_linsolve_batched_dev", "mps_operator_vjp_dev",
+    "mps_efield_dev", "mps_eden_transport_dev", "mps_poisson_source_dev", "mps_plasma_step_dev",
 ]
 
 PROF_SMOOTH, PROF_RESTRICT, PROF_PROLONG, PROF_RESID, PROF_NCLASS = 0, 1, 2, 3, 8
@@ -80,6 +81,19 @@ class ProblemDesc(C.Structure):
     _fields_ = [("g", Grid), ("timederiv", C.c_int), ("dt", C.c_double), ("vel", C.c_void_p),
                 ("dcoeff", C.c_void_p), ("reac", C.c_void_p), ("source", C.c_void_p), ("bc_code", C.c_int * 6),
                 ("bcval", C.c_void_p * 6), ("mgridsterm", C.c_void_p), ("soln", C.c_void_p)]
+
+
+class PlasmaStep(C.Structure):
+    """struct mps_plasma_step: the fields of one implicit potential + electron
+    step (device pointers, ghosted Fortran layout)."""
+    _fields_ = [("g", Grid), ("phi_bc", C.c_int * 6), ("phi_bcval", C.c_void_p * 6), ("eps", C.c_void_p),
+                ("phi", C.c_void_p), ("rho_scale", C.c_double), ("nion", C.c_int), ("n_ion", C.c_void_p),
+                ("ion_charge", C.c_void_p), ("phi_source", C.c_void_p), ("ne_bc", C.c_int * 6),
+                ("ne_bcval", C.c_void_p * 6), ("n_e", C.c_void_p), ("mu_e", C.c_void_p), ("d_e", C.c_void_p),
+                ("te", C.c_void_p), ("prod_e", C.c_void_p), ("dt", C.c_double), ("nemin", C.c_double),
+                ("efield_scale", C.c_double), ("limiter", C.c_int), ("vel_scaling", C.c_double),
+                ("dcoeff_scaling", C.c_double), ("source_scaling", C.c_double), ("efield", C.c_void_p),
+                ("vel", C.c_void_p), ("dcoeff", C.c_void_p), ("source", C.c_void_p)]
 
 
 BATCH_MAX = 4096
@@ -125,7 +139,14 @@ def load(build_if_missing: bool = False):
     L.mps_operator_vjp_dev.argtypes = [C.POINTER(Grid), vp, vp, ip, vp, vp, C.POINTER(Opts), vp, vp, vp, vp]
     L.mps_apply_A_noalloc.argtypes = [C.POINTER(Grid), C.c_int, C.c_double, vp, vp, vp, ip, vp, vp, C.POINTER(Opts),
                                       vp]
-    for name in ("mps_set_profile", "mps_get_profile", "mps_create", "mps_destroy", "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once",
+    L.mps_efield_dev.argtypes = [C.POINTER(Grid), ip, C.POINTER(vp), vp, C.c_double, C.c_int, vp, vp]
+    L.mps_eden_transport_dev.argtypes = [C.POINTER(Grid), vp, vp, vp, vp, vp, vp, C.c_int, C.c_double, dp, vp, vp,
+                                         vp, vp]
+    L.mps_poisson_source_dev.argtypes = [C.POINTER(Grid), vp, C.c_int, vp, vp, C.c_double, vp, C.c_double, vp, vp]
+    L.mps_plasma_step_dev.argtypes = [vp, vp, C.POINTER(PlasmaStep), C.POINTER(Opts), C.POINTER(Opts),
+                                      C.POINTER(Info), C.POINTER(Info), vp]
+    for name in ("mps_efield_dev", "mps_eden_transport_dev", "mps_poisson_source_dev", "mps_plasma_step_dev",
+                 "mps_set_profile", "mps_get_profile", "mps_create", "mps_destroy", "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once",
                  "mps_apply_A_dev", "mps_find_bvec_dev", "mps_fill_ghosts_dev", "mps_apply_A_noalloc",
                  "mps_linsolve_batched_dev", "mps_operator_vjp_dev"):
         getattr(L, name).restype = C.c_int

@@ -212,3 +212,33 @@ def electron_adjoint_case(n: int = 129, v_front: float = 1000.0, length: float =
     nold = _rng(3, 3).lognormal(mean=np.log(1e16), sigma=1.0, size=(n, n, n))
     return {"n": n, "length": length, "dt": dt, "steps": steps, "v_front": v_front, "eps": pp.dcoeff,
             "rho": pp.source, "mu": mu, "te": te, "n_old": nold}
+
+
+def plasma_step_case(n: int = 129, slab_cells: int = None, v_front: float = 1000.0, length: float = 0.01,
+                     dt: float = 1e-11, nemin: float = 1e7):
+    """The potential + electron part of one implicit step on an n^3 grid
+    over a 1 cm cube: the plasma Poisson problem of config 2 (dielectric slab,
+    Dirichlet 0 / v_front on z, periodic x/y) with one singly charged ion
+    species, and the electrons of config 3 (signed mobility
+    -0.03 (1 + 0.5 U[0,1]) m^2/Vs, Te ~ U[1,4] V, D = |mu| Te, dt, periodic
+    x/y and ZGRD z, floor nemin).  Returns a dict of ghosted numpy arrays and
+    settings, and the initial electron density under ``n_e0``."""
+    if slab_cells is None:
+        slab_cells = max(1, int(round(10 * n / 257)))
+    pp = plasma_poisson(n, slab_cells=slab_cells, v_front=v_front, length=length)
+    g = (n + 2,) * 3
+
+    def ghosted(a):
+        out = np.zeros(g)
+        out[1:-1, 1:-1, 1:-1] = a
+        return out
+
+    ni = ghosted(_rng(2, 1).lognormal(mean=np.log(1e16), sigma=1.0, size=(n, n, n)))
+    ne = ghosted(_rng(2, 2).lognormal(mean=np.log(1e16), sigma=1.0, size=(n, n, n)))
+    mu = ghosted(-0.03 * (1.0 + 0.5 * _rng(3, 1).uniform(0.0, 1.0, size=(n, n, n))))
+    te = ghosted(_rng(3, 2).uniform(1.0, 4.0, size=(n, n, n)))
+    return {"shape": (n, n, n), "llen": (length,) * 3, "eps": pp.dcoeff, "phi_bc": list(pp.bc),
+            "phi_bcvals": [None, None, None, None, pp.bcvals[4], pp.bcvals[5]], "n_ion": ni[None], "ion_charge": [1.0],
+            "rho_scale": ECHARGE / EPS0, "ne_bc": ["PERI", "PERI", "PERI", "PERI", "ZGRD", "ZGRD"],
+            "ne_bcvals": [None] * 6, "mu_e": mu, "te": te, "d_e": None, "prod_e": None, "dt": dt, "nemin": nemin,
+            "efield_scale": 1.0, "limiter": False, "scaling": (1.0, 1.0, 1.0), "n_e0": ne}

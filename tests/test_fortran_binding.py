@@ -78,7 +78,8 @@ def c_layout(struct, members):
     return {k: int(v) for k, v in vals.items()}
 
 
-@pytest.mark.parametrize("name", ["mps_grid", "mps_solver_opts", "mps_solve_info", "mps_profile", "mps_problem"])
+@pytest.mark.parametrize("name", ["mps_grid", "mps_solver_opts", "mps_solve_info", "mps_profile", "mps_problem",
+                                  "mps_plasma_step"])
 def test_bind_c_types_match_header_layout(name):
     types = fortran_types()
     assert name in types, f"{name} missing from the Fortran module"
@@ -110,7 +111,7 @@ def _fortran_functions():
 def test_every_header_function_has_a_fortran_interface():
     hdr = _header_functions()
     f90 = _fortran_functions()
-    assert len(hdr) >= 17
+    assert len(hdr) >= 21
     missing = sorted(set(hdr) - set(f90))
     assert not missing, missing
     for name, n in hdr.items():
