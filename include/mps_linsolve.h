@@ -326,6 +326,29 @@ int mps_plasma_step_dev(mps_handle hp, mps_handle he, const mps_plasma_step* ste
                         const mps_solver_opts* opts_phi, const mps_solver_opts* opts_e,
                         mps_solve_info* info_phi, mps_solve_info* info_e, void* stream);
 
+/* ---- VTK output from device buffers (mgridlib/cartwrite.f90) ------------
+ * The reference's RectilinearGrid files byte for byte: XML header, raw
+ * appended Float64 cell data (4-byte size, then the interior in Fortran
+ * order), node coordinates off + (i-1) len/l.  fields are ghosted device
+ * arrays (their interiors are written); names are C strings (trailing blanks
+ * dropped, as Fortran's trim does).  The cell data are gathered and copied
+ * on `stream` (NULL = the legacy default stream) while the previous field is
+ * written; the call returns when the file is complete. */
+
+/* Writeserialvtrfile, cartwrite.f90:8-161: <filename>.vtr; off may be NULL (0). */
+int mps_write_vtr_dev(const char* filename, const mps_grid* g, const double off[3], int nscalars,
+                      const char* const* names, const double* const* fields, void* stream);
+/* Writevtrfile, cartwrite.f90:163-317: <dirname>/file_<rank, 8 digits>.vtr,
+ * the piece of rank `rank` at 1-based block index pind (g = the piece's own
+ * cells and lengths, off = its origin). */
+int mps_write_vtr_piece_dev(const char* dirname, int rank, const int pind[3], const mps_grid* g,
+                            const double off[3], int nscalars, const char* const* names,
+                            const double* const* fields, void* stream);
+/* Writepvtrfile, cartwrite.f90:319-438: creates dirname and writes
+ * <dirname>.pvtr, the index of px*py*pz pieces of lx*ly*lz cells (host only). */
+int mps_write_pvtr(const char* dirname, const int lxyz[3], const int pxyz[3], int nscalars,
+                   const char* const* names);
+
 /* AX = A soln like mps_apply_A_dev, for callers that must not allocate device
  * memory.  No counterpart in the reference: its find_AX works on arrays the
  * caller already owns, so it never needed one.  Callers that cannot allocate

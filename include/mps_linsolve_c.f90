@@ -297,6 +297,41 @@ module mps_linsolve_c
             type(c_ptr), value :: stream
         end function
 
+        ! VTK output, mgridlib/cartwrite.f90 (names: trim(name)//c_null_char)
+        integer(c_int) function mps_write_vtr_dev(filename, g, off, nscalars, names, fields, stream) &
+                bind(C, name="mps_write_vtr_dev")
+            import :: c_ptr, c_int, c_char, c_double, mps_grid
+            character(kind=c_char), intent(in) :: filename(*)
+            type(mps_grid), intent(in) :: g
+            real(c_double), intent(in) :: off(3)
+            integer(c_int), value :: nscalars
+            type(c_ptr), intent(in) :: names(*)
+            type(c_ptr), intent(in) :: fields(*)
+            type(c_ptr), value :: stream
+        end function
+
+        integer(c_int) function mps_write_vtr_piece_dev(dirname, rank, pind, g, off, nscalars, names, fields, &
+                stream) bind(C, name="mps_write_vtr_piece_dev")
+            import :: c_ptr, c_int, c_char, c_double, mps_grid
+            character(kind=c_char), intent(in) :: dirname(*)
+            integer(c_int), value :: rank
+            integer(c_int), intent(in) :: pind(3)
+            type(mps_grid), intent(in) :: g
+            real(c_double), intent(in) :: off(3)
+            integer(c_int), value :: nscalars
+            type(c_ptr), intent(in) :: names(*)
+            type(c_ptr), intent(in) :: fields(*)
+            type(c_ptr), value :: stream
+        end function
+
+        integer(c_int) function mps_write_pvtr(dirname, lxyz, pxyz, nscalars, names) bind(C, name="mps_write_pvtr")
+            import :: c_ptr, c_int, c_char
+            character(kind=c_char), intent(in) :: dirname(*)
+            integer(c_int), intent(in) :: lxyz(3), pxyz(3)
+            integer(c_int), value :: nscalars
+            type(c_ptr), intent(in) :: names(*)
+        end function
+
         ! no handle, no device allocation; stream c_null_ptr is the legacy
         ! default stream here (there is no handle stream)
         integer(c_int) function mps_apply_A_noalloc(g, timederiv, dt, vel, dcoeff, reac, bc_code, &

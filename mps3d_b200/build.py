@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libmps3d_b200.so")
-SOURCES = ["mps_solver.cu", "mps_kernels.cu", "mps_noalloc.cu", "mps_adjoint.cu", "mps_step.cu"]
+SOURCES = ["mps_solver.cu", "mps_kernels.cu", "mps_noalloc.cu", "mps_adjoint.cu", "mps_step.cu", "mps_vtk.cu"]
 HEADERS = ["mps_core.cuh", "mps_kernels.cuh", "mps_batch.cuh", os.path.join("..", "..", "include", "mps_linsolve.h")]
 
 ARCH_FLAGS = [

@@ -42,6 +42,7 @@ EXPORTS = [
     "mps_fill_ghosts_dev", "mps_set_profile", "mps_get_profile", "mps_apply_A_noalloc",
     "mps_linsolve_batched_dev", "mps_operator_vjp_dev",
     "mps_efield_dev", "mps_eden_transport_dev", "mps_poisson_source_dev", "mps_plasma_step_dev",
+    "mps_write_vtr_dev", "mps_write_vtr_piece_dev", "mps_write_pvtr",
 ]
 
 PROF_SMOOTH, PROF_RESTRICT, PROF_PROLONG, PROF_RESID, PROF_NCLASS = 0, 1, 2, 3, 8
@@ -145,7 +146,12 @@ def load(build_if_missing: bool = False):
     L.mps_poisson_source_dev.argtypes = [C.POINTER(Grid), vp, C.c_int, vp, vp, C.c_double, vp, C.c_double, vp, vp]
     L.mps_plasma_step_dev.argtypes = [vp, vp, C.POINTER(PlasmaStep), C.POINTER(Opts), C.POINTER(Opts),
                                       C.POINTER(Info), C.POINTER(Info), vp]
-    for name in ("mps_efield_dev", "mps_eden_transport_dev", "mps_poisson_source_dev", "mps_plasma_step_dev",
+    cp = C.POINTER(C.c_char_p)
+    L.mps_write_vtr_dev.argtypes = [C.c_char_p, C.POINTER(Grid), dp, C.c_int, cp, C.POINTER(vp), vp]
+    L.mps_write_vtr_piece_dev.argtypes = [C.c_char_p, C.c_int, ip, C.POINTER(Grid), dp, C.c_int, cp, C.POINTER(vp),
+                                          vp]
+    L.mps_write_pvtr.argtypes = [C.c_char_p, ip, ip, C.c_int, cp]
+    for name in ("mps_write_vtr_dev", "mps_write_vtr_piece_dev", "mps_write_pvtr", "mps_efield_dev", "mps_eden_transport_dev", "mps_poisson_source_dev", "mps_plasma_step_dev",
                  "mps_set_profile", "mps_get_profile", "mps_create", "mps_destroy", "mps_linsolve", "mps_linsolve_dev", "mps_vcycle_once",
                  "mps_apply_A_dev", "mps_find_bvec_dev", "mps_fill_ghosts_dev", "mps_apply_A_noalloc",
                  "mps_linsolve_batched_dev", "mps_operator_vjp_dev"):

@@ -44,7 +44,7 @@ def _faces(bcvals, device):
 
     out = []
     for v in bcvals:
-        out.append(None if v is None else torch.as_tensor(np.ascontiguousarray(v, dtype=np.float64)).to(device))
+        out.append(None if v is None else torch.from_numpy(np.array(v, dtype=np.float64, order="C")).to(device))
     return out
 
 
