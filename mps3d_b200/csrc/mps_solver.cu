@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -48,6 +49,9 @@ static_assert(offsetof(mps_problem, timederiv) == 40 && offsetof(mps_problem, dt
                   offsetof(mps_problem, soln) == 168 && sizeof(mps_problem) == 176,
               "mps_problem layout");
 #include "mps_kernels.cuh"
+#include "mps_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 namespace mps {
 
@@ -202,6 +206,13 @@ struct Ctx {
     long long kar_n = 0;
     int kar_m = 0;
     Arena inbuf;    // host-API staging of the inputs
+    struct Lane {   // one host thread of the pageable copies: a stream, two pinned buffers
+        cudaStream_t s = nullptr;
+        double* pin[2] = {nullptr, nullptr};
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+    };
+    std::vector<Lane> lanes;  // created at the first host call with pageable arrays
+    bool tma_ok = false;      // the shared-memory colour pass can run (set at workspace set-up)
     size_t inbuf_bytes = 0;
     Signature sig;
     int nlev = 0;
@@ -644,6 +655,148 @@ static RestrictSplit make_restrict_split(const Lev& F, const Lev& C, const Box& 
     return rs;
 }
 
+// ---- the finest colour pass through shared memory (k_colour_tma) ----
+#ifndef MPS_TMA_COLOUR
+#define MPS_TMA_COLOUR 1
+#endif
+#ifndef MPS_TMA_LEVELS
+#define MPS_TMA_LEVELS 1  // the finest level only
+#endif
+#ifndef MPS_TMA_BPS
+#define MPS_TMA_BPS 2  // blocks per SM the tiling aims at
+#endif
+#ifndef MPS_TMA_TJ32
+#define MPS_TMA_TJ32 8
+#endif
+#ifndef MPS_TMA_TJ64
+#define MPS_TMA_TJ64 4
+#endif
+template <class T>
+struct TmaShape {  // rows per block, one warp each; cells per thread
+    static constexpr int TJ = sizeof(T) == 4 ? MPS_TMA_TJ32 : MPS_TMA_TJ64;
+    static constexpr int W = 4;
+};
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && p)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// 3-D map of one colour half (P x ny x nz elements) with boxes of `rows`
+// full rows of one plane
+template <class T>
+static bool encode_half(CUtensorMap* m, const T* base, const Lev& L, int rows)
+{
+    auto fn = tensor_map_encoder();
+    if (!fn) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)L.P, (cuuint64_t)L.ny, (cuuint64_t)L.nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)L.P * sizeof(T), (cuuint64_t)L.P * L.ny * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)L.P, (cuuint32_t)rows, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+              const_cast<T*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the finest level's colour pass from a valid state with k_colour_tma;
+// returns 1 when the pass was launched, 0 when this level or operator does
+// not qualify (the caller runs the register-fed pass), < 0 on an error
+template <class T>
+static int colour_pass_tma(Ctx& ctx, Hier<T>& H, const KOp<T>& op, int l, int c, T* out, const T* fh)
+{
+    constexpr int TJ = TmaShape<T>::TJ, W = TmaShape<T>::W;
+    const Lev& L = ctx.lev[l];
+    // FP32 only: the FP64 pass measured slower through shared memory (104-117
+    // against 87 us at 257^3), the FP32 pass faster (49.6 against 51.2 us)
+    if (sizeof(T) != 4 || !ctx.tma_ok || L.P > 256 || op.dex[0] || L.ny < 3 || L.nz < 3) return 0;
+    ColourSplit cs;
+    if (!make_split(L, W, cs)) return 0;
+    const bool kf = op.k[0] != nullptr;
+    const int oc = c ^ 1;
+    const T* uo = oc == 0 ? H.U[l][H.ri[l]] : H.U[l][H.bi[l]] + L.half;
+    CUtensorMap mU, mKo, mKc, mF;
+    std::memset(&mKo, 0, sizeof(mKo));
+    std::memset(&mKc, 0, sizeof(mKc));
+    if (!encode_half<T>(&mU, uo, L, TJ + 2) || !encode_half<T>(&mF, fh, L, TJ)) return 0;
+    if (kf && (!encode_half<T>(&mKo, op.k[oc], L, TJ + 2) || !encode_half<T>(&mKc, op.k[c], L, TJ))) return 0;
+    TmaColour tc;
+    std::memset(&tc, 0, sizeof(tc));
+    auto pad128 = [](unsigned elems) { return (unsigned)((elems * sizeof(T) + 127) / 128 * 128 / sizeof(T)); };
+    tc.tile_elems = pad128((unsigned)L.P * (TJ + 2));
+    tc.own_elems = pad128((unsigned)L.P * TJ);
+    tc.slot_bytes = (unsigned)(L.P * sizeof(T)) * ((TJ + 2) * (kf ? 2 : 1) + TJ * (kf ? 2 : 1));
+    const size_t smem = kf ? tma_smem_bytes<T, true>(tc) : tma_smem_bytes<T, false>(tc);
+    if (smem > 220 * 1024) return 0;
+    // tiles for the blocks that fit on an SM (shared memory, threads, at most
+    // MPS_TMA_BPS): each tile streams its planes plus two halo planes, so
+    // more tiles re-read more
+    const int bps = std::max(1, std::min({(int)(227 * 1024 / (smem + 1024)), 2048 / (TJ * 32), MPS_TMA_BPS}));
+    // the interior box of the split: rows 1 .. jhi, planes 1 .. khi (one cell
+    // short of merged last cells); the shell blocks take every other row
+    tc.jhi = cs.b.hi[1];
+    tc.khi = cs.b.hi[2];
+    if (cs.b.lo[1] != 1 || cs.b.lo[2] != 1 || tc.jhi < 1 || tc.khi < 1) return 0;
+    tc.njb = (tc.jhi + TJ - 1) / TJ;
+    const int want = std::max(1, ctx.nsm * bps / tc.njb);
+    tc.tk = std::max(1, (tc.khi + want - 1) / want);
+    tc.nkb = (tc.khi + tc.tk - 1) / tc.tk;
+    tc.ntile = tc.njb * tc.nkb;
+    tc.g_lo = cs.g_lo;
+    tc.g_hi = cs.g_hi;
+    tc.n_xe = cs.n_xe;
+    tc.n_face = cs.n_face;
+    const unsigned nsh = tc.n_xe + tc.n_face;
+    tc.nb_shell = std::min<unsigned>((nsh + TJ * 32 - 1) / (TJ * 32), (unsigned)ctx.nsm * 4);
+    tc.flag = ctx.rb.out + 3;
+    auto launch = [&](auto kern) -> int {
+        const cudaError_t e = pdl_launch(kern, tc.ntile + tc.nb_shell, TJ * 32, smem, ctx.s, L, op, c, ccur(H, L, l),
+                                         out, fh, cs, tc, mU, mKo, mKc, mF);
+        if (e != cudaSuccess) {
+            ctx.err.code = MPS_ERR_CUDA;
+            ctx.err.msg = std::string("k_colour_tma launch: ") + cudaGetErrorString(e);
+            return -1;
+        }
+        return 1;
+    };
+    if (L.uniform) return kf ? launch(k_colour_tma<T, W, TJ, true, true>) : launch(k_colour_tma<T, W, TJ, false, true>);
+    return kf ? launch(k_colour_tma<T, W, TJ, true, false>) : launch(k_colour_tma<T, W, TJ, false, false>);
+}
+
+// the attributes the shared-memory colour pass needs, set outside any stream
+// capture (at workspace set-up); false when the device or driver cannot run it
+static bool tma_prepare()
+{
+    static int ready = -1;
+    if (ready >= 0) return ready == 1;
+    ready = 0;
+    if (!MPS_TMA_COLOUR || !tensor_map_encoder()) return false;
+    const int bytes = 220 * 1024;
+    auto set = [&](auto kern) {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+    };
+    constexpr int W32 = TmaShape<float>::W, J32 = TmaShape<float>::TJ;
+    constexpr int W64 = TmaShape<double>::W, J64 = TmaShape<double>::TJ;
+    bool ok = set(k_colour_tma<float, W32, J32, true, true>) && set(k_colour_tma<float, W32, J32, false, true>) &&
+              set(k_colour_tma<float, W32, J32, true, false>) && set(k_colour_tma<float, W32, J32, false, false>) &&
+              set(k_colour_tma<double, W64, J64, true, true>) && set(k_colour_tma<double, W64, J64, false, true>) &&
+              set(k_colour_tma<double, W64, J64, true, false>) && set(k_colour_tma<double, W64, J64, false, false>);
+    if (!ok) cudaGetLastError();
+    ready = ok ? 1 : 0;
+    return ok;
+}
+
 // ---- one colour pass ----
 template <class T, class Op>
 static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zero_state)
@@ -655,6 +808,19 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     if (c == 0) out = H.U[l][H.ri[l] ^ 1];
     else out = H.U[l][H.bi[l] ^ 1] + L.half;
     if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_SMOOTH);
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (l <= MPS_TMA_LEVELS - 1 && zero_state == 0) {
+            const int r = colour_pass_tma<T>(ctx, H, op, l, c, out, fh);
+            if (r < 0) return MPS_ERR_CUDA;
+            if (r == 1) {
+                if (l == ctx.prof.level) prof_end(ctx);
+                CKL();
+                if (c == 0) H.ri[l] ^= 1;
+                else H.bi[l] ^= 1;
+                return 0;
+            }
+        }
+    }
     if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (L.uniform || L.nx >= 16) {
             // vector kernel, W cells per thread (faces at a merged last cell
@@ -920,6 +1086,20 @@ static int fetch(Ctx& ctx, const double* dsrc, int n)
     return 0;
 }
 
+// the residual norms (rb.out[0..1]) and the device failure word rb.out[3],
+// which a kernel whose bounded wait gave up sets (k_colour_tma)
+static int fetch_norms(Ctx& ctx)
+{
+    if (int st = fetch(ctx, ctx.rb.out, 4)) return st;
+    if (ctx.hpin[3] != 0.0) {
+        CK(cudaMemsetAsync(ctx.rb.out + 3, 0, sizeof(double), ctx.s));
+        ctx.err.code = MPS_ERR_TIMEOUT;
+        ctx.err.msg = "a bounded device-side wait expired (colour pass copies)";
+        return MPS_ERR_TIMEOUT;
+    }
+    return 0;
+}
+
 // ----------------------------------------------------------------------
 struct Inputs {  // device pointers (ghosted Fortran-order fields)
     const double* vel;
@@ -1001,6 +1181,7 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
     // the arena zeroes new blocks with cudaMemset on the legacy stream; the
     // solver's stream does not synchronise with it, so wait here
     if (cudaDeviceSynchronize() != cudaSuccess) return MPS_ERR_CUDA;
+    ctx.tma_ok = tma_prepare();
     ctx.sig = sig;
     return 0;
 }
@@ -1384,7 +1565,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         };
         if ((st = residual())) return st;
         for (;;) {
-            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+            if ((st = fetch_norms(ctx))) return st;
             if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
             norms(ctx.hpin[0], ctx.hpin[1]);
             if (it == 0) inf.rel_res0 = rel;
@@ -1394,7 +1575,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 GraphEntry* G = nullptr;
                 for (;;) {  // each replay ends with the residual norms of the new iterate
                     if ((st = run_graph(ctx, gk, &G, iteration))) return st;
-                    if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+                    if ((st = fetch_norms(ctx))) return st;
                     prof_collect_graph(ctx, *G);
                     vcycles++;
                     it++;
@@ -1437,7 +1618,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         };
         if ((st = residual())) return st;
         for (;;) {
-            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+            if ((st = fetch_norms(ctx))) return st;
             if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
             norms(ctx.hpin[0], ctx.hpin[1]);
             if (it == 0) inf.rel_res0 = rel;
@@ -1447,7 +1628,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 GraphEntry* G = nullptr;
                 for (;;) {  // each replay ends with the residual norms of the new iterate
                     if ((st = run_graph(ctx, gk, &G, iteration))) return st;
-                    if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+                    if ((st = fetch_norms(ctx))) return st;
                     prof_collect_graph(ctx, *G);
                     vcycles += inner;
                     it++;
@@ -1478,7 +1659,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 st = resid_norm(ctx, ctx.rop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L),
                                 split<double>(ctx.w, L));
             if (st) return st;
-            if ((st = fetch(ctx, ctx.rb.out, 2))) return st;
+            if ((st = fetch_norms(ctx))) return st;
             if (!(ctx.hpin[0] <= 1e308)) { inf.status = MPS_ERR_NAN; break; }
             norms(ctx.hpin[0], ctx.hpin[1]);
             if (it == 0) { inf.rel_res0 = rel; bnorm = std::sqrt(ctx.hpin[1]); }
@@ -1720,6 +1901,15 @@ int mps_destroy(mps_handle h)
     ctx.ar.clear();
     ctx.kar.clear();
     ctx.inbuf.clear();
+    for (auto& ln : ctx.lanes) {
+        if (ln.s) cudaStreamSynchronize(ln.s);
+        for (int b = 0; b < 2; b++) {
+            if (ln.pin[b]) cudaFreeHost(ln.pin[b]);
+            if (ln.ev[b]) cudaEventDestroy(ln.ev[b]);
+        }
+        if (ln.s) cudaStreamDestroy(ln.s);
+    }
+    ctx.lanes.clear();
     for (cudaEvent_t e : ctx.prof.ev) cudaEventDestroy(e);
     if (ctx.dtab) cudaFree(ctx.dtab);
     if (ctx.dmax) cudaFree(ctx.dmax);
@@ -1835,6 +2025,99 @@ int mps_linsolve_dev(mps_handle h, const mps_grid* g, int timederiv, double dt, 
 }
 
 // host-pointer front end: stage the ghosted inputs on the device
+// ---- copies between pageable host arrays and the device ----
+// A pageable array cannot be read by the DMA engines directly; the driver
+// would stage it through its own small pinned buffers one piece at a time.
+// Here each of several host threads owns a contiguous part of the array, a
+// stream and two pinned chunk buffers: it copies chunk i+1 into one buffer
+// (a plain memcpy, in parallel with the other threads) while the DMA engine
+// moves chunk i from the other.  Pinned (page-locked or device) arrays go
+// straight to cudaMemcpyAsync on the handle's stream.
+constexpr size_t kLaneChunk = 1u << 20;  // doubles per chunk buffer (8 MiB)
+constexpr int kMaxLanes = 8;
+
+static bool is_pageable(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+static int ensure_lanes(Ctx& ctx)
+{
+    if (!ctx.lanes.empty()) return 0;
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int n = std::max(1, std::min<int>(kMaxLanes, hc ? (int)hc / 2 : 4));
+    ctx.lanes.resize(n);
+    for (auto& ln : ctx.lanes) {
+        if (cudaStreamCreateWithFlags(&ln.s, cudaStreamNonBlocking) != cudaSuccess) return MPS_ERR_CUDA;
+        for (int b = 0; b < 2; b++) {
+            if (cudaMallocHost((void**)&ln.pin[b], sizeof(double) * kLaneChunk) != cudaSuccess) return MPS_ERR_NOMEM;
+            if (cudaEventCreateWithFlags(&ln.ev[b], cudaEventDisableTiming) != cudaSuccess) return MPS_ERR_CUDA;
+        }
+    }
+    return 0;
+}
+
+struct HostCopy {
+    double* dev;        // device array
+    double* host;       // pageable host array (const for H2D)
+    size_t n;           // doubles
+};
+
+// all copies of one direction, each array split across the lanes; the
+// handle's stream is ordered after (H2D) or the host waits for (D2H) them
+static int staged_copies(Ctx& ctx, const std::vector<HostCopy>& cps, bool h2d)
+{
+    if (cps.empty()) return 0;
+    if (int st = ensure_lanes(ctx)) return st;
+    const int nl = (int)ctx.lanes.size();
+    if (!h2d) {  // the results must be complete before the lanes read them
+        cudaEvent_t e = ctx.e1;
+        if (cudaEventRecord(e, ctx.s) != cudaSuccess) return MPS_ERR_CUDA;
+        for (auto& ln : ctx.lanes)
+            if (cudaStreamWaitEvent(ln.s, e, 0) != cudaSuccess) return MPS_ERR_CUDA;
+    }
+    std::vector<int> status(nl, 0);
+    auto work = [&](int li) {
+        Ctx::Lane& ln = ctx.lanes[li];
+        int b = 0;
+        bool used[2] = {false, false};
+        for (const HostCopy& cp : cps) {
+            const size_t part = (cp.n + nl - 1) / nl;
+            const size_t lo = std::min(cp.n, part * li), hi = std::min(cp.n, lo + part);
+            for (size_t o = lo; o < hi; o += kLaneChunk) {
+                const size_t m = std::min(kLaneChunk, hi - o);
+                if (used[b] && cudaEventSynchronize(ln.ev[b]) != cudaSuccess) { status[li] = MPS_ERR_CUDA; return; }
+                if (h2d) {
+                    std::memcpy(ln.pin[b], cp.host + o, sizeof(double) * m);
+                    if (cudaMemcpyAsync(cp.dev + o, ln.pin[b], sizeof(double) * m, cudaMemcpyHostToDevice, ln.s) !=
+                        cudaSuccess) { status[li] = MPS_ERR_CUDA; return; }
+                    if (cudaEventRecord(ln.ev[b], ln.s) != cudaSuccess) { status[li] = MPS_ERR_CUDA; return; }
+                } else {
+                    if (cudaMemcpyAsync(ln.pin[b], cp.dev + o, sizeof(double) * m, cudaMemcpyDeviceToHost, ln.s) !=
+                            cudaSuccess ||
+                        cudaStreamSynchronize(ln.s) != cudaSuccess) { status[li] = MPS_ERR_CUDA; return; }
+                    std::memcpy(cp.host + o, ln.pin[b], sizeof(double) * m);
+                }
+                used[b] = true;
+                b ^= 1;
+            }
+        }
+        if (cudaStreamSynchronize(ln.s) != cudaSuccess) status[li] = MPS_ERR_CUDA;
+    };
+    std::vector<std::thread> th;
+    for (int li = 1; li < nl; li++) th.emplace_back(work, li);
+    work(0);
+    for (auto& t : th) t.join();
+    for (int st : status)
+        if (st) return st;
+    return 0;
+}
+
 static int run_host(mps_handle h, const mps_grid* g, int timederiv, double dt, const double* vel,
                     const double* dcoeff, const double* reac, const double* source, const int bc_code[6],
                     const double* const bcval[6], const double* mgridsterm, double* soln,
@@ -1867,29 +2150,44 @@ static int run_host(mps_handle h, const mps_grid* g, int timederiv, double dt, c
     double* d_bc = d_st + ni;
     const double* dbv[6];
     cudaStream_t s = ctx.s;
-#define H2D(dst, src, n) \
-    if (cudaMemcpyAsync(dst, src, sizeof(double) * (n), cudaMemcpyHostToDevice, s) != cudaSuccess) return MPS_ERR_CUDA
-    if (vel) { H2D(d_vel, vel, 3 * ng); }
-    H2D(d_dc, dcoeff, ng);
-    if (reac) { H2D(d_re, reac, ng); }
-    H2D(d_src, source, ng);
-    H2D(d_sol, soln, ng);
-    if (mgridsterm) { H2D(d_st, mgridsterm, ni); }
+    // pinned (or device) arrays: one cudaMemcpyAsync each on the handle's
+    // stream; pageable arrays: the staged, multi-threaded copies above
+    std::vector<HostCopy> staged;
+    auto h2d = [&](double* dst, const double* src, size_t n) -> int {
+        if (is_pageable(src)) {
+            staged.push_back({dst, const_cast<double*>(src), n});
+            return 0;
+        }
+        return cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, s) == cudaSuccess ? 0
+                                                                                                       : MPS_ERR_CUDA;
+    };
+    int st = 0;
+    if (vel && (st = h2d(d_vel, vel, 3 * ng))) return st;
+    if ((st = h2d(d_dc, dcoeff, ng))) return st;
+    if (reac && (st = h2d(d_re, reac, ng))) return st;
+    if ((st = h2d(d_src, source, ng))) return st;
+    if ((st = h2d(d_sol, soln, ng))) return st;
+    if (mgridsterm && (st = h2d(d_st, mgridsterm, ni))) return st;
     double* p = d_bc;
     for (int f = 0; f < 6; f++) {
         dbv[f] = nullptr;
         if (bcval && bcval[f]) {
-            H2D(p, bcval[f], fs[f]);
+            if ((st = h2d(p, bcval[f], fs[f]))) return st;
             dbv[f] = p;
         }
         p += fs[f];
     }
-#undef H2D
-    int st = run_dev(h, g, timederiv, dt, vel ? d_vel : nullptr, d_dc, reac ? d_re : nullptr, d_src, bc_code, dbv,
-                     mgridsterm ? d_st : nullptr, d_sol, opts, info, nullptr, ref_norm_only);
+    if ((st = staged_copies(ctx, staged, true))) return st;  // complete when it returns
+    st = run_dev(h, g, timederiv, dt, vel ? d_vel : nullptr, d_dc, reac ? d_re : nullptr, d_src, bc_code, dbv,
+                 mgridsterm ? d_st : nullptr, d_sol, opts, info, nullptr, ref_norm_only);
     if (st) return st;
-    if (cudaMemcpyAsync(soln, d_sol, sizeof(double) * ng, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPS_ERR_CUDA;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_ERR_CUDA;
+    if (is_pageable(soln)) {
+        if ((st = staged_copies(ctx, {HostCopy{d_sol, soln, ng}}, false))) return st;
+    } else {
+        if (cudaMemcpyAsync(soln, d_sol, sizeof(double) * ng, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return MPS_ERR_CUDA;
+        if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_ERR_CUDA;
+    }
     return info ? info->status : MPS_OK;
 }
 
