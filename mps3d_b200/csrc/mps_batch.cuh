@@ -68,6 +68,8 @@ struct DProlong {
     T* u1;
     const T* e0;
     const T* e1;
+    int mode;  // 1: the black cells and the red cells of odd periodic seams (the
+               // first post-smoothing pass rewrites the other red cells); -1: all
 };
 template <class T>
 struct DOuter {
@@ -121,6 +123,66 @@ __device__ __forceinline__ void load_desc(const D* __restrict__ desc, int seg, u
         __VA_ARGS__                                                                                            \
     }
 
+// Shapes of the batched steps, measured on the 64-problem batch (sizes 33 to
+// 129, 5 outer iterations; ms per batch, mixed / FP64):
+//   colour     restriction          prolongation    mixed / FP64
+//   1 cell     1 thread per cell    all cells       80.0 / 97.0
+//   4 (FP32)   8 lanes per cell     black cells     67.9 / 107.0
+//   4 (FP32)   8 lanes per cell     all cells       74.2 / 113.5
+//   4 (both)   8 lanes per cell     black cells     67.7 / 108.6
+//   4 (FP32)   1 thread per cell    black cells     59.9 / 90.6   <- kept
+// (colour: cells of a row per thread on levels with a vector row evaluation;
+// black cells: the first post-smoothing pass rewrites the red ones)
+#ifndef MPS_BATCH_VEC64
+#define MPS_BATCH_VEC64 0
+#endif
+#ifndef MPS_BATCH_R8
+#define MPS_BATCH_R8 0
+#endif
+#ifndef MPS_BATCH_PB
+#define MPS_BATCH_PB 1
+#endif
+constexpr int BATCH_W = 4;
+template <class T>
+__host__ __device__ __forceinline__ bool batch_vector_level(const Lev& L)
+{
+    return (sizeof(T) == 4 || MPS_BATCH_VEC64) && (L.uniform || L.nx >= 16);
+}
+
+// one group of BATCH_W cells of colour c (thread index t over (P/W) x rows)
+template <class T, class U>
+__device__ __forceinline__ void colour_group_body(const Lev& L, const KOp<T>& op, int c, const U& u,
+                                                  T* __restrict__ out, const T* __restrict__ f, unsigned t)
+{
+    constexpr int W = BATCH_W;
+    const unsigned ng = (unsigned)L.P / W;
+    const unsigned row = L.divG.div(t);
+    if (row >= L.rows) return;
+    const int k = (int)L.divNy.div(row);
+    const int j = (int)row - k * L.ny;
+    const int h0 = W * (int)(t - row * ng);
+    const int q = (j + k + c) & 1;
+    const int o0 = h0 + L.P * (int)row;
+    const VecW<T, W> f4 = ldv<T, W>(f + o0);
+    VecW<T, W> diag, off;
+    if (L.uniform) group_rows<T, W, U, true>(L, op, c, u, (int)row, j, k, h0, q, o0, diag, off);
+    else group_rows<T, W, U, false>(L, op, c, u, (int)row, j, k, h0, q, o0, diag, off);
+    VecW<T, W> res;
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int i = 2 * (h0 + e) + q;
+        res.v[e] = i < L.nx ? gs_value(f4.v[e], diag.v[e], off.v[e]) : T(0);
+    }
+    stv<T, W>(out + o0, res);
+}
+
+template <class T, class U>
+__device__ __forceinline__ void batch_colour(const DColour<T>& d, int c, const U& u, unsigned t)
+{
+    if (batch_vector_level<T>(d.L)) colour_group_body<T, U>(d.L, d.op, c, u, d.out, d.f, t);
+    else colour_body<T, KOp<T>, U>(d.L, d.op, c, u, d.out, d.f, t);
+}
+
 template <class T>
 __global__ void __launch_bounds__(TPB) kb_colour(const DColour<T>* __restrict__ desc, const int* __restrict__ task0,
                                                  const int* __restrict__ pid, int nseg, int total,
@@ -128,17 +190,17 @@ __global__ void __launch_bounds__(TPB) kb_colour(const DColour<T>* __restrict__ 
 {
     BATCH_LOOP(DColour<T>, desc, task0, pid, nseg, total, active, {
         if (zs == 2) {
-            colour_body<T, KOp<T>, ZeroU<T>>(d.L, d.op, c, ZeroU<T>(), d.out, d.f, t);
+            batch_colour<T, ZeroU<T>>(d, c, ZeroU<T>(), t);
         } else if (zs == 1) {
             OtherOnlyU<T> u;
             u.c = c;
             u.other = c == 0 ? d.u1 : d.u0;
-            colour_body<T, KOp<T>, OtherOnlyU<T>>(d.L, d.op, c, u, d.out, d.f, t);
+            batch_colour<T, OtherOnlyU<T>>(d, c, u, t);
         } else {
             CSplit<T> u;
             u.c[0] = d.u0;
             u.c[1] = d.u1;
-            colour_body<T, KOp<T>, CSplit<T>>(d.L, d.op, c, u, d.out, d.f, t);
+            batch_colour<T, CSplit<T>>(d, c, u, t);
         }
     })
 }
@@ -148,16 +210,42 @@ __global__ void __launch_bounds__(TPB) kb_restrict(const DRestrict<T>* __restric
                                                    const int* __restrict__ task0, const int* __restrict__ pid,
                                                    int nseg, int total, const BState* active)
 {
+    // eight lanes per coarse cell, each a share of the children, summed by
+    // shuffles (every thread of the block reaches the shuffles)
     BATCH_LOOP(DRestrict<T>, desc, task0, pid, nseg, total, active, {
         CSplit<T> u, f;
         u.c[0] = d.u0;
         u.c[1] = d.u1;
         f.c[0] = d.f;
         f.c[1] = d.f + d.F.half;
-        Split<T> fc;
-        fc.c[0] = d.fc;
-        fc.c[1] = d.fc + d.C.half;
-        resid_restrict_body<T, KOp<T>>(d.F, d.op, u, f, d.C, fc, d.geom, t);
+        if (!MPS_BATCH_R8) {  // one thread per coarse cell over all its children
+            Split<T> fc;
+            fc.c[0] = d.fc;
+            fc.c[1] = d.fc + d.C.half;
+            resid_restrict_body<T, KOp<T>>(d.F, d.op, u, f, d.C, fc, d.geom, t);
+            continue;
+        }
+        const unsigned ncx = d.C.nx, ncy = d.C.ny, nc = ncx * ncy * (unsigned)d.C.nz;
+        const unsigned cell = t >> 3;
+        const int part = (int)(t & 7u);
+        T sm = T(0), vol = T(0);
+        unsigned I = 0, J = 0, K = 0;
+        if (cell < nc) {
+            K = cell / (ncx * ncy);
+            const unsigned rem = cell - K * ncx * ncy;
+            J = rem / ncx;
+            I = rem - J * ncx;
+            resid_restrict_part<T, KOp<T>>(d.F, d.op, u, f, d.C, d.geom, (int)I, (int)J, (int)K, part, 8, sm, vol);
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            sm += __shfl_xor_sync(0xffffffffu, sm, o, 8);
+            vol += __shfl_xor_sync(0xffffffffu, vol, o, 8);
+        }
+        if (cell < nc && part == 0) {
+            T* dst = scol((int)I, (int)J, (int)K) ? d.fc + d.C.half : d.fc;
+            dst[soff(d.C, (int)I, (int)J, (int)K)] = d.geom ? sm / vol : sm * (T(1) / vol);
+        }
     })
 }
 
@@ -191,7 +279,13 @@ __global__ void __launch_bounds__(TPB) kb_prolong(const DProlong<T>* __restrict_
         CSplit<T> e;
         e.c[0] = d.e0;
         e.c[1] = d.e1;
-        prolong_body<T>(d.F, u, d.C, e, d.X, -1, t);
+        if (d.mode < 0) {
+            prolong_body<T>(d.F, u, d.C, e, d.X, -1, t);
+        } else {
+            prolong_body<T>(d.F, u, d.C, e, d.X, 1, t);
+            if ((d.F.per[0] && (d.F.nx & 1)) || (d.F.per[1] && (d.F.ny & 1)) || (d.F.per[2] && (d.F.nz & 1)))
+                prolong_body<T>(d.F, u, d.C, e, d.X, 2, t);
+        }
     })
 }
 
@@ -482,7 +576,10 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                 else bi[p][d] ^= 1;
                 return x;
             },
-            [&](int p) { return nb(B.sub[p]->lev[d].half); });
+            [&](int p) {
+                const Lev& L = B.sub[p]->lev[d];
+                return batch_vector_level<T>(L) ? nb(L.half / BATCH_W) : nb(L.half);
+            });
     };
     auto vcycle = [&](std::vector<BStep>& list, bool zero) {
         for (int d = 0; d < D; d++) {
@@ -509,7 +606,7 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                 },
                 [&](int p) {
                     const Lev& C = B.sub[p]->lev[d + 1];
-                    return nb((long long)C.nx * C.ny * C.nz);
+                    return nb((MPS_BATCH_R8 ? 8LL : 1LL) * C.nx * C.ny * C.nz);
                 });
         }
         step(
@@ -540,11 +637,12 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                     x.u1 = cur1(p, d);
                     x.e0 = cur0(p, d + 1);
                     x.e1 = cur1(p, d + 1);
+                    x.mode = (MPS_BATCH_PB && o->nu2 >= 1) ? 1 : -1;
                     return x;
                 },
                 [&](int p) {
                     const Lev& F = B.sub[p]->lev[d];
-                    return nb((long long)F.nx * F.ny * F.nz);
+                    return (MPS_BATCH_PB && o->nu2 >= 1) ? nb(F.half) : nb((long long)F.nx * F.ny * F.nz);
                 });
             for (int s = 0; s < o->nu2; s++) {
                 colour(list, d, 0, 0);
