@@ -345,7 +345,7 @@ def timed_solves(dp, xg, h, steps, ws, init=None, **kw):
     return dist_max(e0.elapsed_time(e1), ws) / steps, info
 
 
-def bench_poisson65(args, ws, rank, h, dev):
+def bench_poisson65(args, ws, rank, h, dev, deferred):
     """Plain FP64 Poisson, 65^3 cells on the unit cube, coefficient 1, Dirichlet
     0, U[-1,1] right-hand side, to 1e-10 relative residual: GPU solves/s (mixed
     and FP64) and, on rank 0 with one GPU, the oracle's restatement of the
@@ -361,26 +361,33 @@ def bench_poisson65(args, ws, rank, h, dev):
     out = {"workload": "Poisson 65^3, unit cube, coefficient 1, Dirichlet 0, U[-1,1] source, 1e-10 rel. residual",
            "unit": "solves/s"}
     check = rank == 0 and ws == 1 and not args.skip_oracle
-    ref = oracle_reference(p) if check else None
+    sols = {}
     for prec in ("mixed", "fp64"):
         ms, info = timed_solves(dp, x, h, args.steps, ws, precision=prec, tol=1e-10, maxit=60)
         out[prec] = {"value": ws * 1e3 / ms, "ms_per_solve": ms, "iters": info["iters"], "rel_res": info["rel_res"]}
-        if check:
-            out[prec].update(vs_oracle(p, x.cpu().numpy(), ref))
-    if rank == 0 and ws == 1 and not args.skip_cpu:
-        from oracle import oracle as orc
+        sols[prec] = x.cpu().numpy()
 
-        q = W.poisson_dirichlet(64)
-        t0 = time.perf_counter()
-        _, rel, _ = orc.solve(q, maxit=40, tol=1e-10, tol_kind=1)
-        t = time.perf_counter() - t0
-        out["cpu_oracle_64"] = {"s_per_solve": t, "vcycles": int(len(rel)), "final_rel_res": float(rel[-1]),
-                                "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
-                                "kind": "port (restatement of perform_vcycle, CELL hierarchy, 64^3 twin)"}
+    def later():  # host-core work, after every GPU timing of the run
+        if check:
+            ref = oracle_reference(p)
+            for prec in ("mixed", "fp64"):
+                out[prec].update(vs_oracle(p, sols[prec], ref))
+        if rank == 0 and ws == 1 and not args.skip_cpu:
+            from oracle import oracle as orc
+
+            q = W.poisson_dirichlet(64)
+            t0 = time.perf_counter()
+            _, rel, _ = orc.solve(q, maxit=40, tol=1e-10, tol_kind=1)
+            t = time.perf_counter() - t0
+            out["cpu_oracle_64"] = {"s_per_solve": t, "vcycles": int(len(rel)), "final_rel_res": float(rel[-1]),
+                                    "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                                    "kind": "port (restatement of perform_vcycle, CELL hierarchy, 64^3 twin)"}
+
+    deferred.append(later)
     return out
 
 
-def bench_sg_step(args, ws, h, phi_fine, dev, check=False):
+def bench_sg_step(args, ws, h, phi_fine, dev, deferred, check=False):
     """Implicit SG electron step, 129^3: the potential is the 257^3 plasma
     Poisson solution injected onto 129^3; FGMRES(30) preconditioned by an FP32
     (mixed) or FP64 V-cycle, to 1e-10 relative residual."""
@@ -394,18 +401,25 @@ def bench_sg_step(args, ws, h, phi_fine, dev, check=False):
     out = {"workload": "implicit electron drift-diffusion step 129^3, Scharfetter-Gummel faces, dt 1e-11 s, "
                        "periodic x/y, ZGRD z; potential = 257^3 plasma Poisson solution injected",
            "unit": "solves/s", "tol_rel_residual": 1e-10}
-    ref = oracle_reference(p3, krylov=True) if check else None
+    sols = {}
     for prec in ("mixed", "fp64"):
         ms, info = timed_solves(dp3, x3, h, args.steps, ws, precision=prec, krylov="fgmres", restart=30,
                                 tol=1e-10, maxit=60)
         out[prec] = {"value": ws * 1e3 / ms, "ms_per_solve": ms, "iters": info["iters"],
                      "rel_res": info["rel_res"]}
+        sols[prec] = x3.cpu().numpy()
+
+    def later():
         if check:
-            out[prec].update(vs_oracle(p3, x3.cpu().numpy(), ref))
+            ref = oracle_reference(p3, krylov=True)
+            for prec in ("mixed", "fp64"):
+                out[prec].update(vs_oracle(p3, sols[prec], ref))
+
+    deferred.append(later)
     return out
 
 
-def bench_batch(args, ws, rank, h, dev):
+def bench_batch(args, ws, rank, h, dev, deferred):
     """64 independent constant-coefficient Poisson solves, cubic sizes drawn
     from {33,49,65,97,129}, Dirichlet 0, U[-1,1] right-hand sides, to 1e-10
     relative residual: one batched mixed-precision call (every V-cycle step
@@ -446,8 +460,8 @@ def bench_batch(args, ws, rank, h, dev):
     out = {"workload": "64 Poisson problems, unit cube, cubic sizes from {33,49,65,97,129} (seeded), Dirichlet 0, "
                        "U[-1,1] right-hand sides, 1e-10 relative residual",
            "cells": cells, "unit": "solves/s"}
-    # the oracle's converged FP64 solution of every problem (N=1 only)
-    refs = [oracle_reference(pp) for pp in ps] if (ws == 1 and not args.skip_oracle) else None
+    check = ws == 1 and not args.skip_oracle
+    sols = {}
     for name, fn, prec in (("batched_mixed", batched, "mixed"), ("batched_fp64", batched, "fp64"),
                            ("sequential_fp64", sequential, "fp64"), ("sequential_mixed", sequential, "mixed")):
         for _ in range(3):
@@ -469,20 +483,29 @@ def bench_batch(args, ws, rank, h, dev):
             out[name] = {"value": 64 * 1e3 / ms, "ms_per_batch": ms,
                          "max_rel_res": max(i["rel_res"] for i in every),
                          "iters": sorted({i["iters"] for i in every})}
-        if refs is not None:
-            checks = [vs_oracle(pp, xx.cpu().numpy(), rr) for pp, xx, rr in zip(ps, xs, refs)]
-            out[name]["max_rel_res_by_oracle"] = max(c["rel_res_by_oracle"] for c in checks)
-            out[name]["max_rel_err_vs_oracle"] = max(c["rel_err_vs_oracle"] for c in checks)
+        if check:
+            sols[name] = [xx.cpu().numpy() for xx in xs]
     if rank == 0:
         out["batched_mixed_over_sequential_fp64"] = out["batched_mixed"]["value"] / out["sequential_fp64"]["value"]
         out["ranks"] = ws
         out["scaling"] = "strong (64 problems split across the ranks by cell count)"
     for hh in handles.values():
         hh.close()
+
+    def later():  # the oracle's converged FP64 solution of every problem (N=1 only)
+        if not check:
+            return
+        refs = [oracle_reference(pp) for pp in ps]
+        for name, xl in sols.items():
+            checks = [vs_oracle(pp, xx, rr) for pp, xx, rr in zip(ps, xl, refs)]
+            out[name]["max_rel_res_by_oracle"] = max(c["rel_res_by_oracle"] for c in checks)
+            out[name]["max_rel_err_vs_oracle"] = max(c["rel_err_vs_oracle"] for c in checks)
+
+    deferred.append(later)
     return out
 
 
-def bench_adjoint(args, ws, h, dev):
+def bench_adjoint(args, ws, h, dev, deferred):
     """Electron-flux adjoint at 129^3: loss = electron flux through z = L
     after 5 implicit SG steps; gradients w.r.t. the electrode voltage and the
     FP32 mobility field (torch.autograd over the C ABI: transposed SG solves,
@@ -519,27 +542,34 @@ def bench_adjoint(args, ws, h, dev):
     d = torch.from_numpy(np.random.default_rng(5005).uniform(-1.0, 1.0, size=mu.shape)).to(mu.device) * mu64 * 1e-4
     fd_mu = (f(V, mu64 + d) - f(V, mu64 - d)) / 2.0
     an_mu = float((gmu_t.double() * d).sum())
-    oracle = None
-    if ws == 1 and not args.skip_oracle:
-        # the same model over the FP64 oracle's solves and VJP on the host cores
-        sys.path.insert(0, os.path.join(ROOT, "tests"))
-        from adjoint_oracle import oracle_bvec, oracle_solve
+    g64 = gmu_t.cpu()
+    mu_cpu = mu.double().cpu()
+    res = {}
 
-        ref = ElectronFluxAdjoint(case, device="cpu", solve_fn=oracle_solve, bvec_fn=oracle_bvec)
-        L_r, gV_r, gmu_r = ref.gradient(V, mu.double().cpu())
-        g64 = gmu_t.cpu()
-        oracle = {"rel_err_loss": abs(L0 - L_r) / abs(L_r), "rel_err_dL_dV": abs(gV_t - gV_r) / abs(gV_r),
-                  "rel_err_dL_dmu": float((g64 - gmu_r).norm() / gmu_r.norm()),
-                  "note": "FP64 mobility on both sides; tolerance 1e-12 (GPU) / 1e-14 (oracle)"}
-    return {"workload": "electron flux through z=L after 5 implicit SG steps, 129^3 (plasma Poisson potential with "
+    def later():
+        if ws == 1 and not args.skip_oracle:
+            # the same model over the FP64 oracle's solves and VJP on the host cores
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            from adjoint_oracle import oracle_bvec, oracle_solve
+
+            ref = ElectronFluxAdjoint(case, device="cpu", solve_fn=oracle_solve, bvec_fn=oracle_bvec)
+            L_r, gV_r, gmu_r = ref.gradient(V, mu_cpu)
+            res["vs_fp64_oracle_gradient"] = {
+                "rel_err_loss": abs(L0 - L_r) / abs(L_r), "rel_err_dL_dV": abs(gV_t - gV_r) / abs(gV_r),
+                "rel_err_dL_dmu": float((g64 - gmu_r).norm() / gmu_r.norm()),
+                "note": "FP64 mobility on both sides; tolerance 1e-12 (GPU) / 1e-14 (oracle)"}
+
+    deferred.append(later)
+    res.update({"workload": "electron flux through z=L after 5 implicit SG steps, 129^3 (plasma Poisson potential with "
                         "electrode voltage V; mobility mu FP32 field); gradients w.r.t. V and mu",
             "unit": "gradients/s", "value": ws * 1e3 / ms, "ms_per_gradient": ms, "loss": L0,
             "dL_dV": gV, "fd_dL_dV": fd_V, "rel_err_V": abs(fd_V - gV_t) / abs(gV_t),
-            "rel_err_mu_directional": abs(fd_mu - an_mu) / abs(an_mu), "vs_fp64_oracle_gradient": oracle,
-            "fd_step": "1e-4 relative (V; every mobility cell along a random direction)"}
+            "rel_err_mu_directional": abs(fd_mu - an_mu) / abs(an_mu),
+            "fd_step": "1e-4 relative (V; every mobility cell along a random direction)"})
+    return res
 
 
-def bench_plasma_step(args, ws, dev, check=False):
+def bench_plasma_step(args, ws, dev, deferred, check=False):
     """The potential + electron part of one implicit step at 129^3 on the
     device (mps_plasma_step_dev: space-charge source, potential solve, E
     field, electron operator, SG electron solve, floor, ghosts), against what
@@ -589,14 +619,19 @@ def bench_plasma_step(args, ws, dev, check=False):
            "unit": "steps/s", "value": ws * 1e3 / ms, "ms_per_step": ms, "phi_iters": ip["iters"],
            "electron_iters": ie["iters"], "h2d_ms_avoided": h2d_ms,
            "h2d_bytes_avoided": int(host.numel() * 8)}
-    if check:
-        from oracle import step_oracle as SO
-
-        phi_o, _, _, _, _, ne_o = SO.plasma_step(case, case["n_e0"])
-        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
-        out["rel_err_phi_vs_oracle"] = rel(phi.cpu().numpy(), phi_o)
-        out["rel_err_ne_vs_oracle"] = rel(ne.cpu().numpy(), ne_o)
+    phi_h, ne_h = phi.cpu().numpy(), ne.cpu().numpy()
     stp.close()
+
+    def later():
+        if check:
+            from oracle import step_oracle as SO
+
+            phi_o, _, _, _, _, ne_o = SO.plasma_step(case, case["n_e0"])
+            rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+            out["rel_err_phi_vs_oracle"] = rel(phi_h, phi_o)
+            out["rel_err_ne_vs_oracle"] = rel(ne_h, ne_o)
+
+    deferred.append(later)
     return out
 
 
@@ -750,6 +785,20 @@ def run_ours(args, ws, rank, local):
             e2e["pageable"] = {"value": ws * args.steps / t_pg, "unit": UNIT, "ms_per_step": t_pg / args.steps * 1e3,
                                "buffers": "pageable host memory (numpy arrays, as a Fortran caller passes)"}
 
+    # ---- secondary configurations (figures beside the headline line); every
+    # host-core computation (oracle checks, CPU baselines) is deferred until
+    # all GPU timings of the run are done, so that no OpenMP thread of the
+    # oracle competes with the thread that drives the GPU ----
+    others = {}
+    deferred = []
+    if not args.skip_others and n == 257:
+        check = rank == 0 and ws == 1 and not args.skip_oracle
+        others["poisson_65"] = bench_poisson65(args, ws, rank, h, dev, deferred)
+        others["sg_step_129"] = bench_sg_step(args, ws, h, x, dev, deferred, check=check)
+        others["batch64"] = bench_batch(args, ws, rank, h, dev, deferred)
+        others["adjoint_129"] = bench_adjoint(args, ws, h, dev, deferred)
+        others["plasma_step_129"] = bench_plasma_step(args, ws, dev, deferred, check=check)
+
     # ---- CPU baseline: the oracle port on the host cores (rank 0, N=1) ----
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
@@ -762,16 +811,8 @@ def run_ours(args, ws, rank, local):
         parity = {prec: vs_oracle(p, sol[prec], ref) for prec in ("mixed", "fp64")}
         parity["oracle_final_rel_res"] = ref[3]
         del ref
-
-    # ---- secondary configurations (figures beside the headline line) ----
-    others = {}
-    if not args.skip_others and n == 257:
-        others["poisson_65"] = bench_poisson65(args, ws, rank, h, dev)
-        others["sg_step_129"] = bench_sg_step(args, ws, h, x, dev,
-                                              check=rank == 0 and ws == 1 and not args.skip_oracle)
-        others["batch64"] = bench_batch(args, ws, rank, h, dev)
-        others["adjoint_129"] = bench_adjoint(args, ws, h, dev)
-        others["plasma_step_129"] = bench_plasma_step(args, ws, dev, check=rank == 0 and ws == 1 and not args.skip_oracle)
+    for fn in deferred:
+        fn()
 
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "colour_pass_traffic.json")

@@ -19,9 +19,10 @@
 // iterations, and the check kernel also counts the body's executions and
 // stops at maxit + 2, so the loop always ends.
 //
-// The launch shape (blocks of the grid-stride loop, per level depth) is
-// picked by timing candidate grids on the batch's own finest-to-coarsest
-// colour passes at the first call with a given batch structure.
+// The launch shape (blocks of the grid-stride loop, and the colour pass's
+// cells per thread, per level depth) is picked by timing every candidate
+// pair on the batch's own colour passes at the first call with a given batch
+// structure.
 
 namespace mps {
 
@@ -130,12 +131,11 @@ __device__ __forceinline__ void load_desc(const D* __restrict__ desc, int seg, u
 //   4 (FP32)   8 lanes per cell     black cells     67.9 / 107.0
 //   4 (FP32)   8 lanes per cell     all cells       74.2 / 113.5
 //   4 (both)   8 lanes per cell     black cells     67.7 / 108.6
-//   4 (FP32)   1 thread per cell    black cells     59.9 / 90.6   <- kept
+//   4 (FP32)   1 thread per cell    black cells     59.9 / 90.6
 // (colour: cells of a row per thread on levels with a vector row evaluation;
-// black cells: the first post-smoothing pass rewrites the red ones)
-#ifndef MPS_BATCH_VEC64
-#define MPS_BATCH_VEC64 0
-#endif
+// black cells: the first post-smoothing pass rewrites the red ones).  Kept:
+// one thread per coarse cell, black cells, and the colour-pass body picked
+// per depth by the autotuner together with the grid (below).
 #ifndef MPS_BATCH_R8
 #define MPS_BATCH_R8 0
 #endif
@@ -143,11 +143,7 @@ __device__ __forceinline__ void load_desc(const D* __restrict__ desc, int seg, u
 #define MPS_BATCH_PB 1
 #endif
 constexpr int BATCH_W = 4;
-template <class T>
-__host__ __device__ __forceinline__ bool batch_vector_level(const Lev& L)
-{
-    return (sizeof(T) == 4 || MPS_BATCH_VEC64) && (L.uniform || L.nx >= 16);
-}
+__host__ __device__ __forceinline__ bool batch_vector_level(const Lev& L) { return L.uniform || L.nx >= 16; }
 
 // one group of BATCH_W cells of colour c (thread index t over (P/W) x rows)
 template <class T, class U>
@@ -177,30 +173,32 @@ __device__ __forceinline__ void colour_group_body(const Lev& L, const KOp<T>& op
 }
 
 template <class T, class U>
-__device__ __forceinline__ void batch_colour(const DColour<T>& d, int c, const U& u, unsigned t)
+__device__ __forceinline__ void batch_colour(const DColour<T>& d, int c, const U& u, unsigned t, int vec)
 {
-    if (batch_vector_level<T>(d.L)) colour_group_body<T, U>(d.L, d.op, c, u, d.out, d.f, t);
+    if (vec && batch_vector_level(d.L)) colour_group_body<T, U>(d.L, d.op, c, u, d.out, d.f, t);
     else colour_body<T, KOp<T>, U>(d.L, d.op, c, u, d.out, d.f, t);
 }
 
+// vec: the vector body on the levels that have one (the task layout of the
+// step must be the matching one)
 template <class T>
 __global__ void __launch_bounds__(TPB) kb_colour(const DColour<T>* __restrict__ desc, const int* __restrict__ task0,
                                                  const int* __restrict__ pid, int nseg, int total,
-                                                 const BState* active, int c, int zs)
+                                                 const BState* active, int c, int zs, int vec)
 {
     BATCH_LOOP(DColour<T>, desc, task0, pid, nseg, total, active, {
         if (zs == 2) {
-            batch_colour<T, ZeroU<T>>(d, c, ZeroU<T>(), t);
+            batch_colour<T, ZeroU<T>>(d, c, ZeroU<T>(), t, vec);
         } else if (zs == 1) {
             OtherOnlyU<T> u;
             u.c = c;
             u.other = c == 0 ? d.u1 : d.u0;
-            batch_colour<T, OtherOnlyU<T>>(d, c, u, t);
+            batch_colour<T, OtherOnlyU<T>>(d, c, u, t, vec);
         } else {
             CSplit<T> u;
             u.c[0] = d.u0;
             u.c[1] = d.u1;
-            batch_colour<T, CSplit<T>>(d, c, u, t);
+            batch_colour<T, CSplit<T>>(d, c, u, t, vec);
         }
     })
 }
@@ -401,6 +399,10 @@ struct BStep {
     size_t desc_off = 0;  // bytes into the descriptor buffer
     size_t task_off = 0;  // ints into the task buffer: task0[nseg+1], then pid[nseg]
     int nseg = 0, total = 0, grid = 0;
+    // colour steps: the task layout of the vector body (BATCH_W cells per
+    // thread on the levels that have one) and which of the two runs
+    size_t task_off_v = 0;
+    int total_v = 0, vec = 0;
 };
 
 struct BatchState {
@@ -422,9 +424,11 @@ struct BatchState {
     cudaGraphExec_t exec = nullptr;
     std::vector<long long> graph_key;
     int body_kernels = 0;
-    // autotuned grid per (precision, depth), keyed by the batch structure
+    // autotuned grid and colour-pass body per (precision, depth), keyed by
+    // the batch structure
     std::vector<long long> tune_key;
     std::vector<int> tune_grid;
+    std::vector<int> tune_vec;
 };
 
 static int sub_init(Ctx& parent, Ctx& sc)
@@ -576,10 +580,24 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                 else bi[p][d] ^= 1;
                 return x;
             },
-            [&](int p) {
-                const Lev& L = B.sub[p]->lev[d];
-                return batch_vector_level<T>(L) ? nb(L.half / BATCH_W) : nb(L.half);
-            });
+            [&](int p) { return nb(B.sub[p]->lev[d].half); });
+        if (list.empty() || list.back().kind != B_COLOUR || list.back().depth != d) return;
+        // the task layout of the vector body over the same problems
+        BStep& s = list.back();
+        const int* pid = P.task.data() + s.task_off + s.nseg + 1;
+        std::vector<int> t0v;
+        int tot = 0;
+        for (int q = 0; q < s.nseg; q++) {
+            t0v.push_back(tot);
+            const Lev& L = B.sub[pid[q]]->lev[d];
+            tot += batch_vector_level(L) ? nb(L.half / BATCH_W) : nb(L.half);
+        }
+        t0v.push_back(tot);
+        std::vector<int> pids(pid, pid + s.nseg);
+        s.task_off_v = P.task.size();
+        s.total_v = tot;
+        P.task.insert(P.task.end(), t0v.begin(), t0v.end());
+        P.task.insert(P.task.end(), pids.begin(), pids.end());
     };
     auto vcycle = [&](std::vector<BStep>& list, bool zero) {
         for (int d = 0; d < D; d++) {
@@ -692,7 +710,14 @@ static void launch_step(cudaStream_t s, const BStep& st, const unsigned char* dd
     const void* dp = ddesc + st.desc_off;
     switch (st.kind) {
     case B_COLOUR:
-        kb_colour<T><<<g, TPB, 0, s>>>((const DColour<T>*)dp, t0, pid, st.nseg, st.total, active, st.c, st.zs);
+        if (st.vec) {
+            const int* tv = dtask + st.task_off_v;
+            const unsigned gv = (unsigned)std::max(1, std::min(st.grid, st.total_v));
+            kb_colour<T><<<gv, TPB, 0, s>>>((const DColour<T>*)dp, tv, tv + st.nseg + 1, st.nseg, st.total_v, active,
+                                            st.c, st.zs, 1);
+        } else {
+            kb_colour<T><<<g, TPB, 0, s>>>((const DColour<T>*)dp, t0, pid, st.nseg, st.total, active, st.c, st.zs, 0);
+        }
         break;
     case B_RESTRICT:
         kb_restrict<T><<<g, TPB, 0, s>>>((const DRestrict<T>*)dp, t0, pid, st.nseg, st.total, active);
@@ -746,6 +771,7 @@ static int autotune(Ctx& ctx, BatchState& B, BatchPlan<T>& P, const unsigned cha
 {
     const int D = P.maxdepth;
     B.tune_grid.assign(D + 1, 8 * ctx.nsm);
+    B.tune_vec.assign(D + 1, 0);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
@@ -754,20 +780,31 @@ static int autotune(Ctx& ctx, BatchState& B, BatchPlan<T>& P, const unsigned cha
         for (const BStep& s : P.body)
             if (s.kind == B_COLOUR && s.depth == d && s.zs == 0) { st = &s; break; }
         if (!st) continue;
+        // the grid and the body (one cell or BATCH_W cells per thread) of
+        // this depth's colour passes: every pair timed, the fastest kept
         float best = 1e30f;
-        for (int bps : kTuneBlocksPerSM) {
-            const int g = bps * ctx.nsm;
-            if (g > std::max(st->total, ctx.nsm)) break;
-            BStep s2 = *st;
-            s2.grid = g;
-            launch_step<T>(ctx.s, s2, ddesc, dtask, B.dst, B.dpart);  // warm
-            CK(cudaEventRecord(a, ctx.s));
-            for (int r = 0; r < 3; r++) launch_step<T>(ctx.s, s2, ddesc, dtask, B.dst, B.dpart);
-            CK(cudaEventRecord(b, ctx.s));
-            CK(cudaEventSynchronize(b));
-            float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, a, b));
-            if (ms < best * 0.97f) { best = ms; B.tune_grid[d] = g; }
+        for (int vec = 0; vec < 2; vec++) {
+            const int total = vec ? st->total_v : st->total;
+            if (vec && st->total_v == st->total) continue;  // no level of this depth has the vector body
+            for (int bps : kTuneBlocksPerSM) {
+                const int g = bps * ctx.nsm;
+                if (g > std::max(total, ctx.nsm)) break;
+                BStep s2 = *st;
+                s2.grid = g;
+                s2.vec = vec;
+                launch_step<T>(ctx.s, s2, ddesc, dtask, B.dst, B.dpart);  // warm
+                CK(cudaEventRecord(a, ctx.s));
+                for (int r = 0; r < 3; r++) launch_step<T>(ctx.s, s2, ddesc, dtask, B.dst, B.dpart);
+                CK(cudaEventRecord(b, ctx.s));
+                CK(cudaEventSynchronize(b));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, a, b));
+                if (ms < best * 0.97f) {
+                    best = ms;
+                    B.tune_grid[d] = g;
+                    B.tune_vec[d] = vec;
+                }
+            }
         }
     }
     B.tune_grid[D] = B.tune_grid[0];
@@ -785,8 +822,12 @@ static void assign_grids(BatchState& B, BatchPlan<T>& P)
         if (s.kind == B_OUTER || s.kind == B_AXPY) return B.tune_grid[0];
         return B.tune_grid[std::min(s.depth, (int)B.tune_grid.size() - 1)];
     };
-    for (BStep& s : P.pre) s.grid = grid_of(s);
-    for (BStep& s : P.body) s.grid = grid_of(s);
+    auto vec_of = [&](const BStep& s) {
+        return s.kind == B_COLOUR && !B.tune_vec.empty() ? B.tune_vec[std::min(s.depth, (int)B.tune_vec.size() - 1)]
+                                                         : 0;
+    };
+    for (BStep& s : P.pre) { s.grid = grid_of(s); s.vec = vec_of(s); }
+    for (BStep& s : P.body) { s.grid = grid_of(s); s.vec = vec_of(s); }
 }
 
 template <class T>
@@ -912,7 +953,10 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     long long tb;
     std::memcpy(&tb, &o->tol, 8);
     key.push_back(tb);
-    for (const BStep& s : P.body) key.push_back(s.grid);
+    for (const BStep& s : P.body) {
+        key.push_back(s.grid);
+        key.push_back(s.vec);
+    }
     if (key != B.graph_key) {
         batch_release_graph(B);
         CK(cudaGraphCreate(&B.graph, 0));

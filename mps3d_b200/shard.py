@@ -89,3 +89,17 @@ def gather_results(local: list, indices: Sequence[int], ws: int, rank: int, tota
         for i, r in part:
             out[i] = r
     return out
+
+
+def solve_sharded(problems: Sequence, solve_share, ws: int, rank: int, cost=None):
+    """Independent problems across ranks: each rank solves its cost-balanced
+    share (``solve_share(list of problems) -> list of results``, one per
+    problem, e.g. one batched GPU call) and rank 0 receives every result in
+    problem order (None on the other ranks).  Returns (results, this rank's
+    problem indices)."""
+    cost = cost or (lambda p: p.lx * p.ly * p.lz)
+    mine = partition_by_cost([cost(p) for p in problems], ws)[rank]
+    local = list(solve_share([problems[i] for i in mine])) if mine else []
+    if len(local) != len(mine):
+        raise RuntimeError("solve_share returned %d results for %d problems" % (len(local), len(mine)))
+    return gather_results(local, mine, ws, rank, len(problems)), mine
