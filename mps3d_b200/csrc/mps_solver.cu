@@ -213,6 +213,7 @@ struct Ctx {
     };
     std::vector<Lane> lanes;  // created at the first host call with pageable arrays
     bool tma_ok = false;      // the shared-memory colour pass can run (set at workspace set-up)
+    bool tma_allowed = true;  // MPS_TMA=0 at handle creation: the register-fed kernels only (for comparisons)
     size_t inbuf_bytes = 0;
     Signature sig;
     int nlev = 0;
@@ -1181,7 +1182,7 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
     // the arena zeroes new blocks with cudaMemset on the legacy stream; the
     // solver's stream does not synchronise with it, so wait here
     if (cudaDeviceSynchronize() != cudaSuccess) return MPS_ERR_CUDA;
-    ctx.tma_ok = tma_prepare();
+    ctx.tma_ok = ctx.tma_allowed && tma_prepare();
     ctx.sig = sig;
     return 0;
 }
@@ -1875,6 +1876,9 @@ int mps_create(mps_handle* h, int device)
         const long long v = std::atoll(cap);
         if (v > 0) ctx.ar.limit = ctx.kar.limit = (size_t)v;
     }
+    // the shared-memory (TMA) kernels and the register-fed ones give the same
+    // results; the variable selects the register-fed ones (for comparisons)
+    if (const char* tv = std::getenv("MPS_TMA")) ctx.tma_allowed = std::atoi(tv) != 0;
     if (cudaDeviceGetAttribute(&ctx.nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || ctx.nsm < 1) {
         delete H;
         return MPS_ERR_CUDA;

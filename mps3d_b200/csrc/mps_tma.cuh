@@ -107,6 +107,69 @@ __device__ __forceinline__ VecW<T, W> lds(const T* p)
     return r;
 }
 
+// The diagonal and the off-diagonal sum of one group (W cells of one row) of
+// an interior row from staged rows: U0 the other colour's row of the cells,
+// Uym/Uyp/Uzm/Uzp its y and z neighbour rows, K* the other colour's
+// coefficients on the same rows, Kc the cells' own coefficients.  Faces y-,
+// y+, z-, z+ then x, the operation order of group_rows / row_finish for
+// interior groups.
+template <class T, int W, bool KF>
+__device__ __forceinline__ void tile_rows(const KOp<T>& op, const T* U0, const T* Uym, const T* Uyp, const T* Uzm,
+                                          const T* Uzp, const T* K0, const T* Kym, const T* Kyp, const T* Kzm,
+                                          const T* Kzp, const T* Kc, int h0, int q, T cr0, T cr1, T cr2,
+                                          VecW<T, W>& diag, VecW<T, W>& off)
+{
+    const VecW<T, W> kc4 = KF ? lds<T, W>(Kc + h0) : zerov<T, W>();
+    VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
+    auto face = [&](const T* Ur, const T* Kr, T cf) {
+        const VecW<T, W> un = lds<T, W>(Ur + h0);
+        if (KF) {
+            const VecW<T, W> kn = lds<T, W>(Kr + h0);
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+                const T wt = (kc4.v[e] + kn.v[e]) * cf;
+                wsum.v[e] += wt;
+                acc.v[e] += wt * un.v[e];
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+                wsum.v[e] += cf;
+                acc.v[e] += cf * un.v[e];
+            }
+        }
+    };
+    face(Uym, Kym, cr1);
+    face(Uyp, Kyp, cr1);
+    face(Uzm, Kzm, cr2);
+    face(Uzp, Kzp, cr2);
+    const VecW<T, W> ax = lds<T, W>(U0 + h0);
+    const VecW<T, W> akx = KF ? lds<T, W>(K0 + h0) : zerov<T, W>();
+    const int so = q ? h0 + W : h0 - 1;
+    const T sx = U0[so];
+    const T skx = KF ? K0[so] : T(0);
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        T uxm, kxm, uxp, kxp;
+        if (q) {
+            uxm = ax.v[e]; kxm = akx.v[e];
+            uxp = e < W - 1 ? ax.v[e + 1] : sx; kxp = e < W - 1 ? akx.v[e + 1] : skx;
+        } else {
+            uxm = e > 0 ? ax.v[e - 1] : sx; kxm = e > 0 ? akx.v[e - 1] : skx;
+            uxp = ax.v[e]; kxp = akx.v[e];
+        }
+        const T kc = KF ? kc4.v[e] : op.kc;
+        const T d0 = op.dexc;
+        T w0, w1;
+        if (KF) { w0 = (kc + kxm) * cr0; w1 = (kc + kxp) * cr0; }
+        else { w0 = cr0; w1 = cr0; }
+        const T ws = wsum.v[e] + (w0 + w1);
+        const T ac = acc.v[e] + (w0 * uxm + w1 * uxp);
+        if (KF) { diag.v[e] = d0 + T(0.5) * ws; off.v[e] = T(-0.5) * ac; }
+        else { diag.v[e] = d0 + kc * ws; off.v[e] = -kc * ac; }
+    }
+}
+
 // the launch description of k_colour_tma
 struct TmaColour {
     int njb, nkb, tk;     // row blocks, plane chunks, planes per chunk
@@ -252,59 +315,13 @@ __global__ void __launch_bounds__(TJ * 32) k_colour_tma(Lev L, KOp<T> op, int c,
             T* orow = out + (size_t)P * (j + (size_t)L.ny * k);
             for (int g = tc.g_lo + lane; g <= tc.g_hi; g += 32) {
                 const int h0 = W * g;
-                const VecW<T, W> kc4 = KF ? lds<T, W>(Kc + h0) : zerov<T, W>();
-                VecW<T, W> acc = zerov<T, W>(), wsum = zerov<T, W>();
-                auto face = [&](const T* Ur, const T* Kr, T cf) {
-                    const VecW<T, W> un = lds<T, W>(Ur + h0);
-                    if (KF) {
-                        const VecW<T, W> kn = lds<T, W>(Kr + h0);
-#pragma unroll
-                        for (int e = 0; e < W; e++) {
-                            const T wt = (kc4.v[e] + kn.v[e]) * cf;
-                            wsum.v[e] += wt;
-                            acc.v[e] += wt * un.v[e];
-                        }
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < W; e++) {
-                            wsum.v[e] += cf;
-                            acc.v[e] += cf * un.v[e];
-                        }
-                    }
-                };
-                face(Uym, Kym, cr1);
-                face(Uyp, Kyp, cr1);
-                face(Uzm, Kzm, cr2);
-                face(Uzp, Kzp, cr2);
-                const VecW<T, W> ax = lds<T, W>(U0 + h0);
-                const VecW<T, W> akx = KF ? lds<T, W>(K0 + h0) : zerov<T, W>();
-                const int so = q ? h0 + W : h0 - 1;
-                const T sx = U0[so];
-                const T skx = KF ? K0[so] : T(0);
+                VecW<T, W> diag, off;
+                tile_rows<T, W, KF>(op, U0, Uym, Uyp, Uzm, Uzp, K0, Kym, Kyp, Kzm, Kzp, Kc, h0, q, cr0, cr1, cr2, diag,
+                                    off);
                 const VecW<T, W> f4 = lds<T, W>(Fr + h0);
                 VecW<T, W> res;
 #pragma unroll
-                for (int e = 0; e < W; e++) {
-                    T uxm, kxm, uxp, kxp;
-                    if (q) {
-                        uxm = ax.v[e]; kxm = akx.v[e];
-                        uxp = e < W - 1 ? ax.v[e + 1] : sx; kxp = e < W - 1 ? akx.v[e + 1] : skx;
-                    } else {
-                        uxm = e > 0 ? ax.v[e - 1] : sx; kxm = e > 0 ? akx.v[e - 1] : skx;
-                        uxp = ax.v[e]; kxp = akx.v[e];
-                    }
-                    const T kc = KF ? kc4.v[e] : op.kc;
-                    const T d0 = op.dexc;
-                    T w0, w1;
-                    if (KF) { w0 = (kc + kxm) * cr0; w1 = (kc + kxp) * cr0; }
-                    else { w0 = cr0; w1 = cr0; }
-                    const T ws = wsum.v[e] + (w0 + w1);
-                    const T ac = acc.v[e] + (w0 * uxm + w1 * uxp);
-                    T diag, off;
-                    if (KF) { diag = d0 + T(0.5) * ws; off = T(-0.5) * ac; }
-                    else { diag = d0 + kc * ws; off = -kc * ac; }
-                    res.v[e] = gs_value(f4.v[e], diag, off);
-                }
+                for (int e = 0; e < W; e++) res.v[e] = gs_value(f4.v[e], diag.v[e], off.v[e]);
                 stv<T, W>(orow + h0, res);
             }
         }
