@@ -4,11 +4,12 @@
 // set-up (solve_impl with prepare_only).  The iteration then runs as a fixed
 // list of batched steps -- one kernel launch per colour pass, transfer,
 // coarsest solve, outer residual, correction and convergence check -- that
-// cover every problem taking part in the step.  A launch is a persistent,
-// grid-stride loop over tasks: a task is one block-sized tile of one problem,
-// found by a binary search over the step's task prefix; the block copies that
-// problem's descriptor (its level, operator and buffers) into shared memory
-// and runs the same device function as the single-problem kernel.  Problems
+// cover every problem taking part in the step.  A launch is a persistent
+// loop over tasks: a task is one block-sized tile of one problem, and each
+// block takes a contiguous range of the step's tasks, looking up the problem
+// (a binary search over the step's task prefix) and copying its descriptor
+// (level, operator, buffers) into shared memory when the range enters it; it
+// runs the same device function as the single-problem kernel.  Problems
 // whose hierarchies are shallower simply take no part in the deeper steps;
 // converged problems are skipped at run time through a per-problem flag.
 //
@@ -19,7 +20,7 @@
 // iterations, and the check kernel also counts the body's executions and
 // stops at maxit + 2, so the loop always ends.
 //
-// The launch shape (blocks of the grid-stride loop, and the colour pass's
+// The launch shape (blocks of the task loop, and the colour pass's
 // cells per thread, per level depth) is picked by timing every candidate
 // pair on the batch's own colour passes at the first call with a given batch
 // structure.
@@ -108,20 +109,41 @@ __device__ __forceinline__ void load_desc(const D* __restrict__ desc, int seg, u
     for (int w = threadIdx.x; w < (int)(sizeof(D) / 4); w += blockDim.x) dst[w] = __ldg(&src[w]);
 }
 
-// grid-stride loop over the tasks of one batched step; body(desc, t, problem)
+// The tasks of one batched step, each block taking a contiguous range: the
+// segment (problem) is found, its descriptor copied into shared memory and
+// its active flag read only when the range enters a new segment, and an
+// inactive problem's remaining tasks are skipped at once.  Measured on the
+// 64-problem batch: 52.6 / 68.2 ms (mixed / FP64) against 60.3 / 93.7 ms for
+// a grid-stride loop that looked up the segment and copied the descriptor
+// for every task.
 #define BATCH_LOOP(D, desc, task0, pid, nseg, total, active, ...)                                               \
     __shared__ __align__(16) unsigned char sbuf_[sizeof(D)];                                                   \
-    for (int task = blockIdx.x; task < (total); task += gridDim.x) {                                           \
-        const int seg = find_seg(task0, nseg, task);                                                           \
-        const int prob = __ldg(&(pid)[seg]);                                                                   \
-        if (!((volatile const int*)&(active)[prob].active)[0]) continue;                                       \
-        __syncthreads();                                                                                       \
-        load_desc<D>(desc, seg, sbuf_);                                                                        \
-        __syncthreads();                                                                                       \
-        const D& d = *reinterpret_cast<const D*>(sbuf_);                                                       \
-        const unsigned t = (unsigned)(task - __ldg(&(task0)[seg])) * TPB + threadIdx.x;                        \
-        (void)t;                                                                                               \
-        __VA_ARGS__                                                                                            \
+    {                                                                                                          \
+        const int per_ = ((total) + (int)gridDim.x - 1) / (int)gridDim.x;                                     \
+        const int beg_ = (int)blockIdx.x * per_;                                                               \
+        const int end_ = min((total), beg_ + per_);                                                            \
+        int seg = 0, segbeg_ = 0, segend_ = beg_;                                                              \
+        bool act_ = false;                                                                                     \
+        for (int task = beg_; task < end_; task++) {                                                           \
+            if (task >= segend_) {                                                                             \
+                seg = find_seg(task0, nseg, task);                                                             \
+                segbeg_ = __ldg(&(task0)[seg]);                                                                \
+                segend_ = __ldg(&(task0)[seg + 1]);                                                            \
+                const int prob = __ldg(&(pid)[seg]);                                                           \
+                act_ = ((volatile const int*)&(active)[prob].active)[0] != 0;                                  \
+                __syncthreads();                                                                               \
+                if (act_) load_desc<D>(desc, seg, sbuf_);                                                      \
+                __syncthreads();                                                                               \
+            }                                                                                                  \
+            if (!act_) {                                                                                       \
+                task = segend_ - 1;                                                                            \
+                continue;                                                                                      \
+            }                                                                                                  \
+            const D& d = *reinterpret_cast<const D*>(sbuf_);                                                   \
+            const unsigned t = (unsigned)(task - segbeg_) * TPB + threadIdx.x;                                 \
+            (void)t;                                                                                           \
+            __VA_ARGS__                                                                                        \
+        }                                                                                                      \
     }
 
 // Shapes of the batched steps, measured on the 64-problem batch (sizes 33 to
