@@ -43,6 +43,8 @@ struct DColour {
     const T* u1;  // state: black half (already offset by half)
     T* out;       // this colour's half of the other buffer
     const T* f;   // this colour's half of the right-hand side
+    ColourSplit cs;  // interior groups and shell of the vector body (when split)
+    int split;       // 1: the vector body's tasks follow cs (interior without boundary code, then the shell)
 };
 template <class T>
 struct DRestrict {
@@ -80,6 +82,8 @@ struct DOuter {
     const double* x;  // split base
     const double* b;  // split base
     T* r;             // split base (finest right-hand side of the T hierarchy)
+    ColourSplit cs;   // interior groups and shell of the vector residual (when split)
+    int split;        // 1: the tasks follow cs (BATCH_W cells of a row per thread)
 };
 template <class T>
 struct DAxpy {
@@ -197,8 +201,17 @@ __device__ __forceinline__ void colour_group_body(const Lev& L, const KOp<T>& op
 template <class T, class U>
 __device__ __forceinline__ void batch_colour(const DColour<T>& d, int c, const U& u, unsigned t, int vec)
 {
-    if (vec && batch_vector_level(d.L)) colour_group_body<T, U>(d.L, d.op, c, u, d.out, d.f, t);
-    else colour_body<T, KOp<T>, U>(d.L, d.op, c, u, d.out, d.f, t);
+    if (vec && batch_vector_level(d.L)) {
+        if (d.split) {
+            // the task's block of the split pass (t = block * TPB + thread)
+            if (d.L.uniform) colour_split_block<T, BATCH_W, U, true>(d.L, d.op, c, u, d.out, d.f, d.cs, t / TPB);
+            else colour_split_block<T, BATCH_W, U, false>(d.L, d.op, c, u, d.out, d.f, d.cs, t / TPB);
+        } else {
+            colour_group_body<T, U>(d.L, d.op, c, u, d.out, d.f, t);
+        }
+    } else {
+        colour_body<T, KOp<T>, U>(d.L, d.op, c, u, d.out, d.f, t);
+    }
 }
 
 // vec: the vector body on the levels that have one (the task layout of the
@@ -323,7 +336,8 @@ __global__ void __launch_bounds__(TPB) kb_outer(const DOuter<T>* __restrict__ de
         CSplit<double> x;
         x.c[0] = d.x;
         x.c[1] = d.x + d.L.half;
-        for (int c = 0; c < 2; c++) {
+        if (d.split) resid_split_chunk<double, BATCH_W, T>(d.L, d.op, x, d.b, d.r, d.cs, t / TPB, rr, bb);
+        else for (int c = 0; c < 2; c++) {
             int i, j, k;
             if (t < n && decode(d.L, t, c, i, j, k)) {
                 double diag, off;
@@ -598,6 +612,8 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                 x.u1 = cur1(p, d);
                 x.out = c == 0 ? H.U[d][ri[p][d] ^ 1] : H.U[d][bi[p][d] ^ 1] + L.half;
                 x.f = H.F[d] + (c ? L.half : 0);
+                x.split = batch_vector_level(L) && make_split(L, BATCH_W, x.cs) ? 1 : 0;
+                if (!x.split) std::memset(&x.cs, 0, sizeof(x.cs));
                 if (c == 0) ri[p][d] ^= 1;
                 else bi[p][d] ^= 1;
                 return x;
@@ -612,7 +628,10 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
         for (int q = 0; q < s.nseg; q++) {
             t0v.push_back(tot);
             const Lev& L = B.sub[pid[q]]->lev[d];
-            tot += batch_vector_level(L) ? nb(L.half / BATCH_W) : nb(L.half);
+            ColourSplit cs;
+            if (!batch_vector_level(L)) tot += nb(L.half);
+            else if (make_split(L, BATCH_W, cs)) tot += (int)(cs.nb_in + cs.nb_xe + cs.nb_face);
+            else tot += nb(L.half / BATCH_W);
         }
         t0v.push_back(tot);
         std::vector<int> pids(pid, pid + s.nseg);
@@ -701,9 +720,16 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                 x.x = sc.x64;
                 x.b = sc.b64;
                 x.r = batch_hier<T>(sc).F[0];
+                x.split = sc.lev[0].uniform && make_split(sc.lev[0], BATCH_W, x.cs) ? 1 : 0;
+                if (!x.split) std::memset(&x.cs, 0, sizeof(x.cs));
                 return x;
             },
-            [&](int p) { return nb(B.sub[p]->lev[0].half); });
+            [&](int p) {
+                const Lev& L = B.sub[p]->lev[0];
+                ColourSplit cs;
+                if (L.uniform && make_split(L, BATCH_W, cs)) return (int)(cs.nb_in + cs.nb_xe + cs.nb_face);
+                return nb(L.half);
+            });
     };
     outer(P.pre);
     for (int c = 0; c < inner; c++) vcycle(P.body, c == 0);

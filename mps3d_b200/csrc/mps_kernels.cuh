@@ -1252,14 +1252,15 @@ struct ColourSplit {
 // UNI: the level is uniform (shell rows take the regular coefficients too);
 // on a level whose last cells are merged the interior stops one cell short
 // of them, so its faces are regular either way
-template <class T, int W, class U, int MB, bool UNI = true>
-__global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
-                                                           const T* __restrict__ f, ColourSplit cs)
+// block blk of a split colour pass (TPB threads)
+template <class T, int W, class U, bool UNI = true>
+__device__ __forceinline__ void colour_split_block(const Lev& L, const KOp<T>& op, int c, const U& u,
+                                                   T* __restrict__ out, const T* __restrict__ f,
+                                                   const ColourSplit& cs, unsigned blk)
 {
-    pdl_wait();
     int part;
     unsigned idx;
-    split_chunk(cs.nb_in, cs.nb_xe, blockIdx.x, part, idx);
+    split_chunk(cs.nb_in, cs.nb_xe, blk, part, idx);
     if (part == 0) {
         const unsigned t = idx * TPB + threadIdx.x;
         if (t >= cs.n_in) return;
@@ -1312,19 +1313,27 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
     stv<T, W>(out + o0, res);
 }
 
+template <class T, int W, class U, int MB, bool UNI = true>
+__global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int c, U u, T* __restrict__ out,
+                                                           const T* __restrict__ f, ColourSplit cs)
+{
+    pdl_wait();
+    colour_split_block<T, W, U, UNI>(L, op, c, u, out, f, cs, blockIdx.x);
+}
+
 // Residual r = f - A u of both colours on a uniform level (the outer
 // residual of a solve), the interior groups without boundary code and the
 // shell apart, grid-stride over each part; r optionally stored as R, the
 // sums of r^2 and f^2 reduced as in k_residv.
+// chunk ch (a block's worth of threads, in the interleaved order of
+// split_chunk) of the split residual of both colours on a uniform level:
+// r = f - A u stored as R when rout is set, the sums of r^2 and f^2 added to
+// rr and ff
 template <class T, int W, class R>
-__global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L, KOp<T> op, CSplit<T> u,
-                                                                           const T* __restrict__ f,
-                                                                           R* __restrict__ rout, RedBuf rb,
-                                                                           ColourSplit cs)
+__device__ __forceinline__ void resid_split_chunk(const Lev& L, const KOp<T>& op, const CSplit<T>& u,
+                                                  const T* __restrict__ f, R* __restrict__ rout,
+                                                  const ColourSplit& cs, unsigned ch, double& rr, double& ff)
 {
-    pdl_wait();
-    __shared__ double sh[32];
-    double rr = 0.0, ff = 0.0;
     auto group = [&](int j, int k, int g, auto in) {
         constexpr bool IN = decltype(in)::value;
         const int row = j + L.ny * k;
@@ -1350,38 +1359,49 @@ __global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L
             if (rout) stv<R, W>(rout + (cc ? L.half : 0) + o0, r4);
         }
     };
+    int part;
+    unsigned idx;
+    split_chunk(cs.nb_in, cs.nb_xe, ch, part, idx);
+    const unsigned t = idx * TPB + threadIdx.x;
+    if (part == 0) {
+        if (t >= cs.n_in) return;
+        const unsigned r = cs.gin.div(t);
+        const int g = cs.g_lo + (int)(t - r * cs.gin.d);
+        const unsigned kk = cs.yin.div(r);
+        group(1 + (int)(r - kk * cs.yin.d), 1 + (int)kk, g, std::true_type());
+        return;
+    }
+    int j, k, g;
+    if (part == 1) {
+        if (t >= cs.n_xe) return;
+        const unsigned r = cs.gx.div(t);
+        const unsigned e = t - r * cs.gx.d;
+        g = e < (unsigned)cs.g_lo ? (int)e : cs.g_hi + 1 + (int)(e - cs.g_lo);
+        const unsigned kk = cs.yin.div(r);
+        k = 1 + (int)kk;
+        j = 1 + (int)(r - kk * cs.yin.d);
+    } else {
+        if (t >= cs.n_face) return;
+        const unsigned r = cs.g.div(t);
+        g = (int)(t - r * cs.g.d);
+        shell_row(r, L.ny, cs.b, j, k);
+    }
+    group(j, k, g, std::false_type());
+}
+
+template <class T, int W, class R>
+__global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L, KOp<T> op, CSplit<T> u,
+                                                                           const T* __restrict__ f,
+                                                                           R* __restrict__ rout, RedBuf rb,
+                                                                           ColourSplit cs)
+{
+    pdl_wait();
+    __shared__ double sh[32];
+    double rr = 0.0, ff = 0.0;
     // block-sized chunks, grid-stride, in the interleaved order of split_chunk
     const unsigned nchunks = cs.nb_in + cs.nb_xe + cs.nb_face;
-    for (unsigned ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        int part;
-        unsigned idx;
-        split_chunk(cs.nb_in, cs.nb_xe, ch, part, idx);
-        const unsigned t = idx * TPB + threadIdx.x;
-        if (part == 0) {
-            if (t >= cs.n_in) continue;
-            const unsigned r = cs.gin.div(t);
-            const int g = cs.g_lo + (int)(t - r * cs.gin.d);
-            const unsigned kk = cs.yin.div(r);
-            group(1 + (int)(r - kk * cs.yin.d), 1 + (int)kk, g, std::true_type());
-            continue;
-        }
-        int j, k, g;
-        if (part == 1) {
-            if (t >= cs.n_xe) continue;
-            const unsigned r = cs.gx.div(t);
-            const unsigned e = t - r * cs.gx.d;
-            g = e < (unsigned)cs.g_lo ? (int)e : cs.g_hi + 1 + (int)(e - cs.g_lo);
-            const unsigned kk = cs.yin.div(r);
-            k = 1 + (int)kk;
-            j = 1 + (int)(r - kk * cs.yin.d);
-        } else {
-            if (t >= cs.n_face) continue;
-            const unsigned r = cs.g.div(t);
-            g = (int)(t - r * cs.g.d);
-            shell_row(r, L.ny, cs.b, j, k);
-        }
-        group(j, k, g, std::false_type());
-    }
+    for (unsigned ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
+        resid_split_chunk<T, W, R>(L, op, u, f, rout, cs, ch, rr, ff);
     const double a = block_sum(rr, sh);
     const double b = block_sum(ff, sh);
     if (!rb.partial) return;
