@@ -54,6 +54,13 @@ struct DRestrict {
     const T* u1;
     const T* f;  // fine right-hand side (split base)
     T* fc;       // coarse right-hand side (split base)
+    // the single solve's two-part form (w > 0: the bulk's red residuals, w
+    // coarse cells of a row per thread, then the shell cells, eight lanes
+    // each); w = 0: one thread per coarse cell over all its children
+    RestrictSplit rs;
+    Box bx;
+    unsigned nb_bulk, shell;
+    int w;
     int geom;
 };
 template <class T>
@@ -251,6 +258,27 @@ __global__ void __launch_bounds__(TPB) kb_restrict(const DRestrict<T>* __restric
         u.c[1] = d.u1;
         f.c[0] = d.f;
         f.c[1] = d.f + d.F.half;
+        if (d.w) {
+            Split<T> fc;
+            fc.c[0] = d.fc;
+            fc.c[1] = d.fc + d.C.half;
+            const unsigned blk = t / TPB;
+            if (blk < d.nb_bulk) {
+                if (d.F.uniform) {
+                    if (d.w == 4) resid_restrict_bulk<T, 4, true>(d.F, d.op, u, d.f, d.C, fc, d.bx, d.rs, blk);
+                    else if (d.w == 2) resid_restrict_bulk<T, 2, true>(d.F, d.op, u, d.f, d.C, fc, d.bx, d.rs, blk);
+                    else resid_restrict_bulk<T, 1, true>(d.F, d.op, u, d.f, d.C, fc, d.bx, d.rs, blk);
+                } else {
+                    if (d.w == 4) resid_restrict_bulk<T, 4, false>(d.F, d.op, u, d.f, d.C, fc, d.bx, d.rs, blk);
+                    else if (d.w == 2) resid_restrict_bulk<T, 2, false>(d.F, d.op, u, d.f, d.C, fc, d.bx, d.rs, blk);
+                    else resid_restrict_bulk<T, 1, false>(d.F, d.op, u, d.f, d.C, fc, d.bx, d.rs, blk);
+                }
+            } else {
+                resid_restrict_shell<T, KOp<T>>(d.F, d.op, u, f, d.C, fc, d.geom, d.bx, d.shell,
+                                                (blk - d.nb_bulk) * TPB + threadIdx.x);
+            }
+            continue;
+        }
         if (!MPS_BATCH_R8) {  // one thread per coarse cell over all its children
             Split<T> fc;
             fc.c[0] = d.fc;
@@ -594,6 +622,26 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
         list.push_back(s);
     };
     auto nb = [](long long n) { return (int)((n + TPB - 1) / TPB); };
+    // the two-part restriction of the single solve where it applies (the red
+    // residual alone is valid after a black pass), with the single solve's
+    // cells per thread by level index
+    auto restrict_form = [&](const Lev& F, const Lev& C, int d, RestrictSplit& rs, Box& bx, unsigned& nbb,
+                             unsigned& shell, int& w) {
+        std::memset(&rs, 0, sizeof(rs));
+        std::memset(&bx, 0, sizeof(bx));
+        nbb = shell = 0;
+        w = 0;
+        if (o->nu1 < 1 || F.nx < 16 || !restrict_box(F, C, bx)) return false;
+        w = d == 0 ? RestrictShape<T>::W : d == 1 ? CoarseXferShape<T>::W : SmallXferShape<T>::W;
+        if (w != 1 && w != 2 && w != 4) {
+            w = 0;
+            return false;
+        }
+        rs = make_restrict_split(F, C, bx, w);
+        nbb = rs.nb_in + rs.nb_xe + rs.nb_out;
+        shell = (unsigned)((long long)C.nx * C.ny * C.nz - box_cells(bx));
+        return true;
+    };
     auto cur0 = [&](int p, int d) { return batch_hier<T>(*B.sub[p]).U[d][ri[p][d]]; };
     auto cur1 = [&](int p, int d) {
         return batch_hier<T>(*B.sub[p]).U[d][bi[p][d]] + B.sub[p]->lev[d].half;
@@ -661,10 +709,17 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                     x.f = H.F[d];
                     x.fc = H.F[d + 1];
                     x.geom = sc.xf[d].geom;
+                    restrict_form(x.F, x.C, d, x.rs, x.bx, x.nb_bulk, x.shell, x.w);
                     return x;
                 },
                 [&](int p) {
+                    const Lev& F = B.sub[p]->lev[d];
                     const Lev& C = B.sub[p]->lev[d + 1];
+                    RestrictSplit rs;
+                    Box bx;
+                    unsigned nbb, shell;
+                    int w;
+                    if (restrict_form(F, C, d, rs, bx, nbb, shell, w)) return (int)(nbb + nblk(8LL * shell));
                     return nb((MPS_BATCH_R8 ? 8LL : 1LL) * C.nx * C.ny * C.nz);
                 });
         }
