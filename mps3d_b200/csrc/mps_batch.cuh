@@ -81,6 +81,12 @@ struct DProlong {
     const T* e1;
     int mode;  // 1: the black cells and the red cells of odd periodic seams (the
                // first post-smoothing pass rewrites the other red cells); -1: all
+    // the single solve's vector bulk (w > 0: w cells of a row per thread in
+    // the parts of pp, within box pb; the same cells as mode 1)
+    Box pb, sb;
+    ProlongDiv dv, sv;
+    ProlongParts pp;
+    int w;
 };
 template <class T>
 struct DOuter {
@@ -166,9 +172,14 @@ __device__ __forceinline__ void load_desc(const D* __restrict__ desc, int seg, u
 //   4 (both)   8 lanes per cell     black cells     67.7 / 108.6
 //   4 (FP32)   1 thread per cell    black cells     59.9 / 90.6
 // (colour: cells of a row per thread on levels with a vector row evaluation;
-// black cells: the first post-smoothing pass rewrites the red ones).  Kept:
-// one thread per coarse cell, black cells, and the colour-pass body picked
-// per depth by the autotuner together with the grid (below).
+// black cells: the first post-smoothing pass rewrites the red ones).  Then,
+// with the task ranges of BATCH_LOOP (52.6 / 68.2), the single solve's
+// forms step by step: the colour pass and the outer residual split into
+// interior groups and shell (50.7 / 60.8, then 47.2 / 60.5), the two-part
+// restriction (44.4 / 55.3) and the vector prolongation bulk (40.6 / 51.6).
+// Kept: the single solve's forms where a level has them (the generic
+// bodies elsewhere), and the colour-pass body picked per depth by the
+// autotuner together with the grid (below).
 #ifndef MPS_BATCH_R8
 #define MPS_BATCH_R8 0
 #endif
@@ -340,7 +351,12 @@ __global__ void __launch_bounds__(TPB) kb_prolong(const DProlong<T>* __restrict_
         CSplit<T> e;
         e.c[0] = d.e0;
         e.c[1] = d.e1;
-        if (d.mode < 0) {
+        if (d.w) {
+            const unsigned blk = t / TPB;
+            if (d.w == 4) prolong_v_block<T, 4>(d.F, u, d.C, e, d.X, d.pb, d.dv, d.sb, d.sv, d.pp, blk);
+            else if (d.w == 2) prolong_v_block<T, 2>(d.F, u, d.C, e, d.X, d.pb, d.dv, d.sb, d.sv, d.pp, blk);
+            else prolong_v_block<T, 1>(d.F, u, d.C, e, d.X, d.pb, d.dv, d.sb, d.sv, d.pp, blk);
+        } else if (d.mode < 0) {
             prolong_body<T>(d.F, u, d.C, e, d.X, -1, t);
         } else {
             prolong_body<T>(d.F, u, d.C, e, d.X, 1, t);
@@ -622,6 +638,26 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
         list.push_back(s);
     };
     auto nb = [](long long n) { return (int)((n + TPB - 1) / TPB); };
+    // the single solve's vector prolongation where it applies (black cells
+    // and odd-seam red cells, the geometric hierarchy's regular box), with its
+    // cells per thread by level index
+    auto prolong_vform = [&](const Lev& F, const Lev& C, const Xfer& X, int d, Box& pb, ProlongDiv& dv, Box& sb,
+                             ProlongDiv& sv, ProlongParts& pp, int& w) {
+        std::memset(&pb, 0, sizeof(pb));
+        std::memset(&sb, 0, sizeof(sb));
+        std::memset(&dv, 0, sizeof(dv));
+        std::memset(&sv, 0, sizeof(sv));
+        std::memset(&pp, 0, sizeof(pp));
+        w = 0;
+        if (!MPS_BATCH_PB || o->nu2 < 1 || F.nx < 16 || !prolong_box(F, C, X, pb)) return false;
+        w = d == 0 ? ProlongShape<T>::W : d == 1 ? CoarseXferShape<T>::W : SmallXferShape<T>::W;
+        if (w != 1 && w != 2 && w != 4) {
+            w = 0;
+            return false;
+        }
+        prolong_form(F, pb, w, dv, sb, sv, pp);
+        return true;
+    };
     // the two-part restriction of the single solve where it applies (the red
     // residual alone is valid after a black pass), with the single solve's
     // cells per thread by level index
@@ -752,10 +788,17 @@ static void plan_batch(BatchState& B, BatchPlan<T>& P, const mps_solver_opts* o,
                     x.e0 = cur0(p, d + 1);
                     x.e1 = cur1(p, d + 1);
                     x.mode = (MPS_BATCH_PB && o->nu2 >= 1) ? 1 : -1;
+                    prolong_vform(x.F, x.C, x.X, d, x.pb, x.dv, x.sb, x.sv, x.pp, x.w);
                     return x;
                 },
                 [&](int p) {
                     const Lev& F = B.sub[p]->lev[d];
+                    Box pb, sb;
+                    ProlongDiv dv, sv;
+                    ProlongParts pp;
+                    int w;
+                    if (prolong_vform(F, B.sub[p]->lev[d + 1], B.sub[p]->xf[d], d, pb, dv, sb, sv, pp, w))
+                        return (int)pp.blk0[4];
                     return (MPS_BATCH_PB && o->nu2 >= 1) ? nb(F.half) : nb((long long)F.nx * F.ny * F.nz);
                 });
             for (int s = 0; s < o->nu2; s++) {

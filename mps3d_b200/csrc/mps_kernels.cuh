@@ -1071,15 +1071,17 @@ struct ProlongParts {
     unsigned blk0[5];  // first block of each part, and the total
 };
 
+// block blk (TPB threads) of the prolongation bulk: the parts in pp's order
 template <class T, int W>
-__global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, Box pbox,
-                                                   ProlongDiv pdiv, Box sbox, ProlongDiv sdiv, ProlongParts pp)
+__device__ __forceinline__ void prolong_v_block(const Lev& F, const Split<T>& u, const Lev& C, const CSplit<T>& e,
+                                                const Xfer& X, const Box& pbox, const ProlongDiv& pdiv,
+                                                const Box& sbox, const ProlongDiv& sdiv, const ProlongParts& pp,
+                                                unsigned blk)
 {
-    pdl_wait();
     int part = 0;
-    while (part < 3 && blockIdx.x >= pp.blk0[part + 1]) part++;
+    while (part < 3 && blk >= pp.blk0[part + 1]) part++;
     const int mode = part == 0 ? 0 : (part == 1 ? 3 : (part == 2 ? 1 : 2));
-    const unsigned t = (blockIdx.x - pp.blk0[part]) * TPB + threadIdx.x;
+    const unsigned t = (blk - pp.blk0[part]) * TPB + threadIdx.x;
     if (t >= pp.cnt[part]) return;
     // field-wise selection keeps both parameter structs out of local memory
     const bool m2 = mode == 2;
@@ -1222,6 +1224,14 @@ __global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSp
         lin_axis<T>(X, 0, i, xreg, x0, x1, tx);
         base[el] = base[el] + trilinear<T>(C, e, x0, x1, tx, y0, y1, ty, z0, z1, tz);
     }
+}
+
+template <class T, int W>
+__global__ void __launch_bounds__(TPB) k_prolong_v(Lev F, Split<T> u, Lev C, CSplit<T> e, Xfer X, Box pbox,
+                                                   ProlongDiv pdiv, Box sbox, ProlongDiv sdiv, ProlongParts pp)
+{
+    pdl_wait();
+    prolong_v_block<T, W>(F, u, C, e, X, pbox, pdiv, sbox, sdiv, pp, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------

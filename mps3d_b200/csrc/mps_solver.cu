@@ -571,6 +571,47 @@ static long long box_cells(const Box& b)
     return (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
 }
 
+// the launch description of the prolongation bulk (k_prolong_v) of fine
+// level L with box pb and W cells per thread: the regular rows in 2 x 2
+// blocks, their x ends, the rows outside the box, and the red cells of odd
+// periodic seams; pp.blk0[4] blocks in all
+static void prolong_form(const Lev& L, const Box& pb, int W, ProlongDiv& dv, Box& sb, ProlongDiv& sv,
+                         ProlongParts& pp)
+{
+    const long long G = (L.nh + W - 1) / W;  // groups holding a cell (the rest of the P / W are pads)
+    const long long rall = (long long)L.ny * L.nz;
+    const long long rin = (long long)(pb.hi[1] - pb.lo[1] + 1) * (pb.hi[2] - pb.lo[2] + 1);
+    dv.g.init((unsigned)G);
+    dv.yin.init((unsigned)(pb.hi[1] - pb.lo[1] + 1));
+    dv.yin2.init((unsigned)(pb.hi[1] - pb.lo[1] + 1) / 2);
+    dv.nh.init((unsigned)((L.nx + 1) / 2));
+    // groups with every cell in the box for both row parities: 2Wg >= lo,
+    // 2W(g+1) - 1 <= hi
+    dv.g_lo = (pb.lo[0] + 2 * W - 1) / (2 * W);
+    dv.g_hi = (pb.hi[0] + 1) / (2 * W) - 1;
+    const long long gin = dv.g_hi >= dv.g_lo ? dv.g_hi - dv.g_lo + 1 : 0;
+    if (gin == 0) { dv.g_lo = 0; dv.g_hi = -1; }
+    dv.gin.init((unsigned)std::max<long long>(gin, 1));
+    dv.gout.init((unsigned)std::max<long long>(G - gin, 1));
+    // red cells on odd periodic seams (read by the next red pass)
+    const int sy = L.per[1] && (L.ny & 1), sz = L.per[2] && (L.nz & 1), sx = L.per[0] && (L.nx & 1);
+    sb.lo[0] = 0;
+    sb.hi[0] = L.nx - 1;
+    sb.lo[1] = sy;
+    sb.hi[1] = L.ny - 1 - sy;
+    sb.lo[2] = sz;
+    sb.hi[2] = L.nz - 1 - sz;
+    const long long rin2 = (long long)(sb.hi[1] - sb.lo[1] + 1) * (sb.hi[2] - sb.lo[2] + 1);
+    sv = dv;
+    sv.yin.init((unsigned)(sb.hi[1] - sb.lo[1] + 1));
+    pp.cnt[0] = (unsigned)(rin / 4 * gin);  // 2 x 2 row blocks
+    pp.cnt[1] = (unsigned)(rin * (G - gin));
+    pp.cnt[2] = (unsigned)((rall - rin) * G);
+    pp.cnt[3] = odd_periodic(L) ? (unsigned)((rall - rin2) * ((L.nx + 1) / 2) + (sx ? 2 * rin2 : 0)) : 0u;
+    pp.blk0[0] = 0;
+    for (int q = 0; q < 4; q++) pp.blk0[q + 1] = pp.blk0[q] + nblk(pp.cnt[q]);
+}
+
 // colour passes and the outer residual: interior groups (no boundary code)
 // and the shell as two parts of a launch (measured at 257^3: FP32 colour
 // pass 54.6 against 58.3 us, FP64 91 against 126 us, outer residual 156
@@ -969,41 +1010,10 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     Box pb{};
     auto prolong_bulk = [&](auto wc) {
         constexpr int W = decltype(wc)::value;
-        const long long G = (L.nh + W - 1) / W;  // groups holding a cell (the rest of the P / W are pads)
-        const long long rall = (long long)L.ny * L.nz;
-        const long long rin = (long long)(pb.hi[1] - pb.lo[1] + 1) * (pb.hi[2] - pb.lo[2] + 1);
-        ProlongDiv dv;
-        dv.g.init((unsigned)G);
-        dv.yin.init((unsigned)(pb.hi[1] - pb.lo[1] + 1));
-        dv.yin2.init((unsigned)(pb.hi[1] - pb.lo[1] + 1) / 2);
-        dv.nh.init((unsigned)((L.nx + 1) / 2));
-        // groups with every cell in the box for both row parities: 2Wg >= lo,
-        // 2W(g+1) - 1 <= hi
-        dv.g_lo = (pb.lo[0] + 2 * W - 1) / (2 * W);
-        dv.g_hi = (pb.hi[0] + 1) / (2 * W) - 1;
-        const long long gin = dv.g_hi >= dv.g_lo ? dv.g_hi - dv.g_lo + 1 : 0;
-        if (gin == 0) { dv.g_lo = 0; dv.g_hi = -1; }
-        dv.gin.init((unsigned)std::max<long long>(gin, 1));
-        dv.gout.init((unsigned)std::max<long long>(G - gin, 1));
-        // red cells on odd periodic seams (read by the next red pass)
+        ProlongDiv dv, sv;
         Box sb;
-        const int sy = L.per[1] && (L.ny & 1), sz = L.per[2] && (L.nz & 1), sx = L.per[0] && (L.nx & 1);
-        sb.lo[0] = 0;
-        sb.hi[0] = L.nx - 1;
-        sb.lo[1] = sy;
-        sb.hi[1] = L.ny - 1 - sy;
-        sb.lo[2] = sz;
-        sb.hi[2] = L.nz - 1 - sz;
-        const long long rin2 = (long long)(sb.hi[1] - sb.lo[1] + 1) * (sb.hi[2] - sb.lo[2] + 1);
-        ProlongDiv sv = dv;
-        sv.yin.init((unsigned)(sb.hi[1] - sb.lo[1] + 1));
         ProlongParts pp;
-        pp.cnt[0] = (unsigned)(rin / 4 * gin);  // 2 x 2 row blocks
-        pp.cnt[1] = (unsigned)(rin * (G - gin));
-        pp.cnt[2] = (unsigned)((rall - rin) * G);
-        pp.cnt[3] = odd_periodic(L) ? (unsigned)((rall - rin2) * ((L.nx + 1) / 2) + (sx ? 2 * rin2 : 0)) : 0u;
-        pp.blk0[0] = 0;
-        for (int q = 0; q < 4; q++) pp.blk0[q + 1] = pp.blk0[q] + nblk(pp.cnt[q]);
+        prolong_form(L, pb, W, dv, sb, sv, pp);
         pdl_launch(k_prolong_v<T, W>, pp.blk0[4], TPB, 0, ctx.s, L, cur(H, L, l), C, ccur(H, C, l + 1), ctx.xf[l],
                    pb, dv, sb, sv, pp);
     };
