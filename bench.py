@@ -316,6 +316,33 @@ def vcycle_bytes(levels_cells, s, coeff_field, nu=4):
     return tot
 
 
+def geom_level_cells(nx, ny, nz):
+    """Cells per level of the geometric hierarchy (l/2 per direction, stop
+    at <= 125 cells)."""
+    lev, d = [], [nx, ny, nz]
+    while True:
+        lev.append(d[0] * d[1] * d[2])
+        if lev[-1] <= 125:
+            return lev
+        d = [max(1, q // 2) for q in d]
+
+
+def batch_bytes(probs, infos, s):
+    """Algorithmic bytes of a batch of constant-coefficient solves: each
+    problem's V-cycles (vcycle_bytes with words of s bytes) plus, per outer
+    iteration and once before the first, the FP64 residual (read x and b,
+    write r as s) and, per outer iteration, the FP64 update (read e, read and
+    write x)."""
+    tot = 0.0
+    for p, i in zip(probs, infos):
+        n = p.lx * p.ly * p.lz
+        it = i["iters"]
+        vc = i.get("vcycles") or 2 * it
+        tot += vc * vcycle_bytes(geom_level_cells(p.lx, p.ly, p.lz), s, 0)
+        tot += (it + 1) * (16 + s) * n + it * (16 + s) * n
+    return tot
+
+
 def timed_solves(dp, xg, h, steps, ws, init=None, **kw):
     """ms per solve (CUDA events on the solving stream, max over ranks) and the last info."""
     import torch
@@ -393,7 +420,7 @@ def bench_sg_step(args, ws, h, phi_fine, dev, deferred, check=False):
     (mixed) or FP64 V-cycle, to 1e-10 relative residual."""
     import torch
 
-    from mps3d_b200 import solver, workloads as W
+    from mps3d_b200 import capi, solver, workloads as W
 
     p3 = W.electron_sg_step(129, phi=W.inject_potential(phi_fine.cpu().numpy(), 129))
     dp3 = solver.DeviceProblem(p3, device=f"cuda:{dev}")
@@ -402,12 +429,29 @@ def bench_sg_step(args, ws, h, phi_fine, dev, deferred, check=False):
                        "periodic x/y, ZGRD z; potential = 257^3 plasma Poisson solution injected",
            "unit": "solves/s", "tol_rel_residual": 1e-10}
     sols = {}
+    hbm_peak, _ = load_peaks()
+    cells = p3.lx * p3.ly * p3.lz
     for prec in ("mixed", "fp64"):
         ms, info = timed_solves(dp3, x3, h, args.steps, ws, precision=prec, krylov="fgmres", restart=30,
                                 tol=1e-10, maxit=60)
         out[prec] = {"value": ws * 1e3 / ms, "ms_per_solve": ms, "iters": info["iters"],
                      "rel_res": info["rel_res"]}
         sols[prec] = x3.cpu().numpy()
+        # the finest-level colour pass of the preconditioner, live CUDA-event
+        # times of one more solve: explicit rows (7 coefficients of the
+        # colour's cells), the other colour, f, the write -- 5 words per cell
+        # pair of word size s
+        h.set_profile(True)
+        h.get_profile(reset=True)
+        timed_solves(dp3, x3, h, 1, ws, precision=prec, krylov="fgmres", restart=30, tol=1e-10, maxit=60)
+        pr = h.get_profile(reset=True)
+        h.set_profile(False)
+        if pr.count[capi.PROF_SMOOTH] > 0:
+            s_b = 4 if prec == "mixed" else 8
+            us = 1e3 * pr.ms[capi.PROF_SMOOTH] / pr.count[capi.PROF_SMOOTH]
+            gbs = 5.0 * s_b * cells / (us * 1e-6) / 1e9
+            out[prec]["colour_pass"] = {"us": us, "per_solve": pr.count[capi.PROF_SMOOTH], "bytes": 5.0 * s_b * cells,
+                                        "gbs": gbs, "frac": gbs / hbm_peak}
 
     def later():
         if check:
@@ -483,6 +527,11 @@ def bench_batch(args, ws, rank, h, dev, deferred):
             out[name] = {"value": 64 * 1e3 / ms, "ms_per_batch": ms,
                          "max_rel_res": max(i["rel_res"] for i in every),
                          "iters": sorted({i["iters"] for i in every})}
+            if name.startswith("batched"):
+                # algorithmic bytes of all 64 solves over the batch's time
+                gbs = batch_bytes(allp, every, 4 if prec == "mixed" else 8) / (ms * 1e-3) / 1e9
+                hbm_peak, _ = load_peaks()
+                out[name].update({"hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak})
         if check:
             sols[name] = [xx.cpu().numpy() for xx in xs]
     if rank == 0:
@@ -699,13 +748,7 @@ def run_ours(args, ws, rank, local):
     value = ws * 1e3 / per_mixed
     fp64_value = ws * 1e3 / per_fp64
 
-    # level cell counts of the geometric hierarchy (l/2 per direction, stop at <=125)
-    lev, d = [], [n, n, n]
-    while True:
-        lev.append(d[0] * d[1] * d[2])
-        if lev[-1] <= 125:
-            break
-        d = [max(1, q // 2) for q in d]
+    lev = geom_level_cells(n, n, n)
 
     hbm_peak, peak_kind = load_peaks()
     # roofline of the dominant kernel: finest-level colour pass, mixed solve

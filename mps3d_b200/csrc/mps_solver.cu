@@ -1688,6 +1688,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
             bool done = false;
             for (j = 0; j < m && it < o->maxit; j++) {
                 double* vj = ctx.V + (size_t)j * n;
+                GraphEntry* pg = nullptr;  // the preconditioner's graph replayed this iteration
                 // z_j = M^{-1} v_j (one V-cycle from zero), then w = A z_j in FP64
                 if (mixed) {
                     Hier<float>& P = ctx.h32;
@@ -1695,8 +1696,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                     CKL();
                     if (graphs) {
                         gk.kind = 3;
-                        GraphEntry* G = nullptr;
-                        if ((st = run_graph(ctx, gk, &G, [&]() { return vcycle(ctx, P, sig.opclass, o, true); })))
+                        if ((st = run_graph(ctx, gk, &pg, [&]() { return vcycle(ctx, P, sig.opclass, o, true); })))
                             return st;
                     } else if ((st = vcycle(ctx, P, sig.opclass, o, true))) {
                         return st;
@@ -1717,8 +1717,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                     CK(cudaMemcpyAsync(P.F[0], vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx.s));
                     if (graphs) {
                         gk.kind = 4;
-                        GraphEntry* G = nullptr;
-                        if ((st = run_graph(ctx, gk, &G, [&]() { return vcycle(ctx, P, sig.opclass, o, true); })))
+                        if ((st = run_graph(ctx, gk, &pg, [&]() { return vcycle(ctx, P, sig.opclass, o, true); })))
                             return st;
                     } else if ((st = vcycle(ctx, P, sig.opclass, o, true))) {
                         return st;
@@ -1756,6 +1755,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 CK(cudaMemcpyAsync(ctx.hpin + 256, ctx.hcol + m + 2, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost,
                                    ctx.s));
                 CK(cudaStreamSynchronize(ctx.s));
+                if (pg) prof_collect_graph(ctx, *pg);
                 for (int i = 0; i <= j; i++) HH(i, j) = ctx.hpin[i] + ctx.hpin[256 + i];
                 double hn = std::sqrt(std::max(ctx.hpin[j + 1], 0.0));
                 if (!(hn <= 1e308)) { inf.status = MPS_ERR_NAN; done = true; break; }
