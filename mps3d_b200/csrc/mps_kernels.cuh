@@ -1331,6 +1331,113 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
     colour_split_block<T, W, U, UNI>(L, op, c, u, out, f, cs, blockIdx.x);
 }
 
+// ---------------------------------------------------------------------
+// Colour pass of the explicit-row operator (ROp: Scharfetter-Gummel and
+// convection rows) in two parts of one launch, as k_colourv_split: the
+// interior groups (all six neighbours inside the grid, of the other colour)
+// with W cells of a row per thread -- the colour's seven row arrays and the
+// other colour's neighbour rows as vectors, the x neighbours from the row's
+// own vector plus one scalar -- and the shell cells one at a time through
+// the general row evaluation.  The faces are summed in row_eval's order
+// (x-, x+, y-, y+, z-, z+), so results equal those of k_colour.
+// ---------------------------------------------------------------------
+template <class T, int W, class U>
+__device__ __forceinline__ void rop_group(const Lev& L, const ROp<T>& op, int c, const U& u, int row, int h0,
+                                          int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
+{
+    const int oc = c ^ 1;
+    const T* uo = u.ptr(oc);
+    const int sy = L.P, sz = L.P * L.ny;
+    auto ldu = [&](int o) { return uo ? ldv<T, W>(uo + o) : zerov<T, W>(); };
+    const VecW<T, W> ax = ldu(o0);
+    const int so = q ? o0 + W : o0 - 1;
+    const T sx = uo ? __ldg(uo + so) : T(0);
+    const VecW<T, W> uym = ldu(o0 - sy), uyp = ldu(o0 + sy), uzm = ldu(o0 - sz), uzp = ldu(o0 + sz);
+    VecW<T, W> r[7];
+#pragma unroll
+    for (int f = 0; f < 7; f++) r[f] = ldv<T, W>(sel(op.r[f], c) + o0);
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        T uxm, uxp;
+        if (q) {
+            uxm = ax.v[e];
+            uxp = e < W - 1 ? ax.v[e + 1] : sx;
+        } else {
+            uxm = e > 0 ? ax.v[e - 1] : sx;
+            uxp = ax.v[e];
+        }
+        T acc = T(0);
+        acc += r[1].v[e] * uxm;
+        acc += r[2].v[e] * uxp;
+        acc += r[3].v[e] * uym.v[e];
+        acc += r[4].v[e] * uyp.v[e];
+        acc += r[5].v[e] * uzm.v[e];
+        acc += r[6].v[e] * uzp.v[e];
+        diag.v[e] = r[0].v[e];
+        off.v[e] = acc;
+    }
+}
+
+template <class T, int W, class U>
+__global__ void __launch_bounds__(TPB) k_colourv_split_rop(Lev L, ROp<T> op, int c, U u, T* __restrict__ out,
+                                                           const T* __restrict__ f, ColourSplit cs)
+{
+    pdl_wait();
+    int part;
+    unsigned idx;
+    split_chunk(cs.nb_in, cs.nb_xe, blockIdx.x, part, idx);
+    const unsigned t = idx * TPB + threadIdx.x;
+    int j, k, g;
+    if (part == 0) {
+        if (t >= cs.n_in) return;
+        const unsigned r = cs.gin.div(t);
+        g = cs.g_lo + (int)(t - r * cs.gin.d);
+        const unsigned kk = cs.yin.div(r);
+        k = 1 + (int)kk;
+        j = 1 + (int)(r - kk * cs.yin.d);
+        const int h0 = W * g;
+        const int row = j + L.ny * k;
+        const int q = (j + k + c) & 1;
+        const int o0 = h0 + L.P * row;
+        const VecW<T, W> f4 = ldv<T, W>(f + o0);
+        VecW<T, W> diag, off;
+        rop_group<T, W, U>(L, op, c, u, row, h0, q, o0, diag, off);
+        VecW<T, W> res;
+#pragma unroll
+        for (int e = 0; e < W; e++) res.v[e] = gs_value(f4.v[e], diag.v[e], off.v[e]);
+        stv<T, W>(out + o0, res);
+        return;
+    }
+    if (part == 1) {
+        if (t >= cs.n_xe) return;
+        const unsigned r = cs.gx.div(t);
+        const unsigned e = t - r * cs.gx.d;
+        g = e < (unsigned)cs.g_lo ? (int)e : cs.g_hi + 1 + (int)(e - cs.g_lo);
+        const unsigned kk = cs.yin.div(r);
+        k = 1 + (int)kk;
+        j = 1 + (int)(r - kk * cs.yin.d);
+    } else {
+        if (t >= cs.n_face) return;
+        const unsigned r = cs.g.div(t);
+        g = (int)(t - r * cs.g.d);
+        shell_row(r, L.ny, cs.b, j, k);
+    }
+    // the shell: each cell of the group through the general row evaluation
+    const int q = (j + k + c) & 1;
+    const int o0 = W * g + L.P * (j + L.ny * k);
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int i = 2 * (W * g + e) + q;
+        T v = T(0);
+        if (i < L.nx) {
+            T diag, off;
+            row_any<T>(op, L, u, i, j, k, diag, off);
+            v = gs_value(__ldg(&f[o0 + e]), diag, off);
+        }
+        out[o0 + e] = v;
+    }
+}
+
 // Residual r = f - A u of both colours on a uniform level (the outer
 // residual of a solve), the interior groups without boundary code and the
 // shell apart, grid-stride over each part; r optionally stored as R, the
