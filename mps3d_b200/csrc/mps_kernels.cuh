@@ -700,11 +700,53 @@ __device__ __forceinline__ void shell_row(unsigned r, int ny, const Box& b, int&
     j = (int)(r - kk * uny);
 }
 
+// W cells of one row of colour c of the explicit-row operator whose six
+// neighbours are inside the grid and of the other colour: the colour's seven
+// row arrays and the other colour's neighbour rows as vectors, the x
+// neighbours from the row's own vector plus one scalar; faces summed in
+// row_eval's order (x-, x+, y-, y+, z-, z+)
+template <class T, int W, class U>
+__device__ __forceinline__ void rop_group(const Lev& L, const ROp<T>& op, int c, const U& u, int row, int h0,
+                                          int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
+{
+    const int oc = c ^ 1;
+    const T* uo = u.ptr(oc);
+    const int sy = L.P, sz = L.P * L.ny;
+    auto ldu = [&](int o) { return uo ? ldv<T, W>(uo + o) : zerov<T, W>(); };
+    const VecW<T, W> ax = ldu(o0);
+    const int so = q ? o0 + W : o0 - 1;
+    const T sx = uo ? __ldg(uo + so) : T(0);
+    const VecW<T, W> uym = ldu(o0 - sy), uyp = ldu(o0 + sy), uzm = ldu(o0 - sz), uzp = ldu(o0 + sz);
+    VecW<T, W> r[7];
+#pragma unroll
+    for (int f = 0; f < 7; f++) r[f] = ldv<T, W>(sel(op.r[f], c) + o0);
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        T uxm, uxp;
+        if (q) {
+            uxm = ax.v[e];
+            uxp = e < W - 1 ? ax.v[e + 1] : sx;
+        } else {
+            uxm = e > 0 ? ax.v[e - 1] : sx;
+            uxp = ax.v[e];
+        }
+        T acc = T(0);
+        acc += r[1].v[e] * uxm;
+        acc += r[2].v[e] * uxp;
+        acc += r[3].v[e] * uym.v[e];
+        acc += r[4].v[e] * uyp.v[e];
+        acc += r[5].v[e] * uzm.v[e];
+        acc += r[6].v[e] * uzp.v[e];
+        diag.v[e] = r[0].v[e];
+        off.v[e] = acc;
+    }
+}
+
 // the W coarse cells I = h0 .. h0+W-1 of coarse row (J, K) from their four
 // red fine rows; IN: every fine cell involved has its neighbours inside the
 // grid and regular faces (no boundary code)
-template <class T, int W, bool UNI, bool IN>
-__device__ __forceinline__ void restrict_cells(const Lev& F, const KOp<T>& op, const CSplit<T>& u,
+template <class T, int W, bool UNI, bool IN, class Op = KOp<T>>
+__device__ __forceinline__ void restrict_cells(const Lev& F, const Op& op, const CSplit<T>& u,
                                                const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
                                                const Box& bx, int J, int K, int h0)
 {
@@ -718,7 +760,19 @@ __device__ __forceinline__ void restrict_cells(const Lev& F, const KOp<T>& op, c
             const int q = (j + k) & 1;
             const int o0 = h0 + F.P * row;
             VecW<T, W> diag, off;
-            group_rows<T, W, CSplit<T>, UNI, IN>(F, op, 0, u, row, j, k, h0, q, o0, diag, off);
+            if constexpr (std::is_same<Op, KOp<T>>::value) {
+                group_rows<T, W, CSplit<T>, UNI, IN>(F, op, 0, u, row, j, k, h0, q, o0, diag, off);
+            } else if constexpr (IN) {
+                rop_group<T, W, CSplit<T>>(F, op, 0, u, row, h0, q, o0, diag, off);
+            } else {  // explicit rows near the boundary: cell by cell
+#pragma unroll
+                for (int e = 0; e < W; e++) {
+                    const int i = 2 * (h0 + e) + q;
+                    diag.v[e] = T(0);
+                    off.v[e] = T(0);
+                    if (i < F.nx) row_any<T>(op, F, u, i, j, k, diag.v[e], off.v[e]);
+                }
+            }
             const VecW<T, W> f4 = ldv<T, W>(fred + o0);
             const VecW<T, W> u4 = ldv<T, W>(u.c[0] + o0);
 #pragma unroll
@@ -771,8 +825,8 @@ struct RestrictSplit {
     Box rect;         // the interior coarse rows (y/z bounds)
 };
 
-template <class T, int W, bool UNI>
-__device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& op, const CSplit<T>& u,
+template <class T, int W, bool UNI, class Op = KOp<T>>
+__device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const Op& op, const CSplit<T>& u,
                                                     const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
                                                     const Box& bx, const RestrictSplit& rs, unsigned blk)
 {
@@ -785,7 +839,7 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& 
         const unsigned r = rs.gin.div(t);
         const int g = rs.ga + (int)(t - r * rs.gin.d);
         const unsigned kk = rs.yin.div(r);
-        restrict_cells<T, W, true, true>(F, op, u, fred, C, fc, bx, rs.J0 + (int)(r - kk * rs.yin.d),
+        restrict_cells<T, W, true, true, Op>(F, op, u, fred, C, fc, bx, rs.J0 + (int)(r - kk * rs.yin.d),
                                          rs.K0 + (int)kk, W * g);
         return;
     }
@@ -808,7 +862,7 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const KOp<T>& 
     if (J < bx.lo[1] || J > bx.hi[1] || K < bx.lo[2] || K > bx.hi[2]) return;
     const int h0 = W * g;
     if (h0 > bx.hi[0] || h0 + W - 1 < bx.lo[0]) return;
-    restrict_cells<T, W, UNI, false>(F, op, u, fred, C, fc, bx, J, K, h0);
+    restrict_cells<T, W, UNI, false, Op>(F, op, u, fred, C, fc, bx, J, K, h0);
 }
 
 // the t-th cell of an n[0] x n[1] x n[2] grid outside box b: z slabs first,
@@ -873,8 +927,8 @@ __device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op,
 // bulk and shell in one launch: blocks [0, nb_bulk) take the bulk rows,
 // the rest the shell cells
 // UNI: the fine level is uniform
-template <class T, int W, int MB, bool UNI>
-__global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, KOp<T> op, CSplit<T> u,
+template <class T, int W, int MB, bool UNI, class Op = KOp<T>>
+__global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, Op op, CSplit<T> u,
                                                                                  const T* __restrict__ fred, Lev C,
                                                                                  Split<T> fc, RestrictSplit rs, Box bx,
                                                                                  unsigned nb_bulk, int geom,
@@ -882,12 +936,12 @@ __global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, KOp<T> op, 
 {
     pdl_wait();
     if (blockIdx.x < nb_bulk) {
-        resid_restrict_bulk<T, W, UNI>(F, op, u, fred, C, fc, bx, rs, blockIdx.x);
+        resid_restrict_bulk<T, W, UNI, Op>(F, op, u, fred, C, fc, bx, rs, blockIdx.x);
     } else {
         CSplit<T> f;
         f.c[0] = fred;
         f.c[1] = fred + F.half;
-        resid_restrict_shell<T, KOp<T>>(F, op, u, f, C, fc, geom, bx, shell,
+        resid_restrict_shell<T, Op>(F, op, u, f, C, fc, geom, bx, shell,
                                         (blockIdx.x - nb_bulk) * TPB + threadIdx.x);
     }
 }
@@ -1341,43 +1395,6 @@ __global__ void __launch_bounds__(TPB, MB) k_colourv_split(Lev L, KOp<T> op, int
 // the general row evaluation.  The faces are summed in row_eval's order
 // (x-, x+, y-, y+, z-, z+), so results equal those of k_colour.
 // ---------------------------------------------------------------------
-template <class T, int W, class U>
-__device__ __forceinline__ void rop_group(const Lev& L, const ROp<T>& op, int c, const U& u, int row, int h0,
-                                          int q, int o0, VecW<T, W>& diag, VecW<T, W>& off)
-{
-    const int oc = c ^ 1;
-    const T* uo = u.ptr(oc);
-    const int sy = L.P, sz = L.P * L.ny;
-    auto ldu = [&](int o) { return uo ? ldv<T, W>(uo + o) : zerov<T, W>(); };
-    const VecW<T, W> ax = ldu(o0);
-    const int so = q ? o0 + W : o0 - 1;
-    const T sx = uo ? __ldg(uo + so) : T(0);
-    const VecW<T, W> uym = ldu(o0 - sy), uyp = ldu(o0 + sy), uzm = ldu(o0 - sz), uzp = ldu(o0 + sz);
-    VecW<T, W> r[7];
-#pragma unroll
-    for (int f = 0; f < 7; f++) r[f] = ldv<T, W>(sel(op.r[f], c) + o0);
-#pragma unroll
-    for (int e = 0; e < W; e++) {
-        T uxm, uxp;
-        if (q) {
-            uxm = ax.v[e];
-            uxp = e < W - 1 ? ax.v[e + 1] : sx;
-        } else {
-            uxm = e > 0 ? ax.v[e - 1] : sx;
-            uxp = ax.v[e];
-        }
-        T acc = T(0);
-        acc += r[1].v[e] * uxm;
-        acc += r[2].v[e] * uxp;
-        acc += r[3].v[e] * uym.v[e];
-        acc += r[4].v[e] * uyp.v[e];
-        acc += r[5].v[e] * uzm.v[e];
-        acc += r[6].v[e] * uzp.v[e];
-        diag.v[e] = r[0].v[e];
-        off.v[e] = acc;
-    }
-}
-
 template <class T, int W, class U>
 __global__ void __launch_bounds__(TPB) k_colourv_split_rop(Lev L, ROp<T> op, int c, U u, T* __restrict__ out,
                                                            const T* __restrict__ f, ColourSplit cs)

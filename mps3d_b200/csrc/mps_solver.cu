@@ -1008,7 +1008,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     }
     if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_RESTRICT);
     bool done = false;
-    if constexpr (std::is_same<Op, KOp<T>>::value) {
+    {
         Box bx;
         if (o->nu1 >= 1 && L.nx >= 16 && restrict_box(L, C, bx)) {
             // red residual of the bulk's children restricted in registers, the
@@ -1020,13 +1020,17 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
                 const unsigned nbb = rs.nb_in + rs.nb_xe + rs.nb_out;
                 const unsigned nbs = shell > 0 ? nblk(8 * shell) : 0;
                 if (L.uniform)
-                    pdl_launch(k_resid_restrict_v<T, W, MB, true>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l),
-                               H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
+                    pdl_launch(k_resid_restrict_v<T, W, MB, true, Op>, nbb + nbs, TPB, 0, ctx.s, L, ops[l],
+                               ccur(H, L, l), H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom,
+                               (unsigned)shell);
                 else
-                    pdl_launch(k_resid_restrict_v<T, W, MB, false>, nbb + nbs, TPB, 0, ctx.s, L, ops[l], ccur(H, L, l),
-                               H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom, (unsigned)shell);
+                    pdl_launch(k_resid_restrict_v<T, W, MB, false, Op>, nbb + nbs, TPB, 0, ctx.s, L, ops[l],
+                               ccur(H, L, l), H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom,
+                               (unsigned)shell);
             };
-            if (l == 0)
+            if constexpr (!std::is_same<Op, KOp<T>>::value)  // explicit rows: one coarse cell per thread
+                launch(std::integral_constant<int, 1>(), std::integral_constant<int, RestrictShape<T>::MINB>());
+            else if (l == 0)
                 launch(std::integral_constant<int, RestrictShape<T>::W>(), std::integral_constant<int, RestrictShape<T>::MINB>());
             else if (l == 1)
                 launch(std::integral_constant<int, CoarseXferShape<T>::W>(), std::integral_constant<int, CoarseXferShape<T>::MINB>());
