@@ -1463,8 +1463,8 @@ __global__ void __launch_bounds__(TPB) k_colourv_split_rop(Lev L, ROp<T> op, int
 // split_chunk) of the split residual of both colours on a uniform level:
 // r = f - A u stored as R when rout is set, the sums of r^2 and f^2 added to
 // rr and ff
-template <class T, int W, class R>
-__device__ __forceinline__ void resid_split_chunk(const Lev& L, const KOp<T>& op, const CSplit<T>& u,
+template <class T, int W, class R, class Op = KOp<T>>
+__device__ __forceinline__ void resid_split_chunk(const Lev& L, const Op& op, const CSplit<T>& u,
                                                   const T* __restrict__ f, R* __restrict__ rout,
                                                   const ColourSplit& cs, unsigned ch, double& rr, double& ff)
 {
@@ -1476,7 +1476,19 @@ __device__ __forceinline__ void resid_split_chunk(const Lev& L, const KOp<T>& op
         for (int cc = 0; cc <= 1; cc++) {
             const int q = (j + k + cc) & 1;
             VecW<T, W> diag, off;
-            group_rows<T, W, CSplit<T>, true, IN>(L, op, cc, u, row, j, k, h0, q, o0, diag, off);
+            if constexpr (std::is_same<Op, KOp<T>>::value) {
+                group_rows<T, W, CSplit<T>, true, IN>(L, op, cc, u, row, j, k, h0, q, o0, diag, off);
+            } else if constexpr (IN) {
+                rop_group<T, W, CSplit<T>>(L, op, cc, u, row, h0, q, o0, diag, off);
+            } else {  // explicit rows near the boundary: cell by cell
+#pragma unroll
+                for (int e = 0; e < W; e++) {
+                    const int i = 2 * (h0 + e) + q;
+                    diag.v[e] = T(0);
+                    off.v[e] = T(0);
+                    if (i < L.nx) row_any<T>(op, L, u, i, j, k, diag.v[e], off.v[e]);
+                }
+            }
             const VecW<T, W> f4 = ldv<T, W>(f + (cc ? L.half : 0) + o0);
             const VecW<T, W> u4 = ldv<T, W>(u.half(cc) + o0);
             VecW<R, W> r4;
@@ -1523,8 +1535,8 @@ __device__ __forceinline__ void resid_split_chunk(const Lev& L, const KOp<T>& op
     group(j, k, g, std::false_type());
 }
 
-template <class T, int W, class R>
-__global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L, KOp<T> op, CSplit<T> u,
+template <class T, int W, class R, class Op = KOp<T>>
+__global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L, Op op, CSplit<T> u,
                                                                            const T* __restrict__ f,
                                                                            R* __restrict__ rout, RedBuf rb,
                                                                            ColourSplit cs)
@@ -1535,7 +1547,7 @@ __global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L
     // block-sized chunks, grid-stride, in the interleaved order of split_chunk
     const unsigned nchunks = cs.nb_in + cs.nb_xe + cs.nb_face;
     for (unsigned ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
-        resid_split_chunk<T, W, R>(L, op, u, f, rout, cs, ch, rr, ff);
+        resid_split_chunk<T, W, R, Op>(L, op, u, f, rout, cs, ch, rr, ff);
     const double a = block_sum(rr, sh);
     const double b = block_sum(ff, sh);
     if (!rb.partial) return;

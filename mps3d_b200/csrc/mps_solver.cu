@@ -1127,6 +1127,18 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             prof_end(ctx);
             return 0;
         }
+    } else {
+        // explicit rows: interior cells without boundary code, the shell cell by cell
+        ColourSplit cs;
+        if (MPS_RESID_SPLIT && L.uniform && L.nx >= 16 && make_split(L, 1, cs)) {
+            const unsigned nbv = std::min<unsigned>(cs.nb_in + cs.nb_xe + cs.nb_face,
+                                                    (unsigned)(ctx.nsm * ResidShape<T>::MINB));
+            pdl_launch(k_residv_split<T, 1, R, Op>, nbv, TPB, 0, ctx.s, L, op, u, f.half(0),
+                       rout.c[0] ? rout.half(0) : nullptr, ctx.rb, cs);
+            CKL();
+            prof_end(ctx);
+            return 0;
+        }
     }
     pdl_launch(k_resid_norm<T, Op, R>, nblk((long long)L.P * L.rows), TPB, 0, ctx.s, L, op, u, f, rout, ctx.rb);
     prof_end(ctx);
