@@ -876,7 +876,7 @@ def run_ours(args, ws, rank, local):
         "hbm_gbs_solve": gbs_m,
         "hbm_frac_solve": gbs_m / hbm_peak,
         "fp64_hbm_frac_solve": gbs_d / hbm_peak,
-        "roofline": {"bound": "hbm", "kernel": "finest-level red/black pass, FP32, mixed solve: k_colour_tma<float,4,8> "
+        "roofline": {"bound": "hbm", "kernel": "finest-level red/black pass, FP32, mixed solve: k_colour_tma<float,4,6> "
                                                "(TMA-staged rows; the 84 passes per solve from a valid state) and "
                                                "k_colourv_split<float,4> (the 28 from a zero state), averaged",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,

@@ -704,11 +704,14 @@ static RestrictSplit make_restrict_split(const Lev& F, const Lev& C, const Box& 
 #ifndef MPS_TMA_LEVELS
 #define MPS_TMA_LEVELS 1  // the finest level only
 #endif
+// tile rows and blocks per SM of the FP32 pass, measured on the 257^3 mixed
+// solve (ms): 6 rows at 3 blocks per SM 12.72-12.75, 8 rows at 2 blocks
+// 12.79-12.81, 5 rows at 4 blocks 13.40, 7 rows at 3 blocks 13.78
 #ifndef MPS_TMA_BPS
-#define MPS_TMA_BPS 2  // blocks per SM the tiling aims at
+#define MPS_TMA_BPS 3  // blocks per SM the tiling aims at
 #endif
 #ifndef MPS_TMA_TJ32
-#define MPS_TMA_TJ32 8
+#define MPS_TMA_TJ32 6
 #endif
 #ifndef MPS_TMA_TJ64
 #define MPS_TMA_TJ64 4
