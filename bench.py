@@ -877,8 +877,9 @@ def run_ours(args, ws, rank, local):
         "hbm_frac_solve": gbs_m / hbm_peak,
         "fp64_hbm_frac_solve": gbs_d / hbm_peak,
         "roofline": {"bound": "hbm", "kernel": "finest-level red/black pass, FP32, mixed solve: k_colour_tma<float,4,6> "
-                                               "(TMA-staged rows; the 84 passes per solve from a valid state) and "
-                                               "k_colourv_split<float,4> (the 28 from a zero state), averaged",
+                                               "(TMA-staged rows; the passes from a valid state) and "
+                                               "k_colourv_split<float,4> (the black pass after each outer residual, "
+                                               "which writes the red pass from zero itself), averaged",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "peak_kind": peak_kind, "traffic": traffic, "bytes_per_launch": cp_bytes,
                      "launch_ms": cp_ms, "fp64_achieved": achieved64, "fp64_frac": achieved64 / hbm_peak},

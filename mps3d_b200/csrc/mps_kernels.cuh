@@ -1463,10 +1463,14 @@ __global__ void __launch_bounds__(TPB) k_colourv_split_rop(Lev L, ROp<T> op, int
 // split_chunk) of the split residual of both colours on a uniform level:
 // r = f - A u stored as R when rout is set, the sums of r^2 and f^2 added to
 // rr and ff
+// ured (when set): the first red pass of a V-cycle from a zero state on the
+// residual as right-hand side, ured = r / diag on the red cells (the diagonal
+// of this operator, rounded to R), which the V-cycle then skips
 template <class T, int W, class R, class Op = KOp<T>>
 __device__ __forceinline__ void resid_split_chunk(const Lev& L, const Op& op, const CSplit<T>& u,
                                                   const T* __restrict__ f, R* __restrict__ rout,
-                                                  const ColourSplit& cs, unsigned ch, double& rr, double& ff)
+                                                  const ColourSplit& cs, unsigned ch, double& rr, double& ff,
+                                                  R* __restrict__ ured = nullptr)
 {
     auto group = [&](int j, int k, int g, auto in) {
         constexpr bool IN = decltype(in)::value;
@@ -1491,18 +1495,20 @@ __device__ __forceinline__ void resid_split_chunk(const Lev& L, const Op& op, co
             }
             const VecW<T, W> f4 = ldv<T, W>(f + (cc ? L.half : 0) + o0);
             const VecW<T, W> u4 = ldv<T, W>(u.half(cc) + o0);
-            VecW<R, W> r4;
+            VecW<R, W> r4, z4;
 #pragma unroll
             for (int e = 0; e < W; e++) {
                 const T r = f4.v[e] - (diag.v[e] * u4.v[e] + off.v[e]);
                 const bool ok = IN || 2 * (h0 + e) + q < L.nx;
                 r4.v[e] = ok ? (R)r : R(0);
+                z4.v[e] = ok ? gs_value(r4.v[e], (R)diag.v[e], R(0)) : R(0);
                 if (ok) {
                     rr += (double)r * (double)r;
                     ff += (double)f4.v[e] * (double)f4.v[e];
                 }
             }
             if (rout) stv<R, W>(rout + (cc ? L.half : 0) + o0, r4);
+            if (ured && cc == 0) stv<R, W>(ured + o0, z4);
         }
     };
     int part;
@@ -1539,7 +1545,7 @@ template <class T, int W, class R, class Op = KOp<T>>
 __global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L, Op op, CSplit<T> u,
                                                                            const T* __restrict__ f,
                                                                            R* __restrict__ rout, RedBuf rb,
-                                                                           ColourSplit cs)
+                                                                           ColourSplit cs, R* __restrict__ ured)
 {
     pdl_wait();
     __shared__ double sh[32];
@@ -1547,7 +1553,7 @@ __global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv_split(Lev L
     // block-sized chunks, grid-stride, in the interleaved order of split_chunk
     const unsigned nchunks = cs.nb_in + cs.nb_xe + cs.nb_face;
     for (unsigned ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
-        resid_split_chunk<T, W, R, Op>(L, op, u, f, rout, cs, ch, rr, ff);
+        resid_split_chunk<T, W, R, Op>(L, op, u, f, rout, cs, ch, rr, ff, ured);
     const double a = block_sum(rr, sh);
     const double b = block_sum(ff, sh);
     if (!rb.partial) return;

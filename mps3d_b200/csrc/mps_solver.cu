@@ -214,6 +214,7 @@ struct Ctx {
     std::vector<Lane> lanes;  // created at the first host call with pageable arrays
     bool tma_ok = false;      // the shared-memory colour pass can run (set at workspace set-up)
     bool tma_allowed = true;  // MPS_TMA=0 at handle creation: the register-fed kernels only (for comparisons)
+    bool red0_ready = false;  // the finest level's first red pass from zero was written by the outer residual
     size_t inbuf_bytes = 0;
     Signature sig;
     int nlev = 0;
@@ -1001,7 +1002,12 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     int st;
     for (int s = 0; s < o->nu1; s++) {
         bool z = zero_guess && s == 0;
-        if ((st = colour_pass(ctx, H, ops[l], l, 0, z ? 2 : 0))) return st;
+        if (z && l == 0 && ctx.red0_ready) {
+            // the red pass from zero (red = f / diag) came with the outer residual
+            H.ri[l] ^= 1;
+        } else if ((st = colour_pass(ctx, H, ops[l], l, 0, z ? 2 : 0))) {
+            return st;
+        }
         if ((st = colour_pass(ctx, H, ops[l], l, 1, z ? 1 : 0))) return st;
     }
     if (o->nu1 == 0 && zero_guess) {
@@ -1098,10 +1104,15 @@ static int vcycle(Ctx& ctx, Hier<T>& H, int opclass, const mps_solver_opts* o, b
     return vcycle_rec(ctx, H, H.rop, 0, o, zero_guess);
 }
 
-// r = f - A u, sums (r.r, f.f) -> ctx.rb.out; optional r written to rout (type R)
+// r = f - A u, sums (r.r, f.f) -> ctx.rb.out; optional r written to rout (type R);
+// ured (optional): the red half that a V-cycle's first red pass from a zero
+// state on rout would write (r / diag); *ured_done tells whether it was
+// written (the split kernel only)
 template <class T, class Op, class R>
-static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R> rout)
+static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R> rout, R* ured = nullptr,
+                      bool* ured_done = nullptr)
 {
+    if (ured_done) *ured_done = false;
     const Lev& L = ctx.lev[0];
     prof_begin(ctx, MPS_PROF_RESID);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
@@ -1117,10 +1128,12 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             const unsigned nbv = std::min<unsigned>(nall, (unsigned)(ctx.nsm * ResidShape<T>::MINB));
             ColourSplit cs;
             if (MPS_RESID_SPLIT && make_split(L, W, cs)) {  // interior without boundary code, the shell apart
+                R* ur = rout.c[0] ? ured : nullptr;
                 pdl_launch(k_residv_split<T, W, R>, nbv, TPB, 0, ctx.s, L, op, u, f.half(0),
-                           rout.c[0] ? rout.half(0) : nullptr, ctx.rb, cs);
+                           rout.c[0] ? rout.half(0) : nullptr, ctx.rb, cs, ur);
                 CKL();
                 prof_end(ctx);
+                if (ured_done) *ured_done = ur != nullptr;
                 return 0;
             }
             // both colours in one pass (f and rout as split bases, halves L.half apart)
@@ -1137,7 +1150,7 @@ static int resid_norm(Ctx& ctx, const Op& op, CSplit<T> u, CSplit<T> f, Split<R>
             const unsigned nbv = std::min<unsigned>(cs.nb_in + cs.nb_xe + cs.nb_face,
                                                     (unsigned)(ctx.nsm * ResidShape<T>::MINB));
             pdl_launch(k_residv_split<T, 1, R, Op>, nbv, TPB, 0, ctx.s, L, op, u, f.half(0),
-                       rout.c[0] ? rout.half(0) : nullptr, ctx.rb, cs);
+                       rout.c[0] ? rout.half(0) : nullptr, ctx.rb, cs, (R*)nullptr);
             CKL();
             prof_end(ctx);
             return 0;
@@ -1669,16 +1682,27 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         const int inner = o->inner_cycles > 0 ? o->inner_cycles : 2;
         for (int l = 0; l < nl; l++) H.ri[l] = H.bi[l] = 0;
         gk.inner = inner;
+        // the residual also writes the first V-cycle's red pass from zero on the
+        // finest level (r / diag) where its split kernel runs; the V-cycle then
+        // skips that pass
+        bool red_ready = false;
         auto residual = [&]() -> int {
             Split<float> r32 = split<float>(H.F[0], L);
+            float* ured = o->nu1 >= 1 ? H.U[0][H.ri[0] ^ 1] : nullptr;
             if (sig.opclass == 0)
-                return resid_norm(ctx, ctx.kop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
-            return resid_norm(ctx, ctx.rop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32);
+                return resid_norm(ctx, ctx.kop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32, ured,
+                                  &red_ready);
+            return resid_norm(ctx, ctx.rop64, csplit<double>(ctx.x64, L), csplit<double>(ctx.b64, L), r32, ured,
+                              &red_ready);
         };
         auto iteration = [&]() -> int {
             int s2;
-            for (int c = 0; c < inner; c++)
-                if ((s2 = vcycle(ctx, H, sig.opclass, o, c == 0))) return s2;
+            for (int c = 0; c < inner; c++) {
+                ctx.red0_ready = c == 0 && red_ready;
+                s2 = vcycle(ctx, H, sig.opclass, o, c == 0);
+                ctx.red0_ready = false;
+                if (s2) return s2;
+            }
             const unsigned ab = std::min<unsigned>(nblk(L.half), 4736);
             pdl_launch(k_axpy<float, double>, ab, TPB, 0, ctx.s, L.half, 1.0, H.U[0][H.ri[0]], ctx.x64);
             CKL();
