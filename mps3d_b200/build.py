@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libmps3d_b200.so")
 SOURCES = ["mps_solver.cu", "mps_kernels.cu", "mps_noalloc.cu", "mps_adjoint.cu", "mps_step.cu", "mps_vtk.cu"]
-HEADERS = ["mps_core.cuh", "mps_kernels.cuh", "mps_batch.cuh", "mps_tma.cuh", os.path.join("..", "..", "include", "mps_linsolve.h")]
+HEADERS = ["mps_core.cuh", "mps_kernels.cuh", "mps_batch.cuh", "mps_tma.cuh", "mps_subcycle.cuh", os.path.join("..", "..", "include", "mps_linsolve.h")]
 
 ARCH_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -50,6 +50,7 @@ static_assert(offsetof(mps_problem, timederiv) == 40 && offsetof(mps_problem, dt
               "mps_problem layout");
 #include "mps_kernels.cuh"
 #include "mps_tma.cuh"
+#include "mps_subcycle.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -141,6 +142,9 @@ struct Hier {
     KOp<T> kop[MAXL];
     ROp<T> rop[MAXL];
     double* AinvT = nullptr;
+    unsigned char* subimg = nullptr;  // solve-constant image of the one-block sub-cycle (k_sub_image)
+    size_t subimg_bytes = 0;
+    bool sub_ok = false;              // the image is current: the V-cycle may run k_subcycle
     double* Dprev = nullptr;  // the coarsest matrix whose inverse AinvT holds
     int* gj = nullptr;        // its inversion state (k_gauss_jordan)
 };
@@ -215,6 +219,8 @@ struct Ctx {
     bool tma_ok = false;      // the shared-memory colour pass can run (set at workspace set-up)
     bool tma_allowed = true;  // MPS_TMA=0 at handle creation: the register-fed kernels only (for comparisons)
     bool red0_ready = false;  // the finest level's first red pass from zero was written by the outer residual
+    bool sub_allowed = true;  // MPS_SUBCYCLE=0 at handle creation: one launch per pass on every level (for comparisons)
+    int sub_l0 = -1;          // first level of the one-block sub-cycle (k_subcycle), -1: none
     size_t inbuf_bytes = 0;
     Signature sig;
     int nlev = 0;
@@ -993,10 +999,277 @@ static int coarse_solve(Ctx& ctx, Hier<T>& H, int l)
     return 0;
 }
 
+// ---- the small levels in one block (k_subcycle) ----
+// the shared-memory limit of the sub-cycle kernels, set outside any stream
+// capture (at workspace set-up)
+static bool sub_prepare()
+{
+    static int ready = -1;
+    if (ready >= 0) return ready == 1;
+    auto set = [](const void* kern) {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SUB_SMEM_MAX) == cudaSuccess;
+    };
+    const bool ok = set((const void*)k_subcycle<float, false, false>) && set((const void*)k_subcycle<float, true, false>) &&
+                    set((const void*)k_subcycle<float, false, true>) && set((const void*)k_subcycle<float, true, true>) &&
+                    set((const void*)k_subcycle<double, false, false>) && set((const void*)k_subcycle<double, true, false>) &&
+                    set((const void*)k_subcycle<double, false, true>) && set((const void*)k_subcycle<double, true, true>);
+    if (!ok) cudaGetLastError();
+    ready = ok ? 1 : 0;
+    return ok;
+}
+
+// first level of the one-block sub-cycle, or -1: the geometric hierarchy, a
+// level below the finest with at most SUB_MAX_CELLS cells and at most
+// SUB_MAXL levels from it to the coarsest (two at least), and no odd periodic
+// size on those levels (cells of one colour would touch, and in-place passes
+// would read new values)
+static int sub_first_level(const Ctx& ctx, const mps_solver_opts* o)
+{
+    if (o->hierarchy != MPS_HIER_GEOM) return -1;
+    const int nl = ctx.nlev;
+    int l0 = -1;
+    for (int l = 1; l < nl - 1; l++) {
+        const Lev& L = ctx.lev[l];
+        if ((long long)L.nx * L.ny * L.nz <= SUB_MAX_CELLS && nl - l <= SUB_MAXL) { l0 = l; break; }
+    }
+    if (l0 < 0) return -1;
+    for (int l = l0; l < nl; l++) {
+        if (odd_periodic(ctx.lev[l])) return -1;
+        if (l < nl - 1 && !ctx.xf[l].geom) return -1;
+    }
+    return l0;
+}
+
+// one level of the block's plan: Lev's sizes, widths and boundary flags
+template <class T>
+static SubGeo<T> sub_geo(const Lev& L)
+{
+    SubGeo<T> G;
+    std::memset(&G, 0, sizeof(G));
+    G.nx = L.nx; G.ny = L.ny; G.nz = L.nz; G.nh = L.nh;
+    G.rows = L.ny * L.nz;
+    G.rc = SUB_TPB / L.nh;
+    G.rn = SUB_TPB / L.nx;
+    G.gx = L.nx + 2;
+    G.gy = L.ny + 2;
+    G.pitch = L.P;
+    for (int a = 0; a < 3; a++) {
+        G.per |= L.per[a] ? 1 << a : 0;
+        G.w[a] = (T)L.w[a];
+        G.wl[a] = (T)L.wl[a];
+    }
+    for (int f = 0; f < 6; f++) G.dirc |= L.bc[f] == BC_DIRC && !L.per[f / 2] ? 1 << f : 0;
+    G.dnh.init((unsigned)L.nh);
+    G.dny.init((unsigned)L.ny);
+    G.dnx.init((unsigned)L.nx);
+    return G;
+}
+
+// the axis entries of one level (ghosted strides 1, nx+2, (nx+2)(ny+2)): the
+// face coefficients of fcoef / dcoef by position, periodic faces wrapping
+template <class T>
+static void sub_axes(const Lev& L, SubAx<T>* out)
+{
+    const int n3[3] = {L.nx, L.ny, L.nz};
+    const int st3[3] = {1, L.nx + 2, (L.nx + 2) * (L.ny + 2)};
+    int e = 0;
+    for (int a = 0; a < 3; a++) {
+        const int n = n3[a], st = st3[a];
+        const bool per = L.per[a] != 0;
+        const bool dm = !per && L.bc[2 * a] == BC_DIRC, dp = !per && L.bc[2 * a + 1] == BC_DIRC;
+        for (int p = 0; p < n; p++, e++) {
+            SubAx<T> x;
+            if (p > 0) { x.om = -st; x.cm = (T)(p == n - 1 ? L.cl[a] : L.cr[a]); }
+            else if (per) { x.om = (n - 1) * st; x.cm = (T)(n == 1 ? L.cl[a] : L.cp[a]); }
+            else { x.om = -st; x.cm = dm ? (T)(n == 1 ? L.dlast[a] : L.dr[a]) : T(0); }
+            if (p < n - 1) { x.op = st; x.cp = (T)(p + 1 == n - 1 ? L.cp[a] : L.cr[a]); }
+            else if (per) { x.op = -(n - 1) * st; x.cp = (T)L.cl[a]; }
+            else { x.op = st; x.cp = dp ? (T)L.dlast[a] : T(0); }
+            out[e] = x;
+        }
+    }
+}
+
+// the block's plan from level l0 for word type T: shared-memory layout
+// (dynamic fields, the solve-constant image, tables), per-level geometry,
+// axis entries and prolongation brackets.  false when it does not fit.
+template <class T>
+static bool sub_layout_with(const Ctx& ctx, int l0, bool kf, bool df, const mps_solver_opts* o, SubPlan<T>& P,
+                            size_t& smem, bool ainv_in_smem);
+
+// the layout with the coarsest inverse staged in shared memory when that fits,
+// else read from device memory by the coarsest solve
+template <class T>
+static bool sub_layout(const Ctx& ctx, int l0, bool kf, bool df, const mps_solver_opts* o, SubPlan<T>& P,
+                       size_t& smem)
+{
+    return sub_layout_with<T>(ctx, l0, kf, df, o, P, smem, true) ||
+           sub_layout_with<T>(ctx, l0, kf, df, o, P, smem, false);
+}
+
+template <class T>
+static bool sub_layout_with(const Ctx& ctx, int l0, bool kf, bool df, const mps_solver_opts* o, SubPlan<T>& P,
+                            size_t& smem, bool ainv_in_smem)
+{
+    std::memset(&P, 0, sizeof(P));
+    if (l0 < 1 || ctx.nlev - l0 < 2) return false;
+    const int nl = ctx.nlev - l0;
+    P.nl = nl;
+    P.nu1 = o->nu1;
+    P.nu2 = o->nu2;
+    P.only_black = o->nu2 >= 1;
+    int nax = 0, nrow = 0, nlin = 0;
+    long long off = 0;  // elements of T: u (ghosted) and f of every level
+    for (int s = 0; s < nl; s++) {
+        const Lev& L = ctx.lev[l0 + s];
+        // a row per thread at least in every loop; the tables' capacities
+        if (L.nx > SUB_TPB || nax + L.nx + L.ny + L.nz > SUB_MAX_AX || nrow + L.ny * L.nz > SUB_MAX_ROWS)
+            return false;
+        P.geo[s] = sub_geo<T>(L);
+        P.geo[s].ax0 = nax;
+        P.geo[s].row0 = nrow;
+        sub_axes<T>(L, P.ax + nax);
+        nax += L.nx + L.ny + L.nz;
+        nrow += L.ny * L.nz;
+        P.ou[s] = (int)off; off += (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+        P.of[s] = (int)off; off += (long long)L.nx * L.ny * L.nz;
+        if (s < nl - 1) {
+            const Xfer& X = ctx.xf[l0 + s];
+            const int nf[3] = {L.nx, L.ny, L.nz};
+            for (int a = 0; a < 3; a++) {
+                P.lin0[s][a] = nlin;
+                for (int i = 0; i < nf[a]; i++) {
+                    Lin e;
+                    geom_lin(X, a, i, e.j0, e.j1, e.t);
+                    P.lin[nlin + i].j0 = e.j0;
+                    P.lin[nlin + i].j1 = e.j1;
+                    P.lin[nlin + i].t = (T)e.t;
+                }
+                nlin += nf[a];
+            }
+            // lanes per coarse cell: up to 8, while the coarse cells fill the
+            // block and a coarse row fits one trip
+            const Lev& C = ctx.lev[l0 + s + 1];
+            const long long nc = (long long)C.nx * C.ny * C.nz;
+            int lg = 3;
+            while (lg > 0 && (nc << lg > SUB_TPB || (C.nx << lg) > SUB_TPB)) lg--;
+            P.rlog[s] = lg;
+            P.rrows[s] = (SUB_TPB >> lg) / C.nx;
+        }
+    }
+    // the solve-constant image: coefficients (ghosted), diagonal extras, inverse
+    off = (off + 1) & ~1LL;  // 16-byte boundary for either word size
+    off = ((off * (long long)sizeof(T) + 15) & ~15LL) / (long long)sizeof(T);
+    P.img_off = (int)(off * sizeof(T));
+    for (int s = 0; s < nl; s++) {
+        const Lev& L = ctx.lev[l0 + s];
+        P.ok[s] = kf ? (int)off : -1; off += kf ? (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) : 0;
+        P.od[s] = df ? (int)off : -1; off += df ? (long long)L.nx * L.ny * L.nz : 0;
+    }
+    size_t bytes = ((size_t)off * sizeof(T) + 15) & ~(size_t)15;
+    const Lev& Cc = ctx.lev[ctx.nlev - 1];
+    const long long ncs = (long long)Cc.nx * Cc.ny * Cc.nz;
+    P.ainv_off = ainv_in_smem ? (int)bytes : -1;
+    if (ainv_in_smem) bytes += ((size_t)(ncs * ncs) * sizeof(double) + 15) & ~(size_t)15;
+    P.img_bytes = (int)(bytes - P.img_off);
+    P.lin_off = (int)bytes;
+    bytes += ((size_t)nlin * sizeof(SubLin<T>) + 15) & ~(size_t)15;
+    P.ax_off = (int)bytes;
+    bytes += ((size_t)nax * sizeof(SubAx<T>) + 15) & ~(size_t)15;
+    P.row_off = (int)bytes;
+    bytes += (size_t)nrow * sizeof(SubRow);
+    P.nlin = nlin;
+    P.nax = nax;
+    P.nrow = nrow;
+    int g = 32;
+    while (g > 1 && ncs * g > SUB_TPB) g >>= 1;
+    P.gsz = g;
+    smem = bytes;
+    return bytes <= (size_t)SUB_SMEM_MAX;
+}
+
+static cudaError_t sub_launch(const void* kern, size_t smem, cudaStream_t s, void** args)
+{
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(SUB_TPB);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, kern, args);
+}
+
+// build the solve-constant image of hierarchy H (after its coefficient
+// pyramid and coarsest inverse are set up); H.sub_ok tells the V-cycle
+template <class T>
+static int sub_image(Ctx& ctx, Hier<T>& H, const KOp<T>* ops, const mps_solver_opts* o)
+{
+    H.sub_ok = false;
+    const int l0 = ctx.sub_l0;
+    if (l0 < 1 || !H.subimg) return 0;
+    const bool kf = ops[l0].k[0] != nullptr, df = ops[l0].dex[0] != nullptr;
+    std::unique_ptr<SubPlan<T>> pp(new SubPlan<T>);
+    SubPlan<T>& P = *pp;
+    size_t smem = 0;
+    if (!sub_layout<T>(ctx, l0, kf, df, o, P, smem) || (size_t)P.img_bytes > H.subimg_bytes) return 0;
+    for (int s = 0; s < P.nl; s++)
+        for (int c = 0; c < 2; c++) {
+            P.k[s][c] = ops[l0 + s].k[c];
+            P.dex[s][c] = ops[l0 + s].dex[c];
+        }
+    const Lev& Cc = ctx.lev[ctx.nlev - 1];
+    int ncs = Cc.nx * Cc.ny * Cc.nz;
+    unsigned char* img = H.subimg;
+    const double* ainv = H.AinvT;
+    void* args[] = {(void*)&P, (void*)&img, (void*)&ainv, (void*)&ncs};
+    const void* kern = kf ? (df ? (const void*)k_sub_image<T, true, true> : (const void*)k_sub_image<T, true, false>)
+                          : (df ? (const void*)k_sub_image<T, false, true> : (const void*)k_sub_image<T, false, false>);
+    sub_launch(kern, 0, ctx.s, args);
+    CKL();
+    H.sub_ok = true;
+    return 0;
+}
+
+// the V-cycle from level l0 (zero guess) to the coarsest and back in one
+// launch; -1 when it does not apply (the per-level launches run instead)
+template <class T>
+static int subcycle(Ctx& ctx, Hier<T>& H, const KOp<T>* ops, int l0, const mps_solver_opts* o)
+{
+    if (!H.sub_ok || l0 != ctx.sub_l0) return -1;
+    const bool kf = ops[l0].k[0] != nullptr, df = ops[l0].dex[0] != nullptr;
+    std::unique_ptr<SubPlan<T>> pp(new SubPlan<T>);  // the kernel parameter (copied at launch)
+    SubPlan<T>& P = *pp;
+    size_t smem = 0;
+    if (!sub_layout<T>(ctx, l0, kf, df, o, P, smem)) return -1;
+    P.kc = ops[l0].kc;
+    P.dexc = ops[l0].dexc;
+    CSplit<T> fin = csplit<T>(H.F[l0], ctx.lev[l0]);
+    Split<T> uout = cur(H, ctx.lev[l0], l0);
+    const uint4* img = reinterpret_cast<const uint4*>(H.subimg);
+    const double* ainv = H.AinvT;
+    void* args[] = {(void*)&P, (void*)&fin, (void*)&uout, (void*)&img, (void*)&ainv};
+    const void* kern = kf ? (df ? (const void*)k_subcycle<T, true, true> : (const void*)k_subcycle<T, true, false>)
+                          : (df ? (const void*)k_subcycle<T, false, true> : (const void*)k_subcycle<T, false, false>);
+    sub_launch(kern, smem, ctx.s, args);
+    CKL();
+    return 0;
+}
+
 template <class T, class Op>
 static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solver_opts* o, bool zero_guess)
 {
     if (l == ctx.nlev - 1) return coarse_solve(ctx, H, l);
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (zero_guess && l == ctx.sub_l0) {
+            const int st = subcycle(ctx, H, ops, l, o);
+            if (st >= 0) return st;
+        }
+    }
     const Lev& L = ctx.lev[l];
     const Lev& C = ctx.lev[l + 1];
     int st;
@@ -1255,6 +1528,28 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
     ctx.rb.out = (double*)ctx.ar.get(sizeof(double) * 4);
     ok = ok && ctx.x64 && ctx.b64 && ctx.dense && ctx.gjM && ctx.dstatus && ctx.rb.partial && ctx.rb.counter &&
          ctx.rb.out;
+    // the one-block sub-cycle of the small levels: its first level and the
+    // solve-constant images of both hierarchies
+    ctx.sub_l0 = sig.opclass == 0 && ctx.sub_allowed && sub_prepare() ? sub_first_level(ctx, o) : -1;
+    ctx.h64.subimg = nullptr;
+    ctx.h32.subimg = nullptr;
+    ctx.h64.subimg_bytes = ctx.h32.subimg_bytes = 0;
+    ctx.h64.sub_ok = ctx.h32.sub_ok = false;
+    if (ctx.sub_l0 > 0) {
+        std::unique_ptr<SubPlan<double>> p64(new SubPlan<double>);
+        std::unique_ptr<SubPlan<float>> p32(new SubPlan<float>);
+        size_t sm = 0;
+        if (need64 && sub_layout<double>(ctx, ctx.sub_l0, !sig.kuni, sig.has_reac != 0, o, *p64, sm)) {
+            ctx.h64.subimg_bytes = (size_t)p64->img_bytes;
+            ctx.h64.subimg = (unsigned char*)ctx.ar.get(ctx.h64.subimg_bytes);
+            ok = ok && ctx.h64.subimg;
+        }
+        if (need32 && sub_layout<float>(ctx, ctx.sub_l0, !sig.kuni, sig.has_reac != 0, o, *p32, sm)) {
+            ctx.h32.subimg_bytes = (size_t)p32->img_bytes;
+            ctx.h32.subimg = (unsigned char*)ctx.ar.get(ctx.h32.subimg_bytes);
+            ok = ok && ctx.h32.subimg;
+        }
+    }
     if (!ok) {
         ctx.ar.clear();
         ctx.err.code = MPS_ERR_NOMEM;
@@ -1597,6 +1892,11 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         else st = coarse_inverse(ctx, ctx.h32, ctx.h32.rop[nl - 1]);
     }
     if (st) return st;
+    if (sig.opclass == 0) {  // the one-block sub-cycle's solve-constant image
+        if (need64) st = sub_image(ctx, ctx.h64, ctx.h64.kop, o);
+        else st = sub_image(ctx, ctx.h32, ctx.h32.kop, o);
+        if (st) return st;
+    }
     if (prepare_only) {
         inf.levels = nl;
         if (info) *info = inf;
@@ -1972,6 +2272,9 @@ int mps_create(mps_handle* h, int device)
     // the shared-memory (TMA) kernels and the register-fed ones give the same
     // results; the variable selects the register-fed ones (for comparisons)
     if (const char* tv = std::getenv("MPS_TMA")) ctx.tma_allowed = std::atoi(tv) != 0;
+    // the one-block sub-cycle of the small levels and the per-level launches
+    // solve the same systems; the variable selects the per-level launches
+    if (const char* sv = std::getenv("MPS_SUBCYCLE")) ctx.sub_allowed = std::atoi(sv) != 0;
     if (cudaDeviceGetAttribute(&ctx.nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || ctx.nsm < 1) {
         delete H;
         return MPS_ERR_CUDA;
