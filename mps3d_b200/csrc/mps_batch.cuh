@@ -509,6 +509,16 @@ struct BatchState {
     std::vector<long long> tune_key;
     std::vector<int> tune_grid;
     std::vector<int> tune_vec;
+    // operator detection of every problem (9 words each), read back at once
+    unsigned long long* ddet = nullptr;
+    unsigned long long* hdet = nullptr;  // page-locked
+    int det_cap = 0;
+    // streams of the per-problem set-ups (independent: they overlap on the
+    // device), joined to the handle's stream before the iterations
+    static constexpr int NSET = 8;
+    cudaStream_t set_s[NSET] = {};
+    cudaEvent_t set_e[NSET] = {};
+    cudaEvent_t start_e = nullptr;
 };
 
 static int sub_init(Ctx& parent, Ctx& sc)
@@ -564,6 +574,13 @@ static void destroy_batch(Ctx& ctx)
     cudaFree(B.dncell);
     cudaFree(B.dcounter);
     cudaFree(B.dloops);
+    if (B.ddet) cudaFree(B.ddet);
+    if (B.hdet) cudaFreeHost(B.hdet);
+    for (int i = 0; i < BatchState::NSET; i++) {
+        if (B.set_s[i]) cudaStreamDestroy(B.set_s[i]);
+        if (B.set_e[i]) cudaEventDestroy(B.set_e[i]);
+    }
+    if (B.start_e) cudaEventDestroy(B.start_e);
     delete ctx.batch;
     ctx.batch = nullptr;
 }
@@ -994,8 +1011,58 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     }
     CK(cudaEventRecord(ctx.e0, ctx.s));
     const long long launches0 = ctx.launches;
+    // operator detection of every problem, then one device->host read (each
+    // problem's set-up below then needs no synchronisation of its own);
+    // problems whose arguments solve_impl will refuse are not scanned
+    if (np > B.det_cap) {
+        if (B.ddet) cudaFree(B.ddet);
+        if (B.hdet) cudaFreeHost(B.hdet);
+        B.ddet = nullptr;
+        B.hdet = nullptr;
+        B.det_cap = 0;
+        if (cudaMalloc((void**)&B.ddet, sizeof(unsigned long long) * 9 * np) != cudaSuccess ||
+            cudaMallocHost((void**)&B.hdet, sizeof(unsigned long long) * 9 * np) != cudaSuccess) {
+            ctx.err.msg = "batched: detection buffers";
+            return MPS_ERR_NOMEM;
+        }
+        B.det_cap = np;
+    }
+    std::vector<char> scanned(np, 0);
+    CK(cudaMemsetAsync(B.ddet, 0, sizeof(unsigned long long) * 9 * np, ctx.s));
+    for (int p = 0; p < np; p++) {
+        const mps_problem& q = probs[p];
+        const mps_grid& g = q.g;
+        if (g.lx < 1 || g.ly < 1 || g.lz < 1 || !q.dcoeff || !q.source || !q.soln ||
+            (long long)g.lx * g.ly * g.lz >= (1LL << 31) / 2)
+            continue;
+        bool bcok = true;
+        for (int f = 0; f < 6; f++) bcok = bcok && q.bc_code[f] >= 1 && q.bc_code[f] <= 5;
+        if (!bcok) continue;
+        const double llen[3] = {1.0, 1.0, 1.0};  // the scan reads sizes only
+        const Lev L = make_lev_uniform(g.lx, g.ly, g.lz, llen, q.bc_code);
+        const long long ncell = (long long)g.lx * g.ly * g.lz;
+        pdl_launch(k_maxabs_all, std::min<unsigned>(nblk(ncell), 1184), TPB, 0, ctx.s, L, q.vel, q.reac, q.dcoeff,
+                   q.source, q.soln, B.ddet + 9 * p);
+        CKL();
+        CK(cudaMemcpyAsync(B.ddet + 9 * p + 8, q.dcoeff + 1 + (g.lx + 2) * (1 + (long long)(g.ly + 2)),
+                           sizeof(double), cudaMemcpyDeviceToDevice, ctx.s));
+        scanned[p] = 1;
+    }
+    CK(cudaMemcpyAsync(B.hdet, B.ddet, sizeof(unsigned long long) * 9 * np, cudaMemcpyDeviceToHost, ctx.s));
+    CK(cudaStreamSynchronize(ctx.s));
+    if (!B.start_e) {
+        for (int i = 0; i < BatchState::NSET; i++) {
+            CK(cudaStreamCreateWithFlags(&B.set_s[i], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&B.set_e[i], cudaEventDisableTiming));
+        }
+        CK(cudaEventCreateWithFlags(&B.start_e, cudaEventDisableTiming));
+    }
+    CK(cudaEventRecord(B.start_e, ctx.s));
+    const int nset = std::min(np, (int)BatchState::NSET);
+    for (int i = 0; i < nset; i++) CK(cudaStreamWaitEvent(B.set_s[i], B.start_e, 0));
     for (int p = 0; p < np; p++) {
         Ctx& sc = *B.sub[p];
+        sc.s = B.set_s[p % nset];
         const mps_problem& q = probs[p];
         Inputs in;
         in.vel = q.vel;
@@ -1007,7 +1074,8 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
         in.soln = q.soln;
         mps_solve_info inf;
         sc.launches = 0;
-        int st = solve_impl(sc, &q.g, q.timederiv, q.dt, in, q.bc_code, o, &inf, 0, 1);
+        int st = solve_impl(sc, &q.g, q.timederiv, q.dt, in, q.bc_code, o, &inf, 0, 1,
+                            scanned[p] ? B.hdet + 9 * p : nullptr);
         ctx.launches += sc.launches;
         if (st) {
             ctx.err.msg = "batched problem " + std::to_string(p) + ": " + sc.err.msg;
@@ -1020,6 +1088,11 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
             return MPS_ERR_BAD_ARG;
         }
     }
+    for (int i = 0; i < nset; i++) {
+        CK(cudaEventRecord(B.set_e[i], B.set_s[i]));
+        CK(cudaStreamWaitEvent(ctx.s, B.set_e[i], 0));
+    }
+    for (int p = 0; p < np; p++) B.sub[p]->s = ctx.s;
     // ---- plan, device tables ----
     BatchPlan<T> P;
     plan_batch<T>(B, P, o, inner);

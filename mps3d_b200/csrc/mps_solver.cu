@@ -1672,8 +1672,12 @@ static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
 // ----------------------------------------------------------------------
 // prepare_only: stop after the set-up (hierarchy, operators, right-hand side,
 // initial guess, coarsest inverse), for the batched driver
+// det (optional): the operator detection of these inputs already read back
+// (k_maxabs_all's eight words, then the coefficient of cell (1,1,1)); the
+// batched solve detects every problem with one device->host read
 static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, const Inputs& in, const int bc[6],
-                      const mps_solver_opts* o, mps_solve_info* info, int ref_norm_only, int prepare_only = 0)
+                      const mps_solver_opts* o, mps_solve_info* info, int ref_norm_only, int prepare_only = 0,
+                      const unsigned long long* det = nullptr)
 {
     mps_solve_info inf;
     std::memset(&inf, 0, sizeof(inf));
@@ -1723,15 +1727,22 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 }
                 pos += ctx.xf[l].nf[a];
             }
-        if (tab.size() > ctx.dtab_n) {
-            if (ctx.dtab) cudaFree(ctx.dtab);
-            ctx.dtab = nullptr;
-            ctx.dtab_n = 0;
-            CK(cudaMalloc((void**)&ctx.dtab, sizeof(Lin) * tab.size()));
-            ctx.dtab_n = tab.size();
+        // the device copy is kept while the tables do not change (a copy from
+        // pageable host memory would hold the host until the stream drains)
+        const bool same = ctx.dtab && tab.size() == ctx.htab.size() &&
+                          std::memcmp(tab.data(), ctx.htab.data(), sizeof(Lin) * tab.size()) == 0;
+        if (!same) {
+            if (tab.size() > ctx.dtab_n) {
+                if (ctx.dtab) cudaFree(ctx.dtab);
+                ctx.dtab = nullptr;
+                ctx.dtab_n = 0;
+                CK(cudaMalloc((void**)&ctx.dtab, sizeof(Lin) * tab.size()));
+                ctx.dtab_n = tab.size();
+            }
+            ctx.htab.swap(tab);
+            CK(cudaMemcpyAsync(ctx.dtab, ctx.htab.data(), sizeof(Lin) * ctx.htab.size(), cudaMemcpyHostToDevice,
+                               ctx.s));
         }
-        ctx.htab.swap(tab);
-        CK(cudaMemcpyAsync(ctx.dtab, ctx.htab.data(), sizeof(Lin) * ctx.htab.size(), cudaMemcpyHostToDevice, ctx.s));
         pos = 0;
         for (int l = 0; l + 1 < nl; l++)
             for (int a = 0; a < 3; a++) {
@@ -1745,18 +1756,23 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     CK(cudaEventRecord(ctx.e0, ctx.s));
     // ---- operator detection (one small device->host read) ----
     unsigned long long* dm = ctx.dmax;
-    CK(cudaMemsetAsync(dm, 0, sizeof(unsigned long long) * 8, ctx.s));
     const long long ncell = (long long)L0.nx * L0.ny * L0.nz;
     const long long ng = (long long)(L0.nx + 2) * (L0.ny + 2) * (L0.nz + 2);
-    const unsigned mb = std::min<unsigned>(nblk(ncell), 1184);
-    pdl_launch(k_maxabs_all, mb, TPB, 0, ctx.s, L0, in.vel, in.reac, in.dcoeff, in.source, in.soln, dm);
-    CKL();
     unsigned long long hm[8];
-    CK(cudaMemcpyAsync(hm, dm, sizeof(hm), cudaMemcpyDeviceToHost, ctx.s));
     double k0 = 0.0;
-    CK(cudaMemcpyAsync(&k0, in.dcoeff + 1 + (L0.nx + 2) * (1 + (long long)(L0.ny + 2)), sizeof(double),
-                       cudaMemcpyDeviceToHost, ctx.s));
-    CK(cudaStreamSynchronize(ctx.s));
+    if (det) {
+        std::memcpy(hm, det, sizeof(hm));
+        std::memcpy(&k0, det + 8, sizeof(double));
+    } else {
+        CK(cudaMemsetAsync(dm, 0, sizeof(unsigned long long) * 8, ctx.s));
+        const unsigned mb = std::min<unsigned>(nblk(ncell), 1184);
+        pdl_launch(k_maxabs_all, mb, TPB, 0, ctx.s, L0, in.vel, in.reac, in.dcoeff, in.source, in.soln, dm);
+        CKL();
+        CK(cudaMemcpyAsync(hm, dm, sizeof(hm), cudaMemcpyDeviceToHost, ctx.s));
+        CK(cudaMemcpyAsync(&k0, in.dcoeff + 1 + (L0.nx + 2) * (1 + (long long)(L0.ny + 2)), sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx.s));
+        CK(cudaStreamSynchronize(ctx.s));
+    }
     auto asd = [](unsigned long long b) { double d; std::memcpy(&d, &b, 8); return d; };
     const double maxvel = asd(hm[0]), maxreac = asd(hm[1]), dkvar = asd(hm[2]), maxsrc = asd(hm[3]),
                  maxsol = asd(hm[4]), maxk = asd(hm[5]);
@@ -1892,7 +1908,7 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         else st = coarse_inverse(ctx, ctx.h32, ctx.h32.rop[nl - 1]);
     }
     if (st) return st;
-    if (sig.opclass == 0) {  // the one-block sub-cycle's solve-constant image
+    if (sig.opclass == 0 && !prepare_only) {  // the one-block sub-cycle's solve-constant image
         if (need64) st = sub_image(ctx, ctx.h64, ctx.h64.kop, o);
         else st = sub_image(ctx, ctx.h32, ctx.h32.kop, o);
         if (st) return st;
