@@ -33,6 +33,13 @@ struct BState {
     double rel, rms, rel0;
 };
 
+// every problem active, no iteration done (the start of a batched solve)
+__global__ void kb_reset_state(BState* st, int np)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np) st[p] = BState{1, 0, MPS_OK, 0, 0.0, 0.0, 0.0};
+}
+
 enum BKind { B_COLOUR = 0, B_RESTRICT, B_COARSE, B_PROLONG, B_OUTER, B_AXPY };
 
 template <class T>
@@ -515,6 +522,11 @@ struct BatchState {
     int det_cap = 0;
     // streams of the per-problem set-ups (independent: they overlap on the
     // device), joined to the handle's stream before the iterations
+    // the tables last uploaded (a repeated batch skips the uploads: copies
+    // from pageable host memory hold the host until the stream drains)
+    std::vector<unsigned char> up_desc;
+    std::vector<int> up_task;
+    std::vector<long long> up_cells;
     static constexpr int NSET = 8;
     cudaStream_t set_s[NSET] = {};
     cudaEvent_t set_e[NSET] = {};
@@ -1099,6 +1111,9 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     auto grow = [&](auto*& ptr, size_t& cap, size_t n, size_t elem) -> int {
         if (n <= cap) return 0;
         batch_release_graph(B);
+        B.up_desc.clear();
+        B.up_task.clear();
+        B.up_cells.clear();
         if (ptr) cudaFree(ptr);
         ptr = nullptr;
         cap = 0;
@@ -1131,17 +1146,21 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
         }
         CK(cudaMemsetAsync(B.dcounter, 0, sizeof(unsigned), ctx.s));
         B.cap_prob = np;
+        B.up_cells.clear();
     }
-    std::vector<BState> hs(np);
     std::vector<long long> hn(np);
-    for (int p = 0; p < np; p++) {
-        hs[p] = BState{1, 0, MPS_OK, 0, 0.0, 0.0, 0.0};
-        hn[p] = (long long)probs[p].g.lx * probs[p].g.ly * probs[p].g.lz;
+    for (int p = 0; p < np; p++) hn[p] = (long long)probs[p].g.lx * probs[p].g.ly * probs[p].g.lz;
+    if (P.desc != B.up_desc || P.task != B.up_task || hn != B.up_cells) {
+        CK(cudaMemcpyAsync(B.ddesc, P.desc.data(), P.desc.size(), cudaMemcpyHostToDevice, ctx.s));
+        CK(cudaMemcpyAsync(B.dtask, P.task.data(), sizeof(int) * P.task.size(), cudaMemcpyHostToDevice, ctx.s));
+        CK(cudaMemcpyAsync(B.dncell, hn.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx.s));
+        B.up_desc = P.desc;
+        B.up_task = P.task;
+        B.up_cells = hn;
     }
-    CK(cudaMemcpyAsync(B.ddesc, P.desc.data(), P.desc.size(), cudaMemcpyHostToDevice, ctx.s));
-    CK(cudaMemcpyAsync(B.dtask, P.task.data(), sizeof(int) * P.task.size(), cudaMemcpyHostToDevice, ctx.s));
-    CK(cudaMemcpyAsync(B.dst, hs.data(), sizeof(BState) * np, cudaMemcpyHostToDevice, ctx.s));
-    CK(cudaMemcpyAsync(B.dncell, hn.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx.s));
+    // every problem starts active (the state the loop's check kernel updates)
+    kb_reset_state<<<(np + TPB - 1) / TPB, TPB, 0, ctx.s>>>(B.dst, np);
+    CKL();
     CK(cudaMemsetAsync(B.dloops, 0, sizeof(int), ctx.s));
     const BState* active = B.dst;
     // ---- launch shapes ----
@@ -1219,6 +1238,7 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     CK(cudaGraphLaunch(B.exec, ctx.s));
     // ---- results ----
     int loops = 0;
+    std::vector<BState> hs(np);
     CK(cudaMemcpyAsync(hs.data(), B.dst, sizeof(BState) * np, cudaMemcpyDeviceToHost, ctx.s));
     CK(cudaMemcpyAsync(&loops, B.dloops, sizeof(int), cudaMemcpyDeviceToHost, ctx.s));
     for (int p = 0; p < np; p++) {

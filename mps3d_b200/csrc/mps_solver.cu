@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -83,6 +84,18 @@ static cudaError_t pdl_launch(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
+
+// a kernel attribute (the shared-memory limit) set once per device: the call
+// costs host time, and attributes belong to each device's context
+template <class F>
+static bool once_per_device(int dev, signed char* state, F&& set)
+{
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    if (dev < 0 || dev >= 64) return set();
+    if (state[dev] == 0) state[dev] = set() ? 1 : -1;
+    return state[dev] == 1;
+}
 
 struct Err {
     int code = 0;
@@ -828,25 +841,24 @@ static int colour_pass_tma(Ctx& ctx, Hier<T>& H, const KOp<T>& op, int l, int c,
 
 // the attributes the shared-memory colour pass needs, set outside any stream
 // capture (at workspace set-up); false when the device or driver cannot run it
-static bool tma_prepare()
+static bool tma_prepare(int dev)
 {
-    static int ready = -1;
-    if (ready >= 0) return ready == 1;
-    ready = 0;
+    static signed char state[64] = {};
     if (!MPS_TMA_COLOUR || !tensor_map_encoder()) return false;
-    const int bytes = 220 * 1024;
-    auto set = [&](auto kern) {
-        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
-    };
-    constexpr int W32 = TmaShape<float>::W, J32 = TmaShape<float>::TJ;
-    constexpr int W64 = TmaShape<double>::W, J64 = TmaShape<double>::TJ;
-    bool ok = set(k_colour_tma<float, W32, J32, true, true>) && set(k_colour_tma<float, W32, J32, false, true>) &&
-              set(k_colour_tma<float, W32, J32, true, false>) && set(k_colour_tma<float, W32, J32, false, false>) &&
-              set(k_colour_tma<double, W64, J64, true, true>) && set(k_colour_tma<double, W64, J64, false, true>) &&
-              set(k_colour_tma<double, W64, J64, true, false>) && set(k_colour_tma<double, W64, J64, false, false>);
-    if (!ok) cudaGetLastError();
-    ready = ok ? 1 : 0;
-    return ok;
+    return once_per_device(dev, state, [] {
+        const int bytes = 220 * 1024;
+        auto set = [&](auto kern) {
+            return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+        };
+        constexpr int W32 = TmaShape<float>::W, J32 = TmaShape<float>::TJ;
+        constexpr int W64 = TmaShape<double>::W, J64 = TmaShape<double>::TJ;
+        bool ok = set(k_colour_tma<float, W32, J32, true, true>) && set(k_colour_tma<float, W32, J32, false, true>) &&
+                  set(k_colour_tma<float, W32, J32, true, false>) && set(k_colour_tma<float, W32, J32, false, false>) &&
+                  set(k_colour_tma<double, W64, J64, true, true>) && set(k_colour_tma<double, W64, J64, false, true>) &&
+                  set(k_colour_tma<double, W64, J64, true, false>) && set(k_colour_tma<double, W64, J64, false, false>);
+        if (!ok) cudaGetLastError();
+        return ok;
+    });
 }
 
 // the explicit-row colour pass in two parts (k_colourv_split_rop); cells
@@ -1002,20 +1014,20 @@ static int coarse_solve(Ctx& ctx, Hier<T>& H, int l)
 // ---- the small levels in one block (k_subcycle) ----
 // the shared-memory limit of the sub-cycle kernels, set outside any stream
 // capture (at workspace set-up)
-static bool sub_prepare()
+static bool sub_prepare(int dev)
 {
-    static int ready = -1;
-    if (ready >= 0) return ready == 1;
-    auto set = [](const void* kern) {
-        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SUB_SMEM_MAX) == cudaSuccess;
-    };
-    const bool ok = set((const void*)k_subcycle<float, false, false>) && set((const void*)k_subcycle<float, true, false>) &&
-                    set((const void*)k_subcycle<float, false, true>) && set((const void*)k_subcycle<float, true, true>) &&
-                    set((const void*)k_subcycle<double, false, false>) && set((const void*)k_subcycle<double, true, false>) &&
-                    set((const void*)k_subcycle<double, false, true>) && set((const void*)k_subcycle<double, true, true>);
-    if (!ok) cudaGetLastError();
-    ready = ok ? 1 : 0;
-    return ok;
+    static signed char state[64] = {};
+    return once_per_device(dev, state, [] {
+        auto set = [](const void* kern) {
+            return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SUB_SMEM_MAX) == cudaSuccess;
+        };
+        const bool ok = set((const void*)k_subcycle<float, false, false>) && set((const void*)k_subcycle<float, true, false>) &&
+                        set((const void*)k_subcycle<float, false, true>) && set((const void*)k_subcycle<float, true, true>) &&
+                        set((const void*)k_subcycle<double, false, false>) && set((const void*)k_subcycle<double, true, false>) &&
+                        set((const void*)k_subcycle<double, false, true>) && set((const void*)k_subcycle<double, true, true>);
+        if (!ok) cudaGetLastError();
+        return ok;
+    });
 }
 
 // first level of the one-block sub-cycle, or -1: the geometric hierarchy, a
@@ -1530,7 +1542,7 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
          ctx.rb.out;
     // the one-block sub-cycle of the small levels: its first level and the
     // solve-constant images of both hierarchies
-    ctx.sub_l0 = sig.opclass == 0 && ctx.sub_allowed && sub_prepare() ? sub_first_level(ctx, o) : -1;
+    ctx.sub_l0 = sig.opclass == 0 && ctx.sub_allowed && sub_prepare(ctx.dev) ? sub_first_level(ctx, o) : -1;
     ctx.h64.subimg = nullptr;
     ctx.h32.subimg = nullptr;
     ctx.h64.subimg_bytes = ctx.h32.subimg_bytes = 0;
@@ -1559,7 +1571,7 @@ static int setup_workspace(Ctx& ctx, const Signature& sig, const mps_solver_opts
     // the arena zeroes new blocks with cudaMemset on the legacy stream; the
     // solver's stream does not synchronise with it, so wait here
     if (cudaDeviceSynchronize() != cudaSuccess) return MPS_ERR_CUDA;
-    ctx.tma_ok = ctx.tma_allowed && tma_prepare();
+    ctx.tma_ok = ctx.tma_allowed && tma_prepare(ctx.dev);
     ctx.sig = sig;
     return 0;
 }
@@ -1659,8 +1671,12 @@ static int coarse_inverse(Ctx& ctx, Hier<T>& H, const Op& op)
     pdl_launch(k_gj_prepare, nblk(2LL * n * n), TPB, 0, ctx.s, n, ctx.dense, ctx.gjM, (const int*)H.gj);
     CKL();
     const size_t smem = sizeof(double) * 2 * (size_t)n * n;
-    if (smem <= 200 * 1024) {
-        CK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    static signed char gj_state[64] = {};
+    const bool gj_smem = once_per_device(ctx.dev, gj_state, [] {
+        return cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+               cudaSuccess;
+    });
+    if (smem <= 200 * 1024 && gj_smem) {
         pdl_launch(k_gauss_jordan, 1, 1024, smem, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 1, H.gj);
     } else {
         pdl_launch(k_gauss_jordan, 1, 1024, 0, ctx.s, n, ctx.gjM, H.AinvT, ctx.dstatus, 0, H.gj);
@@ -1895,8 +1911,12 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
         pdl_launch(k_find_bvec, nblk(ncell), TPB, 0, ctx.s, L0, in.vel, in.dcoeff, in.source, bv[0], bv[1], bv[2], bv[3],
                                                     bv[4], bv[5], in.sterm, o->flux, split<double>(ctx.b64, L0));
         CKL();
-        pdl_launch(k_pack<double>, nblk(ncell), TPB, 0, ctx.s, L0, in.soln, split<double>(ctx.x64, L0), 1.0, 0.0);
-        CKL();
+        if (maxsol == 0.0) {  // a zero initial guess (every interior cell): clear instead of packing
+            CK(cudaMemsetAsync(ctx.x64, 0, sizeof(double) * 2 * L0.half, ctx.s));
+        } else {
+            pdl_launch(k_pack<double>, nblk(ncell), TPB, 0, ctx.s, L0, in.soln, split<double>(ctx.x64, L0), 1.0, 0.0);
+            CKL();
+        }
     }
     // ---- coarsest inverse ----
     CK(cudaMemsetAsync(ctx.dstatus, 0, sizeof(int) * 4, ctx.s));
