@@ -33,6 +33,71 @@ struct BState {
     double rel, rms, rel0;
 };
 
+// one problem of the batched operator detection (the scan of k_maxabs_all):
+// its interior fields and the launch blocks it takes
+struct BDetect {
+    const double *vel, *reac, *dcoeff, *source, *soln;
+    int nx, ny, nz;
+    unsigned rows;
+    FastDiv divNy;
+    int blk0, nblk;
+    unsigned long long* out;  // 9 words: k_maxabs_all's six maxima (two spare), dcoeff(1,1,1)
+};
+
+// the detection of every problem of a batch in one launch: each problem's
+// blocks scan its rows (warp per row, as k_maxabs_all) and its first block
+// also records the coefficient of cell (1,1,1)
+__global__ void __launch_bounds__(256) kb_detect(const BDetect* __restrict__ dd, int np)
+{
+    int lo = 0, hi = np - 1;  // the problem whose block range holds this block
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (dd[mid].blk0 <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const BDetect& d = dd[lo];
+    const long long gx = d.nx + 2, gy = d.ny + 2;
+    const long long ng = gx * gy * (d.nz + 2);
+    const double ref = d.dcoeff[1 + gx * (1 + gy)];
+    if (blockIdx.x == (unsigned)d.blk0 && threadIdx.x == 0) d.out[8] = (unsigned long long)__double_as_longlong(ref);
+    long long m[6] = {0, 0, 0, 0, 0, 0};
+    auto upd = [](long long& cur, double v) {
+        v = fabs(v);
+        if (!(v <= 1.0e308)) v = __longlong_as_double(0x7ff8000000000000LL);
+        const long long b = __double_as_longlong(v);
+        cur = b > cur ? b : cur;
+    };
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned warp = ((blockIdx.x - d.blk0) * blockDim.x + threadIdx.x) >> 5, nwarp = (d.nblk * blockDim.x) >> 5;
+    for (unsigned row = warp; row < d.rows; row += nwarp) {
+        const unsigned k = d.divNy.div(row), j = row - k * (unsigned)d.ny;
+        const long long base = 1 + gx * ((long long)(j + 1) + gy * (long long)(k + 1));
+        for (int i = lane; i < d.nx; i += 32) {
+            const long long g = base + i;
+            if (d.vel) {
+                upd(m[0], d.vel[g]);
+                upd(m[0], d.vel[g + ng]);
+                upd(m[0], d.vel[g + 2 * ng]);
+            }
+            if (d.reac) upd(m[1], d.reac[g]);
+            const double c = d.dcoeff[g];
+            upd(m[2], c - ref);
+            upd(m[5], c);
+            upd(m[3], d.source[g]);
+            upd(m[4], d.soln[g]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        long long b = m[q];
+        for (int o = 16; o > 0; o >>= 1) {
+            const long long ob = __shfl_down_sync(0xffffffffu, b, o);
+            b = ob > b ? ob : b;
+        }
+        if (lane == 0 && b > 0) atomicMax(d.out + q, (unsigned long long)b);
+    }
+}
+
 // every problem active, no iteration done (the start of a batched solve)
 __global__ void kb_reset_state(BState* st, int np)
 {
@@ -519,6 +584,8 @@ struct BatchState {
     // operator detection of every problem (9 words each), read back at once
     unsigned long long* ddet = nullptr;
     unsigned long long* hdet = nullptr;  // page-locked
+    BDetect* ddd = nullptr;              // the detection launch's problem table
+    BDetect* hdd = nullptr;              // page-locked
     int det_cap = 0;
     // streams of the per-problem set-ups (independent: they overlap on the
     // device), joined to the handle's stream before the iterations
@@ -531,7 +598,22 @@ struct BatchState {
     cudaStream_t set_s[NSET] = {};
     cudaEvent_t set_e[NSET] = {};
     cudaEvent_t start_e = nullptr;
+    // a repeated batch (same problems, buffers, options and detected
+    // operators) replays its set-up and its unpacking as CUDA graphs, captured
+    // at the second call with that key, and reuses its step plan
+    std::vector<long long> prep_key;
+    int prep_calls = 0;                  // calls in a row with prep_key
+    cudaGraphExec_t prep_exec = nullptr, post_exec = nullptr;
+    std::shared_ptr<void> plan;          // BatchPlan<T> of prep_key
 };
+
+static void batch_release_prep(BatchState& B)
+{
+    if (B.prep_exec) cudaGraphExecDestroy(B.prep_exec);
+    if (B.post_exec) cudaGraphExecDestroy(B.post_exec);
+    B.prep_exec = B.post_exec = nullptr;
+    B.plan.reset();
+}
 
 static int sub_init(Ctx& parent, Ctx& sc)
 {
@@ -588,11 +670,14 @@ static void destroy_batch(Ctx& ctx)
     cudaFree(B.dloops);
     if (B.ddet) cudaFree(B.ddet);
     if (B.hdet) cudaFreeHost(B.hdet);
+    if (B.ddd) cudaFree(B.ddd);
+    if (B.hdd) cudaFreeHost(B.hdd);
     for (int i = 0; i < BatchState::NSET; i++) {
         if (B.set_s[i]) cudaStreamDestroy(B.set_s[i]);
         if (B.set_e[i]) cudaEventDestroy(B.set_e[i]);
     }
     if (B.start_e) cudaEventDestroy(B.start_e);
+    batch_release_prep(B);
     delete ctx.batch;
     ctx.batch = nullptr;
 }
@@ -1005,6 +1090,47 @@ static void assign_grids(BatchState& B, BatchPlan<T>& P)
     for (BStep& s : P.body) { s.grid = grid_of(s); s.vec = vec_of(s); }
 }
 
+// everything a batch's set-up sequence depends on: word size, options, every
+// problem's description (sizes, buffers, boundary codes) and what its
+// detection decides (finite inputs, convection, reaction field, uniform
+// coefficient and its value, zero initial guess) -- not the data itself, so
+// new right-hand sides or initial guesses in the same buffers replay
+static std::vector<long long> prep_key_of(int wordsize, int np, const mps_problem* probs, const mps_solver_opts* o,
+                                          int inner, const unsigned long long* det, const std::vector<char>& scanned)
+{
+    std::vector<long long> k;
+    auto bytes = [&k](const void* p, size_t n) {
+        const size_t w = (n + 7) / 8;
+        const size_t at = k.size();
+        k.resize(at + w, 0);
+        std::memcpy(k.data() + at, p, n);
+    };
+    k.push_back(wordsize);
+    k.push_back(inner);
+    k.push_back(np);
+    bytes(o, sizeof(*o));
+    for (int p = 0; p < np; p++) {
+        bytes(&probs[p], sizeof(mps_problem));
+        k.push_back(scanned[p]);
+        if (scanned[p]) {
+            double v[9];
+            std::memcpy(v, det + 9 * p, sizeof(v));
+            bool finite = true;
+            for (int q = 0; q < 6; q++) finite = finite && v[q] <= 1e308;
+            const bool kuni = v[2] == 0.0;
+            k.push_back(finite);
+            k.push_back(v[0] == 0.0);  // no convection
+            k.push_back(v[1] > 0.0);   // reaction field
+            k.push_back(kuni);
+            k.push_back(v[4] == 0.0);  // zero initial guess
+            long long kb = 0;
+            if (kuni) std::memcpy(&kb, &v[8], 8);  // the uniform coefficient enters the operators
+            k.push_back(kb);
+        }
+    }
+    return k;
+}
+
 template <class T>
 static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_solver_opts* o, mps_solve_info* infos)
 {
@@ -1014,6 +1140,8 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     // ---- per-problem contexts and set-up ----
     if ((int)B.sub.size() != np) {
         batch_release_graph(B);
+        batch_release_prep(B);
+        B.prep_key.clear();
         for (auto& sc : B.sub) sub_free(*sc);
         B.sub.clear();
         for (int p = 0; p < np; p++) {
@@ -1029,18 +1157,24 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     if (np > B.det_cap) {
         if (B.ddet) cudaFree(B.ddet);
         if (B.hdet) cudaFreeHost(B.hdet);
+        if (B.ddd) cudaFree(B.ddd);
+        if (B.hdd) cudaFreeHost(B.hdd);
         B.ddet = nullptr;
         B.hdet = nullptr;
+        B.ddd = nullptr;
+        B.hdd = nullptr;
         B.det_cap = 0;
         if (cudaMalloc((void**)&B.ddet, sizeof(unsigned long long) * 9 * np) != cudaSuccess ||
-            cudaMallocHost((void**)&B.hdet, sizeof(unsigned long long) * 9 * np) != cudaSuccess) {
+            cudaMallocHost((void**)&B.hdet, sizeof(unsigned long long) * 9 * np) != cudaSuccess ||
+            cudaMalloc((void**)&B.ddd, sizeof(BDetect) * np) != cudaSuccess ||
+            cudaMallocHost((void**)&B.hdd, sizeof(BDetect) * np) != cudaSuccess) {
             ctx.err.msg = "batched: detection buffers";
             return MPS_ERR_NOMEM;
         }
         B.det_cap = np;
     }
     std::vector<char> scanned(np, 0);
-    CK(cudaMemsetAsync(B.ddet, 0, sizeof(unsigned long long) * 9 * np, ctx.s));
+    int ndet = 0, blocks = 0;
     for (int p = 0; p < np; p++) {
         const mps_problem& q = probs[p];
         const mps_grid& g = q.g;
@@ -1050,18 +1184,42 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
         bool bcok = true;
         for (int f = 0; f < 6; f++) bcok = bcok && q.bc_code[f] >= 1 && q.bc_code[f] <= 5;
         if (!bcok) continue;
-        const double llen[3] = {1.0, 1.0, 1.0};  // the scan reads sizes only
-        const Lev L = make_lev_uniform(g.lx, g.ly, g.lz, llen, q.bc_code);
-        const long long ncell = (long long)g.lx * g.ly * g.lz;
-        pdl_launch(k_maxabs_all, std::min<unsigned>(nblk(ncell), 1184), TPB, 0, ctx.s, L, q.vel, q.reac, q.dcoeff,
-                   q.source, q.soln, B.ddet + 9 * p);
-        CKL();
-        CK(cudaMemcpyAsync(B.ddet + 9 * p + 8, q.dcoeff + 1 + (g.lx + 2) * (1 + (long long)(g.ly + 2)),
-                           sizeof(double), cudaMemcpyDeviceToDevice, ctx.s));
+        BDetect& d = B.hdd[ndet++];
+        d.vel = q.vel;
+        d.reac = q.reac;
+        d.dcoeff = q.dcoeff;
+        d.source = q.source;
+        d.soln = q.soln;
+        d.nx = g.lx;
+        d.ny = g.ly;
+        d.nz = g.lz;
+        d.rows = (unsigned)g.ly * (unsigned)g.lz;
+        d.divNy.init((unsigned)g.ly);
+        d.blk0 = blocks;
+        d.nblk = (int)std::min<long long>(((long long)d.rows + 7) / 8, 256);  // a warp per row, 8 per block
+        d.out = B.ddet + 9 * p;
+        blocks += d.nblk;
         scanned[p] = 1;
+    }
+    CK(cudaMemsetAsync(B.ddet, 0, sizeof(unsigned long long) * 9 * np, ctx.s));
+    if (ndet > 0) {
+        CK(cudaMemcpyAsync(B.ddd, B.hdd, sizeof(BDetect) * ndet, cudaMemcpyHostToDevice, ctx.s));
+        kb_detect<<<blocks, 256, 0, ctx.s>>>(B.ddd, ndet);
+        CKL();
     }
     CK(cudaMemcpyAsync(B.hdet, B.ddet, sizeof(unsigned long long) * 9 * np, cudaMemcpyDeviceToHost, ctx.s));
     CK(cudaStreamSynchronize(ctx.s));
+    // the set-up of every problem: run eagerly, captured as a graph at the
+    // second call with the same key (then launched), or replayed
+    const std::vector<long long> pkey = prep_key_of((int)sizeof(T), np, probs, o, inner, B.hdet, scanned);
+    if (pkey != B.prep_key) {
+        batch_release_prep(B);
+        B.prep_key = pkey;
+        B.prep_calls = 0;
+    }
+    const bool replay = B.prep_exec != nullptr;
+    const bool capture = !replay && B.prep_calls == 1;
+    B.prep_calls++;
     if (!B.start_e) {
         for (int i = 0; i < BatchState::NSET; i++) {
             CK(cudaStreamCreateWithFlags(&B.set_s[i], cudaStreamNonBlocking));
@@ -1069,45 +1227,75 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
         }
         CK(cudaEventCreateWithFlags(&B.start_e, cudaEventDisableTiming));
     }
-    CK(cudaEventRecord(B.start_e, ctx.s));
-    const int nset = std::min(np, (int)BatchState::NSET);
-    for (int i = 0; i < nset; i++) CK(cudaStreamWaitEvent(B.set_s[i], B.start_e, 0));
-    for (int p = 0; p < np; p++) {
-        Ctx& sc = *B.sub[p];
-        sc.s = B.set_s[p % nset];
-        const mps_problem& q = probs[p];
-        Inputs in;
-        in.vel = q.vel;
-        in.dcoeff = q.dcoeff;
-        in.reac = q.reac;
-        in.source = q.source;
-        for (int f = 0; f < 6; f++) in.bcval[f] = q.bcval[f];
-        in.sterm = q.mgridsterm;
-        in.soln = q.soln;
-        mps_solve_info inf;
-        sc.launches = 0;
-        int st = solve_impl(sc, &q.g, q.timederiv, q.dt, in, q.bc_code, o, &inf, 0, 1,
-                            scanned[p] ? B.hdet + 9 * p : nullptr);
-        ctx.launches += sc.launches;
-        if (st) {
-            ctx.err.msg = "batched problem " + std::to_string(p) + ": " + sc.err.msg;
-            if (infos) { std::memset(&infos[p], 0, sizeof(mps_solve_info)); infos[p].status = st; }
-            return st;
+    auto setups = [&]() -> int {
+        CK(cudaEventRecord(B.start_e, ctx.s));
+        const int nset = std::min(np, (int)BatchState::NSET);
+        for (int i = 0; i < nset; i++) CK(cudaStreamWaitEvent(B.set_s[i], B.start_e, 0));
+        for (int p = 0; p < np; p++) {
+            Ctx& sc = *B.sub[p];
+            sc.s = B.set_s[p % nset];
+            const mps_problem& q = probs[p];
+            Inputs in;
+            in.vel = q.vel;
+            in.dcoeff = q.dcoeff;
+            in.reac = q.reac;
+            in.source = q.source;
+            for (int f = 0; f < 6; f++) in.bcval[f] = q.bcval[f];
+            in.sterm = q.mgridsterm;
+            in.soln = q.soln;
+            mps_solve_info inf;
+            sc.launches = 0;
+            int st = solve_impl(sc, &q.g, q.timederiv, q.dt, in, q.bc_code, o, &inf, 0, 1,
+                                scanned[p] ? B.hdet + 9 * p : nullptr);
+            ctx.launches += sc.launches;
+            if (st) {
+                ctx.err.msg = "batched problem " + std::to_string(p) + ": " + sc.err.msg;
+                if (infos) { std::memset(&infos[p], 0, sizeof(mps_solve_info)); infos[p].status = st; }
+                return st;
+            }
+            if (sc.sig.opclass != 0) {
+                ctx.err.msg = "batched problem " + std::to_string(p) +
+                              ": batched solves take the diffusion class (no convection, upwind flux, no transpose)";
+                return MPS_ERR_BAD_ARG;
+            }
         }
-        if (sc.sig.opclass != 0) {
-            ctx.err.msg = "batched problem " + std::to_string(p) +
-                          ": batched solves take the diffusion class (no convection, upwind flux, no transpose)";
-            return MPS_ERR_BAD_ARG;
+        for (int i = 0; i < nset; i++) {
+            CK(cudaEventRecord(B.set_e[i], B.set_s[i]));
+            CK(cudaStreamWaitEvent(ctx.s, B.set_e[i], 0));
         }
+        for (int p = 0; p < np; p++) B.sub[p]->s = ctx.s;
+        return 0;
+    };
+    if (replay) {
+        CK(cudaGraphLaunch(B.prep_exec, ctx.s));
+    } else if (capture) {
+        CK(cudaStreamBeginCapture(ctx.s, cudaStreamCaptureModeThreadLocal));
+        const int st = setups();
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(ctx.s, &g);
+        if (st == 0 && ce == cudaSuccess && g) ce = cudaGraphInstantiate(&B.prep_exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (st) return st;
+        if (ce != cudaSuccess || !B.prep_exec) {  // not capturable: eager from now on for this key
+            cudaGetLastError();
+            B.prep_exec = nullptr;
+            B.prep_calls = 2;
+            for (int p = 0; p < np; p++) B.sub[p]->s = ctx.s;
+            if (int st2 = setups()) return st2;
+        } else {
+            CK(cudaGraphLaunch(B.prep_exec, ctx.s));
+        }
+    } else if (int st = setups()) {
+        return st;
     }
-    for (int i = 0; i < nset; i++) {
-        CK(cudaEventRecord(B.set_e[i], B.set_s[i]));
-        CK(cudaStreamWaitEvent(ctx.s, B.set_e[i], 0));
-    }
-    for (int p = 0; p < np; p++) B.sub[p]->s = ctx.s;
     // ---- plan, device tables ----
-    BatchPlan<T> P;
-    plan_batch<T>(B, P, o, inner);
+    const bool plan_fresh = !replay || !B.plan;
+    if (plan_fresh) {
+        auto fresh = std::make_shared<BatchPlan<T>>();
+        plan_batch<T>(B, *fresh, o, inner);
+        B.plan = fresh;
+    }
+    BatchPlan<T>& P = *static_cast<BatchPlan<T>*>(B.plan.get());
     auto grow = [&](auto*& ptr, size_t& cap, size_t n, size_t elem) -> int {
         if (n <= cap) return 0;
         batch_release_graph(B);
@@ -1150,7 +1338,9 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     }
     std::vector<long long> hn(np);
     for (int p = 0; p < np; p++) hn[p] = (long long)probs[p].g.lx * probs[p].g.ly * probs[p].g.lz;
-    if (P.desc != B.up_desc || P.task != B.up_task || hn != B.up_cells) {
+    // (a replayed plan is the one uploaded last, unless a buffer was reallocated)
+    if ((plan_fresh || B.up_desc.empty() || B.up_cells.empty()) &&
+        (P.desc != B.up_desc || P.task != B.up_task || hn != B.up_cells)) {
         CK(cudaMemcpyAsync(B.ddesc, P.desc.data(), P.desc.size(), cudaMemcpyHostToDevice, ctx.s));
         CK(cudaMemcpyAsync(B.dtask, P.task.data(), sizeof(int) * P.task.size(), cudaMemcpyHostToDevice, ctx.s));
         CK(cudaMemcpyAsync(B.dncell, hn.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx.s));
@@ -1241,20 +1431,39 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     std::vector<BState> hs(np);
     CK(cudaMemcpyAsync(hs.data(), B.dst, sizeof(BState) * np, cudaMemcpyDeviceToHost, ctx.s));
     CK(cudaMemcpyAsync(&loops, B.dloops, sizeof(int), cudaMemcpyDeviceToHost, ctx.s));
-    for (int p = 0; p < np; p++) {
-        Ctx& sc = *B.sub[p];
-        const Lev& L0 = sc.lev[0];
-        const long long n = (long long)L0.nx * L0.ny * L0.nz;
-        k_unpack<double><<<nblk(n), TPB, 0, ctx.s>>>(L0, csplit<double>(sc.x64, L0), probs[p].soln);
-        CKL();
-        if (o->fill_ghosts) {
-            const int mx = std::max(std::max(L0.ny * L0.nz, L0.nx * L0.nz), L0.nx * L0.ny);
-            const double* zf[6];
-            for (int f = 0; f < 6; f++) zf[f] = probs[p].bcval[f];
-            k_fill_ghosts<<<nblk(mx), TPB, 0, ctx.s>>>(L0, probs[p].soln, zf[0], zf[1], zf[2], zf[3], zf[4], zf[5]);
+    auto unpack = [&]() -> int {  // every solution back to its caller's ghosted array
+        for (int p = 0; p < np; p++) {
+            Ctx& sc = *B.sub[p];
+            const Lev& L0 = sc.lev[0];
+            const long long n = (long long)L0.nx * L0.ny * L0.nz;
+            k_unpack<double><<<nblk(n), TPB, 0, ctx.s>>>(L0, csplit<double>(sc.x64, L0), probs[p].soln);
             CKL();
+            if (o->fill_ghosts) {
+                const int mx = std::max(std::max(L0.ny * L0.nz, L0.nx * L0.nz), L0.nx * L0.ny);
+                const double* zf[6];
+                for (int f = 0; f < 6; f++) zf[f] = probs[p].bcval[f];
+                k_fill_ghosts<<<nblk(mx), TPB, 0, ctx.s>>>(L0, probs[p].soln, zf[0], zf[1], zf[2], zf[3], zf[4],
+                                                            zf[5]);
+                CKL();
+            }
+        }
+        return 0;
+    };
+    if (B.prep_exec && !B.post_exec) {  // a repeated batch: capture the unpacking too
+        CK(cudaStreamBeginCapture(ctx.s, cudaStreamCaptureModeThreadLocal));
+        const int st = unpack();
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(ctx.s, &g);
+        if (st == 0 && ce == cudaSuccess && g) ce = cudaGraphInstantiate(&B.post_exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (st) return st;
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            B.post_exec = nullptr;
         }
     }
+    if (B.post_exec) CK(cudaGraphLaunch(B.post_exec, ctx.s));
+    else if (int st = unpack()) return st;
     CK(cudaEventRecord(ctx.e1, ctx.s));
     CK(cudaStreamSynchronize(ctx.s));
     float ms = 0.f;

@@ -95,3 +95,44 @@ def test_batched_limits_and_repeats(handle):
     # the handle still solves single problems afterwards
     x, info = solver.linsolve(ps[0], handle=handle)
     assert info["status"] == 0
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_repeated_batch_replays_setup_with_new_data(prec):
+    """A repeated batch (same problems and buffers) runs its set-up eagerly,
+    then captures it as a CUDA graph, then replays it.  New right-hand sides
+    and initial guesses written into the same buffers must be picked up by
+    the replayed set-up: every solve equals an eager solve of the same data on
+    a fresh handle (the same kernels, so to rounding of the FP64 sums)."""
+    ps = _mixed_batch()
+    dps = [solver.DeviceProblem(p) for p in ps]
+    xs = [torch.zeros(p.ghost_shape, dtype=torch.float64, device="cuda") for p in ps]
+    rep = capi.Handle(0)
+    rng = np.random.default_rng(7)
+    try:
+        for call in range(5):
+            if call >= 3:  # new data in the same device buffers
+                for dp, p in zip(dps, ps):
+                    if np.abs(p.source).max() == 0.0:
+                        continue
+                    dp.source.copy_(torch.from_numpy(rng.uniform(-1.0, 1.0, size=p.ghost_shape)))
+            for x in xs:
+                x.zero_()
+            if call == 4:  # and a non-zero initial guess
+                for x in xs:
+                    x.copy_(torch.from_numpy(rng.uniform(-0.1, 0.1, size=tuple(x.shape))))
+            x0 = [x.clone() for x in xs]
+            infos = solver.linsolve_batched_dev(dps, xs, handle=rep, tol=1e-11, precision=prec, maxit=60)
+            fresh = capi.Handle(0)
+            try:
+                ys = [x.clone() for x in x0]
+                ref = solver.linsolve_batched_dev(dps, ys, handle=fresh, tol=1e-11, precision=prec, maxit=60)
+            finally:
+                fresh.close()
+            for x, y, a, b in zip(xs, ys, infos, ref):
+                assert a["status"] == b["status"] == 0, (call, a, b)
+                assert a["iters"] == b["iters"], (call, a["iters"], b["iters"])
+                scale = max(float(y.abs().max()), 1e-300)
+                assert float((x - y).abs().max()) <= 1e-12 * scale, call
+    finally:
+        rep.close()
