@@ -604,6 +604,7 @@ struct BatchState {
     std::vector<long long> prep_key;
     int prep_calls = 0;                  // calls in a row with prep_key
     cudaGraphExec_t prep_exec = nullptr, post_exec = nullptr;
+    long long prep_kernels = 0, post_kernels = 0;  // kernels in those graphs (the launch counts)
     std::shared_ptr<void> plan;          // BatchPlan<T> of prep_key
 };
 
@@ -1268,9 +1269,12 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
     };
     if (replay) {
         CK(cudaGraphLaunch(B.prep_exec, ctx.s));
+        ctx.launches += B.prep_kernels;
     } else if (capture) {
         CK(cudaStreamBeginCapture(ctx.s, cudaStreamCaptureModeThreadLocal));
+        const long long k0 = ctx.launches;
         const int st = setups();
+        B.prep_kernels = ctx.launches - k0;
         cudaGraph_t g = nullptr;
         cudaError_t ce = cudaStreamEndCapture(ctx.s, &g);
         if (st == 0 && ce == cudaSuccess && g) ce = cudaGraphInstantiate(&B.prep_exec, g, 0);
@@ -1280,6 +1284,7 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
             cudaGetLastError();
             B.prep_exec = nullptr;
             B.prep_calls = 2;
+            ctx.launches = k0;  // the captured launches never ran
             for (int p = 0; p < np; p++) B.sub[p]->s = ctx.s;
             if (int st2 = setups()) return st2;
         } else {
@@ -1449,9 +1454,13 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
         }
         return 0;
     };
+    bool post_captured = false;
     if (B.prep_exec && !B.post_exec) {  // a repeated batch: capture the unpacking too
         CK(cudaStreamBeginCapture(ctx.s, cudaStreamCaptureModeThreadLocal));
+        const long long k0 = ctx.launches;
         const int st = unpack();
+        B.post_kernels = ctx.launches - k0;
+        post_captured = true;
         cudaGraph_t g = nullptr;
         cudaError_t ce = cudaStreamEndCapture(ctx.s, &g);
         if (st == 0 && ce == cudaSuccess && g) ce = cudaGraphInstantiate(&B.post_exec, g, 0);
@@ -1462,8 +1471,12 @@ static int batched_solve(Ctx& ctx, int np, const mps_problem* probs, const mps_s
             B.post_exec = nullptr;
         }
     }
-    if (B.post_exec) CK(cudaGraphLaunch(B.post_exec, ctx.s));
-    else if (int st = unpack()) return st;
+    if (B.post_exec) {
+        CK(cudaGraphLaunch(B.post_exec, ctx.s));
+        if (!post_captured) ctx.launches += B.post_kernels;
+    } else if (int st = unpack()) {
+        return st;
+    }
     CK(cudaEventRecord(ctx.e1, ctx.s));
     CK(cudaStreamSynchronize(ctx.s));
     float ms = 0.f;

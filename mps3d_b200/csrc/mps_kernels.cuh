@@ -1958,4 +1958,21 @@ __global__ void k_axpy(long long n, double a, const A* __restrict__ x, B* __rest
         y[t] = (B)((double)y[t] + a * (double)x[t]);
 }
 
+// y0 += a x0 and y1 += a x1 in one launch (both colour halves of a split
+// field: the mixed solve's FP64 update x += e)
+template <class A, class B>
+__global__ void k_axpy2(long long n, double a, const A* __restrict__ x0, B* __restrict__ y0,
+                        const A* __restrict__ x1, B* __restrict__ y1)
+{
+    pdl_wait();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 2 * n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const bool h = t >= n;
+        const long long e = h ? t - n : t;
+        const A* x = h ? x1 : x0;
+        B* y = h ? y1 : y0;
+        y[e] = (B)((double)y[e] + a * (double)x[e]);
+    }
+}
+
 }  // namespace mps

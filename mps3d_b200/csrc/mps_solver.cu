@@ -1183,13 +1183,14 @@ static bool sub_layout_with(const Ctx& ctx, int l0, bool kf, bool df, const mps_
     const long long ncs = (long long)Cc.nx * Cc.ny * Cc.nz;
     P.ainv_off = ainv_in_smem ? (int)bytes : -1;
     if (ainv_in_smem) bytes += ((size_t)(ncs * ncs) * sizeof(double) + 15) & ~(size_t)15;
-    P.img_bytes = (int)(bytes - P.img_off);
+    // the tables are part of the image too (built once per solve)
     P.lin_off = (int)bytes;
     bytes += ((size_t)nlin * sizeof(SubLin<T>) + 15) & ~(size_t)15;
     P.ax_off = (int)bytes;
     bytes += ((size_t)nax * sizeof(SubAx<T>) + 15) & ~(size_t)15;
     P.row_off = (int)bytes;
-    bytes += (size_t)nrow * sizeof(SubRow);
+    bytes += ((size_t)nrow * sizeof(SubRow) + 15) & ~(size_t)15;
+    P.img_bytes = (int)(bytes - P.img_off);
     P.nlin = nlin;
     P.nax = nax;
     P.nrow = nrow;
@@ -2039,10 +2040,9 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
                 ctx.red0_ready = false;
                 if (s2) return s2;
             }
-            const unsigned ab = std::min<unsigned>(nblk(L.half), 4736);
-            pdl_launch(k_axpy<float, double>, ab, TPB, 0, ctx.s, L.half, 1.0, H.U[0][H.ri[0]], ctx.x64);
-            CKL();
-            pdl_launch(k_axpy<float, double>, ab, TPB, 0, ctx.s, L.half, 1.0, H.U[0][H.bi[0]] + L.half, ctx.x64 + L.half);
+            const unsigned ab = std::min<unsigned>(nblk(2 * L.half), 4736);
+            pdl_launch(k_axpy2<float, double>, ab, TPB, 0, ctx.s, L.half, 1.0, (const float*)H.U[0][H.ri[0]], ctx.x64,
+                       (const float*)(H.U[0][H.bi[0]] + L.half), ctx.x64 + L.half);
             CKL();
             return residual();
         };

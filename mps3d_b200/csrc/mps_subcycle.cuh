@@ -401,6 +401,23 @@ __global__ void __launch_bounds__(SUB_TPB) k_sub_image(const __grid_constant__ S
         double* ai = reinterpret_cast<double*>(img + (P.ainv_off - P.img_off));
         for (int e = threadIdx.x; e < ncoarse * ncoarse; e += SUB_TPB) ai[e] = AinvT[e];
     }
+    SubLin<T>* lin = reinterpret_cast<SubLin<T>*>(img + (P.lin_off - P.img_off));
+    SubAx<T>* axt = reinterpret_cast<SubAx<T>*>(img + (P.ax_off - P.img_off));
+    SubRow* rowt = reinterpret_cast<SubRow*>(img + (P.row_off - P.img_off));
+    for (int e = threadIdx.x; e < P.nlin; e += SUB_TPB) lin[e] = P.lin[e];
+    for (int e = threadIdx.x; e < P.nax; e += SUB_TPB) axt[e] = P.ax[e];
+    for (int s = 0; s < P.nl; s++) {
+        const SubGeo<T>& G = P.geo[s];
+        for (int r = threadIdx.x; r < G.rows; r += SUB_TPB) {
+            const int k = (int)G.dny.div((unsigned)r), j = r - k * G.ny;
+            SubRow R;
+            R.j = j;
+            R.k = k;
+            R.g0 = sub_gidx(G, 0, j, k);
+            R.n0 = G.nx * r;
+            rowt[G.row0 + r] = R;
+        }
+    }
 }
 
 // the V-cycle from geo[0] (zero initial guess, right-hand side fin) down to
@@ -420,9 +437,10 @@ __global__ void __launch_bounds__(SUB_TPB, 1) k_subcycle(const __grid_constant__
     M.lin = lin;
     M.ax = axt;
     M.row = rowt;
-    // the solve-constant image and the top level's right-hand side from
-    // device memory (all loads issued before the first wait), the tables
-    // from the parameter, zero u (ghosts included)
+    // the solve-constant image (coefficients, diagonal extras, inverse, row
+    // and axis tables, brackets) and the top level's right-hand side from
+    // device memory (loads issued in batches before their stores), zero u
+    // (ghosts included)
     {
         uint4* dst = reinterpret_cast<uint4*>(sub_smem + P.img_off);
         const int nv = P.img_bytes >> 4;
@@ -441,19 +459,8 @@ __global__ void __launch_bounds__(SUB_TPB, 1) k_subcycle(const __grid_constant__
             }
         }
     }
-    for (int e = threadIdx.x; e < P.nax; e += SUB_TPB) axt[e] = P.ax[e];
-    for (int e = threadIdx.x; e < P.nlin; e += SUB_TPB) lin[e] = P.lin[e];
     for (int s = 0; s < P.nl; s++) {
         const SubGeo<T>& G = P.geo[s];
-        for (int r = threadIdx.x; r < G.rows; r += SUB_TPB) {
-            const int k = (int)G.dny.div((unsigned)r), j = r - k * G.ny;
-            SubRow R;
-            R.j = j;
-            R.k = k;
-            R.g0 = sub_gidx(G, 0, j, k);
-            R.n0 = G.nx * r;
-            rowt[G.row0 + r] = R;
-        }
         const int ng = G.gx * G.gy * (G.nz + 2);
         T* u = M.fld + P.ou[s];
         for (int e = threadIdx.x; e < ng; e += SUB_TPB) u[e] = T(0);
