@@ -546,6 +546,24 @@ __global__ void __launch_bounds__(TPB, ResidShape<T>::MINB) k_residv(Lev L, KOp<
 // exist (restriction, mgridsteps.f90:11-53, applied to the residual at :531).
 // One thread per coarse cell, natural order.
 // ---------------------------------------------------------------------
+// the coarse level's first red pass from a zero state, written with the
+// restriction: u(red) = f / diag (gs_value with a zero off-diagonal part, as the
+// zero-state colour pass computes it); d holds the coarse rows' diagonals
+// (red half).  u == nullptr: no such write.
+template <class T>
+struct RedZ {
+    T* u;
+    const T* d;
+};
+
+// the red pass from zero at coarse cell (I,J,K) (split offset o) whose
+// right-hand side is v
+template <class T>
+__device__ __forceinline__ void redz_put(const RedZ<T>& rz, int colour, long long o, T v)
+{
+    if (rz.u && colour == 0) rz.u[o] = gs_value<T>(v, __ldg(&rz.d[o]), T(0));
+}
+
 // the share `part` of `nparts` of the children of coarse cell (I,J,K):
 // sum of width-weighted residuals and of the weights
 template <class T, class Op>
@@ -579,7 +597,7 @@ __device__ __forceinline__ void resid_restrict_part(const Lev& F, const Op& op, 
 template <class T, class Op>
 __device__ __forceinline__ void resid_restrict_body(const Lev& F, const Op& op, const CSplit<T>& u,
                                                     const CSplit<T>& f, const Lev& C, const Split<T>& fc, int geom,
-                                                    unsigned t)
+                                                    unsigned t, RedZ<T> rz = RedZ<T>{nullptr, nullptr})
 {
     const unsigned ncx = C.nx, ncy = C.ny;
     if (t >= ncx * ncy * (unsigned)C.nz) return;
@@ -589,15 +607,17 @@ __device__ __forceinline__ void resid_restrict_body(const Lev& F, const Op& op, 
     const unsigned I = rem - J * ncx;
     T s, vol;
     resid_restrict_part<T, Op>(F, op, u, f, C, geom, (int)I, (int)J, (int)K, 0, 1, s, vol);
-    fc.half(scol(I, J, K))[soff(C, I, J, K)] = geom ? s / vol : s * (T(1) / vol);
+    const T v = geom ? s / vol : s * (T(1) / vol);
+    fc.half(scol(I, J, K))[soff(C, I, J, K)] = v;
+    redz_put(rz, scol(I, J, K), soff(C, I, J, K), v);
 }
 
 template <class T, class Op>
 __global__ void __launch_bounds__(TPB) k_resid_restrict(Lev F, Op op, CSplit<T> u, CSplit<T> f, Lev C,
-                                                        Split<T> fc, int geom)
+                                                        Split<T> fc, int geom, RedZ<T> rz)
 {
     pdl_wait();
-    resid_restrict_body<T, Op>(F, op, u, f, C, fc, geom, blockIdx.x * TPB + threadIdx.x);
+    resid_restrict_body<T, Op>(F, op, u, f, C, fc, geom, blockIdx.x * TPB + threadIdx.x, rz);
 }
 
 // ---------------------------------------------------------------------
@@ -748,7 +768,8 @@ __device__ __forceinline__ void rop_group(const Lev& L, const ROp<T>& op, int c,
 template <class T, int W, bool UNI, bool IN, class Op = KOp<T>>
 __device__ __forceinline__ void restrict_cells(const Lev& F, const Op& op, const CSplit<T>& u,
                                                const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
-                                               const Box& bx, int J, int K, int h0)
+                                               const Box& bx, int J, int K, int h0,
+                                               const RedZ<T>& rz = RedZ<T>{nullptr, nullptr})
 {
     VecW<T, W> s = zerov<T, W>();
 #pragma unroll
@@ -782,7 +803,11 @@ __device__ __forceinline__ void restrict_cells(const Lev& F, const Op& op, const
 #pragma unroll
     for (int e = 0; e < W; e++) {
         const int I = h0 + e;
-        if (I >= bx.lo[0] && I <= bx.hi[0]) fc.half((I + J + K) & 1)[(I >> 1) + cb] = s.v[e] * T(0.125);
+        if (I >= bx.lo[0] && I <= bx.hi[0]) {
+            const T v = s.v[e] * T(0.125);
+            fc.half((I + J + K) & 1)[(I >> 1) + cb] = v;
+            redz_put(rz, (I + J + K) & 1, (I >> 1) + cb, v);
+        }
     }
 }
 
@@ -828,7 +853,8 @@ struct RestrictSplit {
 template <class T, int W, bool UNI, class Op = KOp<T>>
 __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const Op& op, const CSplit<T>& u,
                                                     const T* __restrict__ fred, const Lev& C, const Split<T>& fc,
-                                                    const Box& bx, const RestrictSplit& rs, unsigned blk)
+                                                    const Box& bx, const RestrictSplit& rs, unsigned blk,
+                                                    const RedZ<T>& rz = RedZ<T>{nullptr, nullptr})
 {
     int part;
     unsigned idx;
@@ -840,7 +866,7 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const Op& op, 
         const int g = rs.ga + (int)(t - r * rs.gin.d);
         const unsigned kk = rs.yin.div(r);
         restrict_cells<T, W, true, true, Op>(F, op, u, fred, C, fc, bx, rs.J0 + (int)(r - kk * rs.yin.d),
-                                         rs.K0 + (int)kk, W * g);
+                                         rs.K0 + (int)kk, W * g, rz);
         return;
     }
     const unsigned t = idx * TPB + threadIdx.x;
@@ -862,7 +888,7 @@ __device__ __forceinline__ void resid_restrict_bulk(const Lev& F, const Op& op, 
     if (J < bx.lo[1] || J > bx.hi[1] || K < bx.lo[2] || K > bx.hi[2]) return;
     const int h0 = W * g;
     if (h0 > bx.hi[0] || h0 + W - 1 < bx.lo[0]) return;
-    restrict_cells<T, W, UNI, false, Op>(F, op, u, fred, C, fc, bx, J, K, h0);
+    restrict_cells<T, W, UNI, false, Op>(F, op, u, fred, C, fc, bx, J, K, h0, rz);
 }
 
 // the t-th cell of an n[0] x n[1] x n[2] grid outside box b: z slabs first,
@@ -904,7 +930,8 @@ __device__ __forceinline__ void shell_cell(unsigned t, const int n[3], const Box
 template <class T, class Op>
 __device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op, const CSplit<T>& u,
                                                      const CSplit<T>& f, const Lev& C, const Split<T>& fc, int geom,
-                                                     const Box& bx, unsigned count, unsigned t)
+                                                     const Box& bx, unsigned count, unsigned t,
+                                                     const RedZ<T>& rz = RedZ<T>{nullptr, nullptr})
 {
     const unsigned cell = t >> 3;
     const int part = (int)(t & 7);
@@ -921,7 +948,11 @@ __device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op,
         s += __shfl_xor_sync(0xffffffffu, s, o, 8);
         vol += __shfl_xor_sync(0xffffffffu, vol, o, 8);
     }
-    if (ok && part == 0) fc.half(scol(I, J, K))[soff(C, I, J, K)] = geom ? s / vol : s * (T(1) / vol);
+    if (ok && part == 0) {
+        const T v = geom ? s / vol : s * (T(1) / vol);
+        fc.half(scol(I, J, K))[soff(C, I, J, K)] = v;
+        redz_put(rz, scol(I, J, K), soff(C, I, J, K), v);
+    }
 }
 
 // bulk and shell in one launch: blocks [0, nb_bulk) take the bulk rows,
@@ -932,18 +963,32 @@ __global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, Op op, CSpl
                                                                                  const T* __restrict__ fred, Lev C,
                                                                                  Split<T> fc, RestrictSplit rs, Box bx,
                                                                                  unsigned nb_bulk, int geom,
-                                                                                 unsigned shell)
+                                                                                 unsigned shell, RedZ<T> rz)
 {
     pdl_wait();
     if (blockIdx.x < nb_bulk) {
-        resid_restrict_bulk<T, W, UNI, Op>(F, op, u, fred, C, fc, bx, rs, blockIdx.x);
+        resid_restrict_bulk<T, W, UNI, Op>(F, op, u, fred, C, fc, bx, rs, blockIdx.x, rz);
     } else {
         CSplit<T> f;
         f.c[0] = fred;
         f.c[1] = fred + F.half;
         resid_restrict_shell<T, Op>(F, op, u, f, C, fc, geom, bx, shell,
-                                        (blockIdx.x - nb_bulk) * TPB + threadIdx.x);
+                                        (blockIdx.x - nb_bulk) * TPB + threadIdx.x, rz);
     }
+}
+
+// the diagonal of every red row of a level (the zero-state colour pass's
+// divisor), for the red pass written with the restriction
+template <class T, class Op>
+__global__ void __launch_bounds__(TPB) k_diag_red(Lev L, Op op, T* __restrict__ d)
+{
+    pdl_wait();
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    int i, j, k;
+    if (!decode(L, t, 0, i, j, k)) return;
+    T diag, off;
+    row_any<T>(op, L, ZeroU<T>(), i, j, k, diag, off);
+    d[soff(L, i, j, k)] = diag;
 }
 
 // coarse ghost rule for the correction (update_boundary_ghostvalues applied

@@ -151,6 +151,7 @@ struct Hier {
     T* U[MAXL][2] = {};  // two full split buffers (2*half) per level
     T* F[MAXL] = {};     // right-hand side (split)
     T* R[MAXL] = {};     // residual scratch (split)
+    T* D[MAXL] = {};     // diagonal of the red rows (levels 1 .. nlev-2; the red pass written by the restriction)
     int ri[MAXL] = {}, bi[MAXL] = {};
     KOp<T> kop[MAXL];
     ROp<T> rop[MAXL];
@@ -232,6 +233,7 @@ struct Ctx {
     bool tma_ok = false;      // the shared-memory colour pass can run (set at workspace set-up)
     bool tma_allowed = true;  // MPS_TMA=0 at handle creation: the register-fed kernels only (for comparisons)
     bool red0_ready = false;  // the finest level's first red pass from zero was written by the outer residual
+    bool redz[MAXL] = {};     // level l's first red pass from zero was written by the restriction into it
     bool sub_allowed = true;  // MPS_SUBCYCLE=0 at handle creation: one launch per pass on every level (for comparisons)
     int sub_l0 = -1;          // first level of the one-block sub-cycle (k_subcycle), -1: none
     size_t inbuf_bytes = 0;
@@ -1288,9 +1290,11 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     int st;
     for (int s = 0; s < o->nu1; s++) {
         bool z = zero_guess && s == 0;
-        if (z && l == 0 && ctx.red0_ready) {
-            // the red pass from zero (red = f / diag) came with the outer residual
+        if (z && ((l == 0 && ctx.red0_ready) || ctx.redz[l])) {
+            // the red pass from zero (red = f / diag) came with the outer
+            // residual (finest level) or with the restriction (coarse levels)
             H.ri[l] ^= 1;
+            ctx.redz[l] = false;
         } else if ((st = colour_pass(ctx, H, ops[l], l, 0, z ? 2 : 0))) {
             return st;
         }
@@ -1302,6 +1306,17 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         CK(cudaMemsetAsync(H.U[l][H.bi[l]] + L.half, 0, sizeof(T) * L.half, ctx.s));
     }
     if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_RESTRICT);
+    // the coarse level's first red pass from zero comes with its right-hand
+    // side (cell-coefficient operators; not for the coarsest level or a level
+    // the one-block sub-cycle takes)
+    RedZ<T> rz{nullptr, nullptr};
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (o->nu1 >= 1 && l + 1 < ctx.nlev - 1 && H.D[l + 1] && !(l + 1 == ctx.sub_l0 && H.sub_ok)) {
+            rz.u = H.U[l + 1][H.ri[l + 1] ^ 1];
+            rz.d = H.D[l + 1];
+            ctx.redz[l + 1] = true;
+        }
+    }
     bool done = false;
     {
         Box bx;
@@ -1317,11 +1332,11 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
                 if (L.uniform)
                     pdl_launch(k_resid_restrict_v<T, W, MB, true, Op>, nbb + nbs, TPB, 0, ctx.s, L, ops[l],
                                ccur(H, L, l), H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom,
-                               (unsigned)shell);
+                               (unsigned)shell, rz);
                 else
                     pdl_launch(k_resid_restrict_v<T, W, MB, false, Op>, nbb + nbs, TPB, 0, ctx.s, L, ops[l],
                                ccur(H, L, l), H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom,
-                               (unsigned)shell);
+                               (unsigned)shell, rz);
             };
             if constexpr (!std::is_same<Op, KOp<T>>::value)  // explicit rows: one coarse cell per thread
                 launch(std::integral_constant<int, 1>(), std::integral_constant<int, RestrictShape<T>::MINB>());
@@ -1337,7 +1352,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     }
     if (!done) {
         pdl_launch(k_resid_restrict<T, Op>, nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s, 
-            L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom);
+            L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, rz);
         CKL();
     }
     if (l == ctx.prof.level) prof_end(ctx);
@@ -1386,6 +1401,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
 template <class T>
 static int vcycle(Ctx& ctx, Hier<T>& H, int opclass, const mps_solver_opts* o, bool zero_guess)
 {
+    for (int l = 0; l < MAXL; l++) ctx.redz[l] = false;  // set and consumed within one V-cycle
     if (opclass == 0) return vcycle_rec(ctx, H, H.kop, 0, o, zero_guess);
     return vcycle_rec(ctx, H, H.rop, 0, o, zero_guess);
 }
@@ -1490,8 +1506,9 @@ static void alloc_hier(Ctx& ctx, Hier<T>& H, bool& ok)
         H.U[l][1] = (T*)ctx.ar.get(b);
         H.F[l] = (T*)ctx.ar.get(b);
         H.R[l] = (T*)ctx.ar.get(b);
+        H.D[l] = (l >= 1 && l < ctx.nlev - 1) ? (T*)ctx.ar.get(sizeof(T) * L.half) : nullptr;
         H.ri[l] = H.bi[l] = 0;
-        ok = ok && H.U[l][0] && H.U[l][1] && H.F[l] && H.R[l];
+        ok = ok && H.U[l][0] && H.U[l][1] && H.F[l] && H.R[l] && (H.D[l] || l < 1 || l >= ctx.nlev - 1);
     }
     const Lev& C = ctx.lev[ctx.nlev - 1];
     const long long n = (long long)C.nx * C.ny * C.nz;
@@ -1932,6 +1949,23 @@ static int solve_impl(Ctx& ctx, const mps_grid* g, int timederiv, double dt, con
     if (sig.opclass == 0 && !prepare_only) {  // the one-block sub-cycle's solve-constant image
         if (need64) st = sub_image(ctx, ctx.h64, ctx.h64.kop, o);
         else st = sub_image(ctx, ctx.h32, ctx.h32.kop, o);
+        if (st) return st;
+        // the red rows' diagonals of the levels with their own launches (the
+        // restriction into such a level also writes its first red pass)
+        auto diag_red = [&](auto& H) -> int {
+            using TT = typename std::remove_reference<decltype(*H.D[0])>::type;
+            const int lend = (ctx.sub_l0 > 0 && H.sub_ok) ? ctx.sub_l0 : nl - 1;
+            for (int l = 1; l < lend && l < nl - 1; l++) {
+                if (!H.D[l]) continue;
+                const Lev& Ll = ctx.lev[l];
+                pdl_launch(k_diag_red<TT, KOp<TT>>, nblk((long long)Ll.P * Ll.rows), TPB, 0, ctx.s, Ll, H.kop[l],
+                           H.D[l]);
+                CKL();
+            }
+            return 0;
+        };
+        if (need64) st = diag_red(ctx.h64);
+        else st = diag_red(ctx.h32);
         if (st) return st;
     }
     if (prepare_only) {
