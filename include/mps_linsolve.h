@@ -228,7 +228,12 @@ typedef struct mps_problem {
  * precision MIXED (FP32 V-cycles, FP64 residual and update) or FP64,
  * nu1 >= 1 and nu1+nu2 even.  infos[p] (may be NULL) gets each problem's
  * result; the return value is MPS_OK unless a problem failed to set up
- * (its status) or produced NaN (MPS_ERR_NAN). */
+ * (its status) or produced NaN (MPS_ERR_NAN).  A call that repeats the
+ * previous one's problems (same sizes, boundary codes, buffers and options,
+ * and inputs of the same operator class: convection, reaction field,
+ * uniform coefficient and its value, zero initial guess) replays the
+ * per-problem set-up as a CUDA graph captured at the second such call; the
+ * buffers' contents may change between calls. */
 int mps_linsolve_batched_dev(mps_handle h, int nprob, const mps_problem* probs,
                              const mps_solver_opts* opts, mps_solve_info* infos, void* stream);
 
