@@ -806,7 +806,8 @@ __device__ __forceinline__ void restrict_cells(const Lev& F, const Op& op, const
         if (I >= bx.lo[0] && I <= bx.hi[0]) {
             const T v = s.v[e] * T(0.125);
             fc.half((I + J + K) & 1)[(I >> 1) + cb] = v;
-            redz_put(rz, (I + J + K) & 1, (I >> 1) + cb, v);
+            // (the 4-cell form of the finest level has no registers to spare)
+            if constexpr (W <= 2) redz_put(rz, (I + J + K) & 1, (I >> 1) + cb, v);
         }
     }
 }
@@ -927,7 +928,7 @@ __device__ __forceinline__ void shell_cell(unsigned t, const int n[3], const Box
 
 // eight lanes per shell cell, each summing a share of the children (every
 // lane of the warp takes part in the shuffles)
-template <class T, class Op>
+template <class T, class Op, bool RZ = true>
 __device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op, const CSplit<T>& u,
                                                      const CSplit<T>& f, const Lev& C, const Split<T>& fc, int geom,
                                                      const Box& bx, unsigned count, unsigned t,
@@ -951,7 +952,7 @@ __device__ __forceinline__ void resid_restrict_shell(const Lev& F, const Op& op,
     if (ok && part == 0) {
         const T v = geom ? s / vol : s * (T(1) / vol);
         fc.half(scol(I, J, K))[soff(C, I, J, K)] = v;
-        redz_put(rz, scol(I, J, K), soff(C, I, J, K), v);
+        if constexpr (RZ) redz_put(rz, scol(I, J, K), soff(C, I, J, K), v);
     }
 }
 
@@ -972,8 +973,8 @@ __global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, Op op, CSpl
         CSplit<T> f;
         f.c[0] = fred;
         f.c[1] = fred + F.half;
-        resid_restrict_shell<T, Op>(F, op, u, f, C, fc, geom, bx, shell,
-                                        (blockIdx.x - nb_bulk) * TPB + threadIdx.x, rz);
+        resid_restrict_shell<T, Op, (W <= 2)>(F, op, u, f, C, fc, geom, bx, shell,
+                                              (blockIdx.x - nb_bulk) * TPB + threadIdx.x, rz);
     }
 }
 

@@ -1307,14 +1307,15 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
     }
     if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_RESTRICT);
     // the coarse level's first red pass from zero comes with its right-hand
-    // side (cell-coefficient operators; not for the coarsest level or a level
-    // the one-block sub-cycle takes)
+    // side (cell-coefficient operators; not for the coarsest level, a level
+    // the one-block sub-cycle takes, or from the finest level, whose
+    // restriction has no registers to spare: the launches below pass rz only
+    // to the forms that write it and then set the level's flag)
     RedZ<T> rz{nullptr, nullptr};
     if constexpr (std::is_same<Op, KOp<T>>::value) {
-        if (o->nu1 >= 1 && l + 1 < ctx.nlev - 1 && H.D[l + 1] && !(l + 1 == ctx.sub_l0 && H.sub_ok)) {
+        if (l >= 1 && o->nu1 >= 1 && l + 1 < ctx.nlev - 1 && H.D[l + 1] && !(l + 1 == ctx.sub_l0 && H.sub_ok)) {
             rz.u = H.U[l + 1][H.ri[l + 1] ^ 1];
             rz.d = H.D[l + 1];
-            ctx.redz[l + 1] = true;
         }
     }
     bool done = false;
@@ -1329,14 +1330,16 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
                 const long long shell = (long long)C.nx * C.ny * C.nz - box_cells(bx);
                 const unsigned nbb = rs.nb_in + rs.nb_xe + rs.nb_out;
                 const unsigned nbs = shell > 0 ? nblk(8 * shell) : 0;
+                const RedZ<T> rzw = W <= 2 ? rz : RedZ<T>{nullptr, nullptr};
+                if (rzw.u) ctx.redz[l + 1] = true;
                 if (L.uniform)
                     pdl_launch(k_resid_restrict_v<T, W, MB, true, Op>, nbb + nbs, TPB, 0, ctx.s, L, ops[l],
                                ccur(H, L, l), H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom,
-                               (unsigned)shell, rz);
+                               (unsigned)shell, rzw);
                 else
                     pdl_launch(k_resid_restrict_v<T, W, MB, false, Op>, nbb + nbs, TPB, 0, ctx.s, L, ops[l],
                                ccur(H, L, l), H.F[l], C, split<T>(H.F[l + 1], C), rs, bx, nbb, ctx.xf[l].geom,
-                               (unsigned)shell, rz);
+                               (unsigned)shell, rzw);
             };
             if constexpr (!std::is_same<Op, KOp<T>>::value)  // explicit rows: one coarse cell per thread
                 launch(std::integral_constant<int, 1>(), std::integral_constant<int, RestrictShape<T>::MINB>());
@@ -1351,6 +1354,7 @@ static int vcycle_rec(Ctx& ctx, Hier<T>& H, const Op* ops, int l, const mps_solv
         }
     }
     if (!done) {
+        if (rz.u) ctx.redz[l + 1] = true;
         pdl_launch(k_resid_restrict<T, Op>, nblk((long long)C.nx * C.ny * C.nz), TPB, 0, ctx.s, 
             L, ops[l], ccur(H, L, l), csplit<T>(H.F[l], L), C, split<T>(H.F[l + 1], C), ctx.xf[l].geom, rz);
         CKL();
