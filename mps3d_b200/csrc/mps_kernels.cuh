@@ -978,6 +978,20 @@ __global__ void __launch_bounds__(TPB, MB) k_resid_restrict_v(Lev F, Op op, CSpl
     }
 }
 
+// the red pass of a colour pass from a zero state, elementwise: u(red) =
+// f(red) / diag with the red rows' diagonals of k_diag_red (no neighbour is
+// read: every one is zero); pads untouched
+template <class T>
+__global__ void __launch_bounds__(TPB) k_red_from_zero(Lev L, const T* __restrict__ f, const T* __restrict__ d,
+                                                       T* __restrict__ out)
+{
+    pdl_wait();
+    const unsigned t = blockIdx.x * TPB + threadIdx.x;
+    int i, j, k;
+    if (!decode(L, t, 0, i, j, k)) return;
+    out[t] = gs_value<T>(f[t], d[t], T(0));
+}
+
 // the diagonal of every red row of a level (the zero-state colour pass's
 // divisor), for the red pass written with the restriction
 template <class T, class Op>

@@ -891,6 +891,15 @@ static int colour_pass(Ctx& ctx, Hier<T>& H, const Op& op, int l, int c, int zer
     else out = H.U[l][H.bi[l] ^ 1] + L.half;
     if (l == ctx.prof.level) prof_begin(ctx, MPS_PROF_SMOOTH);
     if constexpr (std::is_same<Op, KOp<T>>::value) {
+        if (zero_state == 2 && c == 0 && H.D[l]) {  // from zero: f / diag, elementwise
+            pdl_launch(k_red_from_zero<T>, nb, TPB, 0, ctx.s, L, (const T*)fh, (const T*)H.D[l], out);
+            if (l == ctx.prof.level) prof_end(ctx);
+            CKL();
+            H.ri[l] ^= 1;
+            return 0;
+        }
+    }
+    if constexpr (std::is_same<Op, KOp<T>>::value) {
         if (l <= MPS_TMA_LEVELS - 1 && zero_state == 0) {
             const int r = colour_pass_tma<T>(ctx, H, op, l, c, out, fh);
             if (r < 0) return MPS_ERR_CUDA;
@@ -1054,6 +1063,15 @@ static int sub_first_level(const Ctx& ctx, const mps_solver_opts* o)
     return l0;
 }
 
+// the ghosted row pitch of a level in the block: nx+2, or 24 for FP32 rows of
+// 16 cells (8 per colour), so that the four rows a warp takes in a colour pass
+// (stride-2 accesses) fall on distinct banks
+template <class T>
+static int sub_gx(const Lev& L)
+{
+    return (sizeof(T) == 4 && L.nh == 8 && L.nx + 2 <= 24) ? 24 : L.nx + 2;
+}
+
 // one level of the block's plan: Lev's sizes, widths and boundary flags
 template <class T>
 static SubGeo<T> sub_geo(const Lev& L)
@@ -1064,7 +1082,7 @@ static SubGeo<T> sub_geo(const Lev& L)
     G.rows = L.ny * L.nz;
     G.rc = SUB_TPB / L.nh;
     G.rn = SUB_TPB / L.nx;
-    G.gx = L.nx + 2;
+    G.gx = sub_gx<T>(L);
     G.gy = L.ny + 2;
     G.pitch = L.P;
     for (int a = 0; a < 3; a++) {
@@ -1085,7 +1103,8 @@ template <class T>
 static void sub_axes(const Lev& L, SubAx<T>* out)
 {
     const int n3[3] = {L.nx, L.ny, L.nz};
-    const int st3[3] = {1, L.nx + 2, (L.nx + 2) * (L.ny + 2)};
+    const int gx = sub_gx<T>(L);
+    const int st3[3] = {1, gx, gx * (L.ny + 2)};
     int e = 0;
     for (int a = 0; a < 3; a++) {
         const int n = n3[a], st = st3[a];
@@ -1145,7 +1164,7 @@ static bool sub_layout_with(const Ctx& ctx, int l0, bool kf, bool df, const mps_
         sub_axes<T>(L, P.ax + nax);
         nax += L.nx + L.ny + L.nz;
         nrow += L.ny * L.nz;
-        P.ou[s] = (int)off; off += (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+        P.ou[s] = (int)off; off += (long long)sub_gx<T>(L) * (L.ny + 2) * (L.nz + 2);
         P.of[s] = (int)off; off += (long long)L.nx * L.ny * L.nz;
         if (s < nl - 1) {
             const Xfer& X = ctx.xf[l0 + s];
@@ -1177,7 +1196,7 @@ static bool sub_layout_with(const Ctx& ctx, int l0, bool kf, bool df, const mps_
     P.img_off = (int)(off * sizeof(T));
     for (int s = 0; s < nl; s++) {
         const Lev& L = ctx.lev[l0 + s];
-        P.ok[s] = kf ? (int)off : -1; off += kf ? (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) : 0;
+        P.ok[s] = kf ? (int)off : -1; off += kf ? (long long)sub_gx<T>(L) * (L.ny + 2) * (L.nz + 2) : 0;
         P.od[s] = df ? (int)off : -1; off += df ? (long long)L.nx * L.ny * L.nz : 0;
     }
     size_t bytes = ((size_t)off * sizeof(T) + 15) & ~(size_t)15;

@@ -72,7 +72,7 @@ template <class T>
 struct SubGeo {
     int nx, ny, nz, nh;
     int rows;              // ny*nz
-    int gx, gy;            // ghosted row and plane sizes: nx+2, ny+2
+    int gx, gy;            // ghosted row and plane sizes: nx+2 (or a padded pitch), ny+2
     int pitch;             // row pitch of the level's split layout (Lev::P)
     int per;               // bit a: periodic axis a
     int dirc;              // bit f: Dirichlet face f (LEFT..FRONT)
